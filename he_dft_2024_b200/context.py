@@ -1,0 +1,203 @@
+"""Host-side mirror of the reference's call surface over the C-ABI.
+
+``Context`` owns one he_ctx_t.  Its methods carry the names of the Fortran routines they replace
+(poten, potenimp, forceimp, steprk, steppc, energy, steprkr, steppcr, varmu, derden) and keep
+their argument meaning; module arrays move with ``upload``/``download`` in the reference's
+column-major layout.  Errors raise ``HeError`` with the library's message (the reference STOPs).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import FIELDS, HeError, dptr
+from .config import MP_U, KTOPS, Workload, potion_table
+
+COMPLEX_DYN = {"psi", "pc", "q", "psiold1", "psiold2", "psiold3", "hpsiold1", "hpsiold2"}
+
+
+class Context:
+    def __init__(self, w: Workload, mode="dynamics", compute_kernels=True):
+        self.L = _lib.load()
+        self.w = w
+        self.mode = _lib.HE_MODE_DYNAMICS if mode == "dynamics" else _lib.HE_MODE_STATICS
+        g = _lib.HeGrid(w.nx, w.ny, w.nz, w.xmax, w.ymax, w.zmax, w.npd, w.icon)
+        core = {"OT": b"OT ", "OP": b"OP ", "OTC": b"OTC"}[w.core]
+        f = _lib.HeFunctional(core, w.h4, w.eps4, w.sigma4, w.cp4, w.cpp4, w.den4c, w.alphas,
+                              w.l, w.den0s, w.h2o2m4, w.lsolid, w.C, w.beta, w.den_m)
+        h = ctypes.c_void_p()
+        st = self.L.he_ctx_create(ctypes.byref(g), ctypes.byref(f), self.mode, _lib.HE_PREC_F64,
+                                  ctypes.byref(h))
+        self.h = h.value
+        if st != 0:
+            msg = self.L.he_last_error(self.h).decode() if self.h else "no context"
+            self.close()
+            raise HeError(st, msg)
+        if compute_kernels:
+            self._ck(self.L.he_compute_kernels(self.h))
+        if self.mode == _lib.HE_MODE_DYNAMICS:
+            ab = _lib.HeAbsorber(w.lambdah, w.txmean, w.txsurf, w.tymean, w.tysurf, w.tzmean,
+                                 w.tzsurf)
+            self._ck(self.L.he_set_absorber(self.h, ctypes.byref(ab)))
+            if w.n_imp > 0:
+                self.set_impurities(w)
+
+    # ---- plumbing -------------------------------------------------------------------------------
+    def _ck(self, st):
+        if st != 0:
+            raise HeError(st, self.L.he_last_error(self.h).decode())
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.he_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def launches(self):
+        return int(self.L.he_launch_count(self.h))
+
+    @property
+    def device_bytes(self):
+        return int(self.L.he_device_bytes(self.h))
+
+    def synchronize(self):
+        self._ck(self.L.he_synchronize(self.h))
+
+    def set_stream(self, stream_ptr):
+        self._ck(self.L.he_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def _shape(self, name):
+        w = self.w
+        if name in ("fden", "fvlj4", "wcgk"):
+            return (w.nx // 2 + 1, w.ny, w.nz)
+        if name in ("rimp", "vimp", "aimp", "F", "pcr", "pcv", "qr", "qv"):
+            return (w.n_imp, 3)
+        if name in ("rimpold", "vimpold"):
+            return (w.n_imp, 3, 3)
+        if name == "aimpold":
+            return (w.n_imp, 3, 2)
+        if name == "ring":
+            return (13,)
+        return (w.nx, w.ny, w.nz)
+
+    def _is_complex(self, name):
+        return name == "fden" or (self.mode == _lib.HE_MODE_DYNAMICS and name in COMPLEX_DYN)
+
+    def upload(self, name, arr):
+        dt = np.complex128 if self._is_complex(name) else np.float64
+        a = np.asarray(arr, dtype=dt).reshape(self._shape(name), order="F")
+        buf = np.ascontiguousarray(a.ravel(order="F"))
+        self._ck(self.L.he_upload(self.h, FIELDS[name], buf.ctypes.data_as(ctypes.c_void_p),
+                                  buf.nbytes))
+
+    def download(self, name):
+        dt = np.complex128 if self._is_complex(name) else np.float64
+        shape = self._shape(name)
+        buf = np.empty(int(np.prod(shape)), dtype=dt)
+        self._ck(self.L.he_download(self.h, FIELDS[name], buf.ctypes.data_as(ctypes.c_void_p),
+                                    buf.nbytes))
+        return buf.reshape(shape, order="F")
+
+    # ---- set-up ---------------------------------------------------------------------------------
+    def set_kernels(self, fvlj4, wcgk):
+        a = np.ascontiguousarray(np.asarray(fvlj4, np.float64).ravel(order="F"))
+        b = np.ascontiguousarray(np.asarray(wcgk, np.float64).ravel(order="F"))
+        self._ck(self.L.he_set_kernels(self.h, dptr(a), dptr(b), None))
+
+    def set_impurities(self, w: Workload):
+        potion, npot, delinter, rmax = potion_table(w)
+        self._potion = np.ascontiguousarray(potion.ravel(order="F"))
+        self._m = np.ascontiguousarray(np.asarray(w.m_imp_u, np.float64))
+        im = _lib.HeImpurities(w.n_imp, dptr(self._m), dptr(self._potion), npot, delinter, rmax,
+                               w.ii_kind, w.ii_D, w.ii_re, w.ii_a, w.ii_rcut, w.ii_umax)
+        self._ck(self.L.he_set_impurities(self.h, ctypes.byref(im)))
+        if w.rimp0:
+            self.upload("rimp", np.array(w.rimp0, dtype=np.float64))
+        if w.vimp0_aps:
+            # imp.input gives A/ps; the driver converts to A K (DFT4He3d.f90:313)
+            self.upload("vimp", np.array(w.vimp0_aps, dtype=np.float64) * KTOPS)
+
+    # ---- Dynamics_TDDFT routines ----------------------------------------------------------------
+    def poten(self):
+        self._ck(self.L.he_poten(self.h))
+
+    def potenimp(self):
+        self._ck(self.L.he_potenimp(self.h))
+
+    def forceimp(self, want=False):
+        if want:
+            F = np.zeros(3 * max(self.w.n_imp, 1))
+            self._ck(self.L.he_forceimp(self.h, dptr(F)))
+            return F[: 3 * self.w.n_imp].reshape((self.w.n_imp, 3), order="F")
+        self._ck(self.L.he_forceimp(self.h, None))
+        return None
+
+    def set_accel(self):
+        self._ck(self.L.he_set_accel(self.h))
+
+    def lstopimp(self):
+        f = ctypes.c_int(0)
+        self._ck(self.L.he_lstopimp(self.h, ctypes.byref(f)))
+        return bool(f.value)
+
+    def steprk(self, deltat):
+        self._ck(self.L.he_steprk(self.h, deltat))
+
+    def steppc(self, deltat, errors=True):
+        if not errors:
+            self._ck(self.L.he_steppc(self.h, deltat, None, None, None))
+            return None
+        e = [ctypes.c_double(0.0) for _ in range(3)]
+        self._ck(self.L.he_steppc(self.h, deltat, *[ctypes.byref(x) for x in e]))
+        return tuple(x.value for x in e)
+
+    def energy(self):
+        e = _lib.HeEnergies()
+        self._ck(self.L.he_energy(self.h, ctypes.byref(e)))
+        return {k: getattr(e, k) for k, _ in _lib.HeEnergies._fields_}
+
+    def derden(self):
+        self._ck(self.L.he_derden(self.h))
+
+    # ---- He_statics routines --------------------------------------------------------------------
+    def refresh_density(self):
+        self._ck(self.L.he_refresh_density(self.h))
+
+    def evolo0(self, mu4, n4):
+        m, e = ctypes.c_double(mu4), ctypes.c_double(0.0)
+        self._ck(self.L.he_evolo0(self.h, ctypes.byref(m), ctypes.byref(e), n4))
+        return m.value, e.value
+
+    def steprkr(self, deltat, mu4, n4):
+        m, e = ctypes.c_double(mu4), ctypes.c_double(0.0)
+        self._ck(self.L.he_steprkr(self.h, deltat, ctypes.byref(m), ctypes.byref(e), n4))
+        return m.value, e.value
+
+    def steppcr(self, deltat, mu4, n4):
+        m, e, p = ctypes.c_double(mu4), ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._ck(self.L.he_steppcr(self.h, deltat, ctypes.byref(m), ctypes.byref(e), n4,
+                                   ctypes.byref(p)))
+        self.errpc = p.value
+        return m.value, e.value
+
+    def varmu(self, npart, mu):
+        e = ctypes.c_double(0.0)
+        self._ck(self.L.he_varmu(self.h, npart, mu, ctypes.byref(e)))
+        return e.value
+
+
+def mass_of(w: Workload):
+    return np.asarray(w.m_imp_u, np.float64) * MP_U

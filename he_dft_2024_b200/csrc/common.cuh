@@ -1,0 +1,65 @@
+// common.cuh -- shared device helpers for the sm_100a mean-field / time-step kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#define HE_HD __host__ __device__ __forceinline__
+#define HE_D __device__ __forceinline__
+
+namespace he {
+
+// ---- complex binary64 arithmetic on double2 (re, im) ------------------------------------------
+HE_HD double2 c2(double re, double im) { return make_double2(re, im); }
+HE_HD double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+HE_HD double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+HE_HD double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+HE_HD double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+HE_HD double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+HE_HD double2 cmul_conj_if(double2 a, double2 w, bool conj_w) {
+  double wy = conj_w ? -w.y : w.y;
+  return make_double2(a.x * w.x - a.y * wy, a.x * wy + a.y * w.x);
+}
+HE_HD double cnorm2(double2 a) { return a.x * a.x + a.y * a.y; }
+// -i * a
+HE_HD double2 cmi(double2 a) { return make_double2(a.y, -a.x); }
+// +i * a
+HE_HD double2 cpi(double2 a) { return make_double2(-a.y, a.x); }
+
+// Generic helpers so stencil code can be written once for real and complex fields.
+HE_HD double zero_of(double) { return 0.0; }
+HE_HD double2 zero_of(double2) { return make_double2(0.0, 0.0); }
+HE_HD double axpy(double w, double f, double acc) { return acc + w * f; }
+HE_HD double2 axpy(double w, double2 f, double2 acc) {
+  return make_double2(acc.x + w * f.x, acc.y + w * f.y);
+}
+HE_HD double neg_if(double v, bool n) { return n ? -v : v; }
+HE_HD double2 neg_if(double2 v, bool n) { return n ? make_double2(-v.x, -v.y) : v; }
+
+// ---- block reduction of NV doubles (fixed order => deterministic) ------------------------------
+template <int NV>
+__device__ void block_reduce_store(double (&v)[NV], double* __restrict__ out) {
+  __shared__ double red[32][NV > 0 ? NV : 1];
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthr = blockDim.x * blockDim.y * blockDim.z;
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp][k] = s;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int nw = (nthr + 31) >> 5;
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += red[w][k];
+      out[k] = s;
+    }
+  }
+}
+
+}  // namespace he

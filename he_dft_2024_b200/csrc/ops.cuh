@@ -1,0 +1,472 @@
+// ops.cuh -- consumers fused into the 13-point stencil pass, pointwise passes and the classical
+// impurity integrator (binary64).
+#pragma once
+#include "stencil.cuh"
+
+namespace he {
+
+// ---- deterministic grid reduction: per-block partials, the last CTA to finish sums them ------
+struct ReduceTail {
+  double* partials;
+  unsigned* counter;
+  double* out;
+};
+
+template <int NV>
+__device__ void reduce_tail(const ReduceTail& rt, long nb) {
+  __shared__ bool s_last;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthr = blockDim.x * blockDim.y * blockDim.z;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(rt.counter, 1u);
+    s_last = (t == (unsigned)(nb - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = 0.0;
+    for (long b = tid; b < nb; b += nthr) s += __ldcg(rt.partials + b * NV + k);
+    v[k] = s;
+  }
+  block_reduce_store<NV>(v, rt.out);
+  if (tid == 0) *rt.counter = 0u;
+}
+
+// Stencil kernel with the reduction tail (ops with NV > 0).
+template <class Op, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY)
+    k_stencil_red(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
+                  const ReduceTail rt) {
+  using T = typename Op::T;
+  constexpr int NV = Op::NV;
+  __shared__ T tile[TY + 12][TX + 12];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + TX * ty;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int ix = x0 + tx, iy = y0 + ty;
+  const int z0 = blockIdx.z * g.zc;
+  const int z1 = min(z0 + g.zc, g.nz);
+  const bool inside = (ix < g.nx) && (iy < g.ny);
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  T q[13];
+#pragma unroll
+  for (int m = 0; m < 12; ++m)
+    q[m + 1] = inside ? load_bc(f, g, ix, iy, z0 - 6 + m) : zero_of(T());
+  for (int iz = z0; iz < z1; ++iz) {
+#pragma unroll
+    for (int m = 0; m < 12; ++m) q[m] = q[m + 1];
+    q[12] = inside ? load_bc(f, g, ix, iy, iz + 6) : zero_of(T());
+    tile[ty + 6][tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
+    for (int e = tid; e < 12 * TY; e += TX * TY) {
+      const int r = e / 12, c = e - r * 12;
+      const int sx = (c < 6) ? c : TX + c;
+      tile[r + 6][sx] = load_bc(f, g, x0 + sx - 6, y0 + r, iz);
+    }
+    for (int e = tid; e < 12 * TX; e += TX * TY) {
+      const int r = e / TX, c = e - r * TX;
+      const int sy = (r < 6) ? r : TY + r;
+      tile[sy][c + 6] = load_bc(f, g, x0 + c, y0 + sy - 6, iz);
+    }
+    __syncthreads();
+    if (inside) {
+      T dx = zero_of(T()), dy = zero_of(T()), dz = zero_of(T());
+      if (g.axis_on[0]) {
+#pragma unroll
+        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tile[ty + 6][tx + m], dx);
+      }
+      if (g.axis_on[1]) {
+#pragma unroll
+        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tile[ty + m][tx + 6], dy);
+      }
+      if (g.axis_on[2]) {
+#pragma unroll
+        for (int m = 0; m < 13; ++m) dz = axpy(g.w[2][m], q[m], dz);
+      }
+      const long idx = (long)ix + (long)g.nx * ((long)iy + (long)g.ny * iz);
+      op.at(ix, iy, iz, idx, dx, dy, dz, q[6], acc);
+    }
+    __syncthreads();
+  }
+  const long nb = (long)gridDim.x * gridDim.y * gridDim.z;
+  const long b = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
+  block_reduce_store<NV>(acc, rt.partials + b * NV);
+  reduce_tail<NV>(rt, nb);
+}
+
+// ---- absorbing mask: timec = (Lambdah*(1+tx+1+ty+1+tz), 1)  (DFT4He3d.f90:592-601) -----------
+struct Timec {
+  const double* ax;  // tanh((|x_i|-txmean)/txsurf), host-evaluated per axis
+  const double* ay;
+  const double* az;
+  double lambdah;
+  HE_D double re(int ix, int iy, int iz) const {
+    double s = 1.0 + ax[ix];
+    s = s + 1.0 + ay[iy];
+    s = s + 1.0 + az[iz];
+    return lambdah * s;
+  }
+};
+
+// H psi of the real-time classical path (steprk.f90:67, steppc.f90:51,118):
+//   timec*((d2x+d2y+d2z)*h2o2m4 - pot4*psi) - i*uimp*psi,  timec = (tr, 1).
+HE_D double2 hpsi_rt(double2 dx, double2 dy, double2 dz, double2 c, double pot, double u,
+                     double tr, double h2o2m) {
+  const double2 lap = cadd(cadd(dx, dy), dz);
+  const double ax = lap.x * h2o2m - pot * c.x;
+  const double ay = lap.y * h2o2m - pot * c.y;
+  return make_double2(tr * ax - ay + u * c.y, tr * ay + ax - u * c.x);
+}
+
+// steppc predictor + modifier (steppc.f90:51-61).  po3 = psiold(ioldp(3)) is read and receives
+// the new psi (the host then swaps it with the psi buffer, so psiold(ioldp(3)) holds the old psi).
+struct OpPredict {
+  using T = double2;
+  static constexpr int NV = 0;
+  const double* pot4;
+  const double* uimp;
+  double2* po3;
+  const double2* h1;
+  double2* h2;
+  double2* pc;
+  double* den;
+  Timec tm;
+  double h2o2m, s43, c112;
+  HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
+               double*) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, pot4[i], uimp[i], tm.re(ix, iy, iz), h2o2m);
+    const double2 hh1 = h1[i], hh2 = h2[i];
+    const double2 t = make_double2(2.0 * s4.x - hh1.x + 2.0 * hh2.x, 2.0 * s4.y - hh1.y + 2.0 * hh2.y);
+    const double2 p3 = po3[i];
+    const double2 sto1 = make_double2(p3.x + s43 * t.x, p3.y + s43 * t.y);
+    const double2 pcv = pc[i];
+    const double2 pn = make_double2(sto1.x - c112 * pcv.x, sto1.y - c112 * pcv.y);
+    pc[i] = sto1;
+    h2[i] = s4;
+    po3[i] = pn;
+    den[i] = cnorm2(pn);
+  }
+};
+
+// steppc corrector + final value (steppc.f90:118-127); accumulates sum |pc|.
+struct OpCorrect {
+  using T = double2;
+  static constexpr int NV = 1;
+  const double* pot4;
+  const double* uimp;
+  const double2* po3;
+  const double2* po2;
+  const double2* h1;
+  const double2* h2;
+  double2* pc;
+  double2* out;
+  double* den;
+  Timec tm;
+  double h2o2m, s3, c9;
+  HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
+               double* acc) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, pot4[i], uimp[i], tm.re(ix, iy, iz), h2o2m);
+    const double2 a3 = po3[i], a2 = po2[i], b1 = h1[i], b2 = h2[i];
+    const double2 inner = make_double2(s4.x + 2.0 * b1.x - b2.x, s4.y + 2.0 * b1.y - b2.y);
+    const double2 s5 = make_double2(0.125 * (9.0 * a3.x - a2.x + s3 * inner.x),
+                                    0.125 * (9.0 * a3.y - a2.y + s3 * inner.y));
+    const double2 p = pc[i];
+    const double2 pn = make_double2(p.x - s5.x, p.y - s5.y);
+    pc[i] = pn;
+    const double2 o = make_double2(s5.x + c9 * pn.x, s5.y + c9 * pn.y);
+    out[i] = o;
+    den[i] = cnorm2(o);
+    acc[0] += hypot(pn.x, pn.y);
+  }
+};
+
+// One RK-Gill stage (steprk.f90:67-79).  hsave (stage 1 only) receives H psi for hpsiold(1).
+struct OpRK {
+  using T = double2;
+  static constexpr int NV = 0;
+  const double* pot4;
+  const double* uimp;
+  double2* q;
+  double2* out;
+  double2* hsave;
+  double* den;
+  Timec tm;
+  double h2o2m, a, b, cc, dt;
+  HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
+               double*) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, pot4[i], uimp[i], tm.re(ix, iy, iz), h2o2m);
+    const double2 qq = q[i];
+    const double2 s1 = make_double2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
+    q[i] = make_double2(qq.x + 3.0 * s1.x - cc * s4.x, qq.y + 3.0 * s1.y - cc * s4.y);
+    if (hsave) hsave[i] = s4;
+    const double2 pn = make_double2(c.x + dt * s1.x, c.y + dt * s1.y);
+    out[i] = pn;
+    den[i] = cnorm2(pn);
+  }
+};
+
+// energy(): Dynamics_TDDFT/energy.f90:107-165 sums (first derivatives of psi).
+//   acc = {sum |grad psi|^2, sum delj4*den, sum den*dencg^2*(cp4/2+cpp4/3*dencg),
+//          sum den*(1+tanh(beta*(den-den_m))), sum uimp*den}
+template <typename TT>
+struct OpEnergy {
+  using T = TT;
+  static constexpr int NV = 5;
+  const double* den;
+  const double* dencg;
+  const double* delj4;
+  const double* uimp;  // may be null (statics)
+  double aux1, aux2, beta, den_m;
+  int lsolid;
+  HE_D static double n2(double v) { return v * v; }
+  HE_D static double n2(double2 v) { return v.x * v.x + v.y * v.y; }
+  HE_D void at(int, int, int, long i, T dx, T dy, T dz, T, double* acc) const {
+    const double a3 = den[i], a4 = dencg[i];
+    acc[0] += n2(dx) + n2(dy) + n2(dz);
+    acc[1] += delj4[i] * a3;
+    acc[2] += a3 * a4 * a4 * (aux1 + aux2 * a4);
+    if (lsolid) acc[3] += a3 * (1.0 + tanh(beta * (a3 - den_m)));
+    if (uimp) acc[4] += uimp[i] * a3;
+  }
+};
+
+// derden(): dxden, dyden, dzden (derden.f90:26-28).
+struct OpDerden {
+  using T = double;
+  static constexpr int NV = 0;
+  double* gx;
+  double* gy;
+  double* gz;
+  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double, double*) const {
+    gx[i] = dx;
+    gy[i] = dy;
+    gz[i] = dz;
+  }
+};
+
+// ---- classical impurities ----------------------------------------------------------------------
+constexpr int kMaxImp = 8;
+
+// Device copy of the classicimp module (modules.f90:303-343).  Arrays use the Fortran layout
+// with leading dimension n: (n,3) -> k + n*c, (n,3,slot) -> k + n*c + 3n*(slot-1).
+struct ImpDev {
+  int n;
+  double m[kMaxImp];
+  double rimp[3 * kMaxImp], vimp[3 * kMaxImp], aimp[3 * kMaxImp], F[3 * kMaxImp];
+  double qr[3 * kMaxImp], qv[3 * kMaxImp], pcr[3 * kMaxImp], pcv[3 * kMaxImp];
+  double rimpold[9 * kMaxImp], vimpold[9 * kMaxImp], aimpold[6 * kMaxImp];
+  int ioldr[3], ioldv[3], iolda[2];
+  double errimp, errvimp;
+  int lstopimp, lgridnoout;
+  int ii_kind;
+  double ii_D, ii_re, ii_a, ii_rcut, ii_umax;
+};
+
+// updatepoten + the He part of forceimp (potenimp.f90:95-121, :49-52) in one stencil pass over
+// den: uimp = sum_k V_k(|r-R_k|) by linear interpolation of the potenimpini table, and
+// acc[3k+c] = sum d_c(den) * V_k.  Off-table radii set lstopimp (potenimp.f90:104-109); the
+// radius is clamped to the table end and the index is taken after the clamp.
+template <int NI>
+struct OpImpField {
+  using T = double;
+  static constexpr int NV = 3 * NI;
+  const double* tab;  // (npot) per impurity, impurity-major
+  ImpDev* imp;
+  double* uimp;
+  int n, npot;
+  double delinter, rmax;
+  double xmax, ymax, zmax, hx, hy, hz;
+  HE_D void at(int ix, int iy, int iz, long i, double dx, double dy, double dz, double,
+               double* acc) const {
+    const double x = -xmax + hx * ix, y = -ymax + hy * iy, z = -zmax + hz * iz;
+    double u = 0.0;
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      if (k < n) {
+        const double rx = imp->rimp[k], ry = imp->rimp[k + n], rz = imp->rimp[k + 2 * n];
+        const double zt = (z - rz) * (z - rz);
+        const double yt = (y - ry) * (y - ry) + zt;
+        double r = sqrt((x - rx) * (x - rx) + yt);
+        if (!(r <= rmax)) {  // also catches a NaN radius
+          if (imp->lgridnoout) atomicExch(&imp->lstopimp, 1);
+          r = rmax;
+        }
+        int i0 = (int)(r / delinter);
+        if (i0 > npot - 2) i0 = npot - 2;
+        const double rmod = fmod(r, delinter) / delinter;
+        const double* t = tab + (long)k * npot;
+        const double uk = t[i0] * (1.0 - rmod) + t[i0 + 1] * rmod;
+        u = u + uk;
+        acc[3 * k + 0] += dx * uk;
+        acc[3 * k + 1] += dy * uk;
+        acc[3 * k + 2] += dz * uk;
+      }
+    }
+    uimp[i] = u;
+  }
+};
+
+HE_D double pair_pot(const ImpDev& s, double r) {
+  if (s.ii_kind == 0) return (r < s.ii_rcut) ? s.ii_umax : 0.0;
+  if (r < s.ii_rcut) return s.ii_umax;
+  const double e = 1.0 - exp(-s.ii_a * (r - s.ii_re));
+  return s.ii_D * (e * e - 1.0);
+}
+HE_D double pair_dpot(const ImpDev& s, double r) {
+  if (s.ii_kind == 0 || r < s.ii_rcut) return 0.0;
+  const double ex = exp(-s.ii_a * (r - s.ii_re));
+  return 2.0 * s.ii_D * s.ii_a * (1.0 - ex) * ex;
+}
+
+// forceimp: F(k,c) = -sum(d_c den * uimp_k)*dxyz + sum_m F_ij(k,m,c)  (potenimp.f90:40-58).
+__global__ void k_imp_force(ImpDev* s, const double* sums, double dxyz) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = s->n;
+  for (int k = 0; k < n; ++k)
+    for (int c = 0; c < 3; ++c) s->F[k + n * c] = -sums[3 * k + c] * dxyz;
+  for (int k = 0; k < n; ++k)
+    for (int m = 0; m < n; ++m) {
+      if (m == k) continue;
+      double d[3];
+      for (int c = 0; c < 3; ++c) d[c] = s->rimp[k + n * c] - s->rimp[m + n * c];
+      const double a1 = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      const double dv = pair_dpot(*s, a1);
+      for (int c = 0; c < 3; ++c) s->F[k + n * c] = s->F[k + n * c] + (-dv * d[c] / a1);
+    }
+}
+
+// aimp = F / m_imp (DFT4He3d.f90:571-573).
+__global__ void k_imp_accel(ImpDev* s) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = s->n;
+  for (int k = 0; k < n; ++k)
+    for (int c = 0; c < 3; ++c) s->aimp[k + n * c] = s->F[k + n * c] / s->m[k];
+}
+
+// Impurity part of one RK-Gill stage (steprk.f90:92-125).
+__global__ void k_imp_rk(ImpDev* s, int jr, double a, double b, double cc, double dt) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = s->n;
+  double stor[3 * kMaxImp];
+  for (int i = 0; i < 3 * n; ++i) {
+    stor[i] = a * (s->vimp[i] - b * s->qr[i]);
+    s->qr[i] = s->qr[i] + 3.0 * stor[i] - cc * s->vimp[i];
+  }
+  if (jr == 0)
+    for (int i = 0; i < 3 * n; ++i) {
+      s->rimpold[i + 6 * n] = s->rimpold[i + 3 * n];
+      s->rimpold[i + 3 * n] = s->rimpold[i];
+      s->rimpold[i] = s->rimp[i];
+    }
+  for (int i = 0; i < 3 * n; ++i) s->rimp[i] = s->rimp[i] + dt * stor[i];
+  for (int i = 0; i < 3 * n; ++i) {
+    stor[i] = a * (s->aimp[i] - b * s->qv[i]);
+    s->qv[i] = s->qv[i] + 3.0 * stor[i] - cc * s->aimp[i];
+  }
+  if (jr == 0)
+    for (int i = 0; i < 3 * n; ++i) {
+      s->aimpold[i + 3 * n] = s->aimpold[i];
+      s->aimpold[i] = s->aimp[i];
+      s->vimpold[i + 6 * n] = s->vimpold[i + 3 * n];
+      s->vimpold[i + 3 * n] = s->vimpold[i];
+      s->vimpold[i] = s->vimp[i];
+    }
+  for (int i = 0; i < 3 * n; ++i) s->vimp[i] = s->vimp[i] + dt * stor[i];
+  if (jr == 3) {
+    for (int i = 0; i < 3; ++i) { s->ioldr[i] = i + 1; s->ioldv[i] = i + 1; }
+    for (int i = 0; i < 2; ++i) s->iolda[i] = i + 1;
+  }
+}
+
+// Impurity predictor + modifier (steppc.f90:80-99).  The velocity prediction is stored in
+// vimpold(:,:,ioldv(3)) and vimp keeps v_n, as in the reference.
+__global__ void k_imp_predict(ImpDev* s, double dt) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = s->n;
+  const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
+  const double sd = c4o3 * dt;
+  const int r3 = 3 * n * (s->ioldr[2] - 1);
+  const int v1 = 3 * n * (s->ioldv[0] - 1), v2 = 3 * n * (s->ioldv[1] - 1),
+            v3 = 3 * n * (s->ioldv[2] - 1);
+  const int a1 = 3 * n * (s->iolda[0] - 1), a2 = 3 * n * (s->iolda[1] - 1);
+  for (int i = 0; i < 3 * n; ++i) {
+    const double st = s->rimpold[r3 + i] +
+                      sd * (2.0 * s->vimp[i] - s->vimpold[v1 + i] + 2.0 * s->vimpold[v2 + i]);
+    s->rimpold[r3 + i] = s->rimp[i];
+    s->rimp[i] = st - c112 * s->pcr[i];
+    s->pcr[i] = st;
+  }
+  for (int i = 0; i < 3 * n; ++i) {
+    const double st = s->vimpold[v3 + i] +
+                      sd * (2.0 * s->aimp[i] - s->aimpold[a1 + i] + 2.0 * s->aimpold[a2 + i]);
+    s->vimpold[v3 + i] = st - c112 * s->pcv[i];
+    s->pcv[i] = st;
+  }
+  for (int i = 0; i < 3 * n; ++i) s->aimpold[a2 + i] = s->aimp[i];
+  const int t = s->iolda[1];
+  s->iolda[1] = s->iolda[0];
+  s->iolda[0] = t;
+}
+
+// Impurity corrector (steppc.f90:149-174).  aimp is the value set by the driver before the step
+// (the forceimp inside steppc refreshes F but not aimp), as in the reference.
+__global__ void k_imp_correct(ImpDev* s, double dt) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = s->n;
+  const double c9 = 9.0 / 121.0;
+  const double s3 = 3.0 * dt;
+  int r2 = 3 * n * (s->ioldr[1] - 1), r3 = 3 * n * (s->ioldr[2] - 1);
+  int v1 = 3 * n * (s->ioldv[0] - 1), v2 = 3 * n * (s->ioldv[1] - 1),
+      v3 = 3 * n * (s->ioldv[2] - 1);
+  const int a1 = 3 * n * (s->iolda[0] - 1), a2 = 3 * n * (s->iolda[1] - 1);
+  double er = 0.0;
+  for (int i = 0; i < 3 * n; ++i) {
+    const double st = 0.125 * (9.0 * s->rimpold[r3 + i] - s->rimpold[r2 + i] +
+                               s3 * (s->vimpold[v3 + i] + 2.0 * s->vimp[i] - s->vimpold[v1 + i]));
+    s->pcr[i] = s->pcr[i] - st;
+    s->rimp[i] = st + c9 * s->pcr[i];
+  }
+  for (int i = 0; i < 3 * n; ++i) er += fabs(c9 * s->pcr[i]);
+  s->errimp = er * 0.3333333333 / n;
+  int t = s->ioldr[2];
+  s->ioldr[2] = s->ioldr[1];
+  s->ioldr[1] = s->ioldr[0];
+  s->ioldr[0] = t;
+  double ev = 0.0;
+  for (int i = 0; i < 3 * n; ++i) {
+    const double st = 0.125 * (9.0 * s->vimp[i] - s->vimpold[v2 + i] +
+                               s3 * (s->aimp[i] + 2.0 * s->aimpold[a1 + i] - s->aimpold[a2 + i]));
+    s->pcv[i] = s->pcv[i] - st;
+    s->vimpold[v3 + i] = s->vimp[i];
+    s->vimp[i] = st + c9 * s->pcv[i];
+  }
+  for (int i = 0; i < 3 * n; ++i) ev += fabs(c9 * s->pcv[i]);
+  s->errvimp = ev * 0.3333333333 / n;
+  t = s->ioldv[2];
+  s->ioldv[2] = s->ioldv[1];
+  s->ioldv[1] = s->ioldv[0];
+  s->ioldv[0] = t;
+}
+
+// ---- statics (real psi) ------------------------------------------------------------------------
+// hpsi = -(d2x+d2y+d2z)*h2o2m4 + pot4*psi; acc = sum psi*hpsi  (steppcr.f90:40-42).
+struct OpHpsiR {
+  using T = double;
+  static constexpr int NV = 1;
+  const double* pot4;
+  double* out;
+  double h2o2m;
+  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double c,
+               double* acc) const {
+    const double h = -((dx + dy) + dz) * h2o2m + pot4[i] * c;
+    out[i] = h;
+    acc[0] += c * h;
+  }
+};
+
+}  // namespace he

@@ -1,0 +1,72 @@
+"""Driver sequences of the reference main loops, written against the call surface only.
+
+These functions mirror what the unchanged Fortran drivers do around the replaced routines
+(Dynamics_TDDFT/DFT4He3d.f90:540-576 set-up and :671-697 loop; He_statics/BCN4HeDFT.f90:815-875
+set-up and :1086-1160 loop).  They take any object exposing the routines (the device Context,
+or the CPU oracle in the tests), so both sides run the identical sequence.
+"""
+import numpy as np
+
+from .config import Workload, grid_axes
+
+
+def initial_wavefunction(w: Workload, den, kick=(0.0, 0.0, 0.0)):
+    """psi = sqrt(den) * exp(i (x*lx + y*ly + z*lz)) (DFT4He3d.f90:540-557)."""
+    x, y, z = grid_axes(w)
+    lx, ly, lz = kick
+    ph = x[:, None, None] * lx + y[None, :, None] * ly + z[None, None, :] * lz
+    return np.asfortranarray(np.sqrt(den) * (np.cos(ph) + 1j * np.sin(ph)))
+
+
+def dynamics_setup(s, psi, n_imp):
+    """den = conjg(psi)*psi; potenimp; poten; forceimp; aimp = F/m (DFT4He3d.f90:562-573)."""
+    s.set("psi", psi) if hasattr(s, "set") else s.upload("psi", psi)
+    den = (np.conj(psi) * psi).real
+    s.set("den", den) if hasattr(s, "set") else s.upload("den", den)
+    if n_imp > 0:
+        s.potenimp()
+    s.poten()
+    if n_imp > 0:
+        s.forceimp()
+        s.set_accel()
+
+
+def dynamics_iteration(s, iteraux, deltat, n_imp, lrk=False, errors=False):
+    """One pass of the time loop body (DFT4He3d.f90:677-697): steprk for the first three
+    iterations (or always when lrk), steppc after; then potenimp, poten, forceimp, aimp=F/m."""
+    err = None
+    if iteraux <= 3 or lrk:
+        s.steprk(deltat)
+    else:
+        err = s.steppc(deltat) if errors or not hasattr(s, "upload") else s.steppc(deltat, errors=False)
+    if n_imp > 0:
+        s.potenimp()
+    s.poten()
+    if n_imp > 0:
+        s.forceimp()
+        s.set_accel()
+    return err
+
+
+def statics_setup(s, den, n4):
+    """psi = sqrt(den); derden; fden; dencg; poten; evolo(0) (BCN4HeDFT.f90:815-875, :1050)."""
+    psi = np.sqrt(den)
+    put = s.set if hasattr(s, "set") else s.upload
+    put("den", den)
+    put("psi", psi)
+    s.refresh() if hasattr(s, "refresh") else s.refresh_density()
+    s.poten()
+    mu, _ = s.evolo0(0.0, n4)
+    return mu
+
+
+def statics_iteration(s, iterrk, deltat, mu4, n4):
+    """One pass of the statics loop (BCN4HeDFT.f90:1113-1160) with Lrkpc: steprkr for the first
+    four iterations, steppcr after; then derden, fden, dencg and poten (ppot = 1)."""
+    if iterrk <= 4:
+        mu4, err = s.steprkr(deltat, mu4, n4)
+    else:
+        mu4, err = s.steppcr(deltat, mu4, n4)
+    s.refresh() if hasattr(s, "refresh") else s.refresh_density()
+    s.poten()
+    return mu4, err

@@ -1,0 +1,194 @@
+/*
+ * he_dft.h -- C-ABI of the B200 (sm_100a) mean-field and time-step path of BCN-4He-DFT.
+ *
+ * This is the drop-in boundary.  The reference Fortran drivers call argument-less subroutines
+ * that work on module arrays (Dynamics_TDDFT/DFT4He3d.f90:566-576,677-697,709-715;
+ * He_statics/BCN4HeDFT.f90:1113-1160,1217).  Here the same state lives in device memory owned by
+ * an he_ctx_t; the caller uploads module arrays once (after readen/readenc), calls the
+ * replacement routines, and downloads at I/O points (printout/printoutc, energy prints).
+ *
+ * Conventions
+ *   - Every function returns 0 (HE_OK) on success; a non-zero status leaves a message in
+ *     he_last_error().  Nothing aborts the process.
+ *   - Host arrays use the reference's layout: Fortran column-major (nx,ny,nz), x fastest,
+ *     complex interleaved (re,im) binary64, half spectrum (nx/2+1,ny,nz), impurity arrays
+ *     (N_imp,3) column-major.  Host-side values are always binary64, whatever the device
+ *     precision.
+ *   - Work is queued on the context's CUDA stream; functions that return scalars through
+ *     pointers synchronise that stream, functions given NULL scalar pointers do not.
+ *   - A context is not thread-safe; use one context per host thread.
+ */
+#ifndef HE_DFT_H
+#define HE_DFT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HE_OK 0
+#define HE_ERR_ARG 1      /* invalid argument or size */
+#define HE_ERR_CUDA 2     /* CUDA runtime error (message has the CUDA error string) */
+#define HE_ERR_STATE 3    /* call not valid in this context mode / before set-up */
+#define HE_ERR_NOMEM 4    /* device allocation failed */
+
+typedef struct he_ctx he_ctx_t;
+
+enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1 };
+enum he_precision { HE_PREC_F64 = 0 };
+
+/* Grid: Dynamics_TDDFT/modules.f90:88-105 (grid), deriva npd/icon :31-37.  h = 2*xmax/n and
+ * x_i = -xmax + h*(i-1) (DFT4He3d.f90:265-329).  npd must be 13; icon 13 (zero padding), 8
+ * (periodic) or 18 (antiperiodic).  n must be a tstgrid size (tstgrid.f90:9-13). */
+typedef struct {
+  int nx, ny, nz;
+  double xmax, ymax, zmax;
+  int npd, icon;
+} he_grid_t;
+
+/* Orsay-Trento functional: he4 and lenard4 modules (Dynamics_TDDFT/modules.f90:133-153,
+ * :225-237).  core4 is the effective core after the driver's "If(Lsolid) core4='OT '" rule
+ * (DFT4He3d.f90:456): "OT ", "OP " or "OTC".  h4 is the core radius the driver selects
+ * (h4ot or h4op). */
+typedef struct {
+  char core4[4];
+  double h4, eps4, sigma4;
+  double cp4, cpp4, den4c, alphas, l, den0s, h2o2m4;
+  int lsolid;
+  double C, beta, den_m;
+} he_functional_t;
+
+/* Absorbing mask timec (DFT4He3d.f90:592-601): timec = (Lambdah*sum_axes(1+tanh((|x|-tmean)/
+ * tsurf)), 1).  The device evaluates it from these parameters instead of storing the array. */
+typedef struct {
+  double lambdah, txmean, txsurf, tymean, tysurf, tzmean, tzsurf;
+} he_absorber_t;
+
+/* Classical impurities (classicimp/interpol modules, modules.f90:303-343,386-399).  potion is the
+ * (N_imp, npot) table that potenimpini builds with Select_Pot (potenimpini.f90:31-59);
+ * npot = 100*max(n)+1, delinter = rmax/(npot-1), rmaxinterpol = 4*max(xmax).  ii_* is the
+ * impurity-impurity pair potential used by forceimp/energy: kind 0 = null, 1 = Morse
+ * D[(1-exp(-a(r-re)))^2-1] (r < ii_rcut gives ii_umax). */
+typedef struct {
+  int n_imp;
+  const double* m_imp_u; /* n_imp masses in u; m_imp = m_imp_u * mp_u (mp_u = 0.02061484) */
+  const double* potion;
+  int npot;
+  double delinter, rmaxinterpol;
+  int ii_kind;
+  double ii_D, ii_re, ii_a, ii_rcut, ii_umax;
+} he_impurities_t;
+
+/* energies module (Dynamics_TDDFT/modules.f90:39-51). */
+typedef struct {
+  double etot4, ekin4, elj4, ecor4, esolid, ealphas;
+  double ekinx, eHeX, eimpu_impu, eimpu, etot;
+} he_energies_t;
+
+/* Field identifiers for he_upload / he_download.  Sizes in binary64 words: N = nx*ny*nz,
+ * Nk = (nx/2+1)*ny*nz.  Complex fields count 2 words per point. */
+enum he_field {
+  HE_F_PSI = 0,      /* dynamics: complex N; statics: real N */
+  HE_F_DEN = 1,      /* real N */
+  HE_F_POT4 = 2,     /* real N */
+  HE_F_DENCG = 3,    /* real N */
+  HE_F_DELJ4 = 4,    /* real N */
+  HE_F_UIMP = 5,     /* real N (dynamics) */
+  HE_F_FDEN = 6,     /* complex Nk */
+  HE_F_PC = 7,       /* dynamics complex N; statics real N */
+  HE_F_Q = 8,        /* dynamics complex N; statics real N */
+  HE_F_PSIOLD1 = 9,  /* psiold(:,:,:,1..3), same type as psi */
+  HE_F_PSIOLD2 = 10,
+  HE_F_PSIOLD3 = 11,
+  HE_F_HPSIOLD1 = 12, /* hpsiold(:,:,:,1..2) */
+  HE_F_HPSIOLD2 = 13,
+  HE_F_DXDEN = 14,   /* real N, materialised by he_derden */
+  HE_F_DYDEN = 15,
+  HE_F_DZDEN = 16,
+  HE_F_HPSI = 17,    /* statics real N */
+  HE_F_FVLJ4 = 18,   /* real Nk */
+  HE_F_WCGK = 19,    /* real Nk */
+  HE_F_RIMP = 20,    /* (N_imp,3) */
+  HE_F_VIMP = 21,
+  HE_F_AIMP = 22,
+  HE_F_FIMP = 23,    /* F(N_imp,3) */
+  HE_F_RIMPOLD = 24, /* (N_imp,3,3) */
+  HE_F_VIMPOLD = 25, /* (N_imp,3,3) */
+  HE_F_AIMPOLD = 26, /* (N_imp,3,2) */
+  HE_F_PCR = 27,     /* (N_imp,3) */
+  HE_F_PCV = 28,
+  HE_F_QR = 29,
+  HE_F_QV = 30,
+  HE_F_RING = 31     /* 13 ints as doubles: ioldp(3), ioldh(2), ioldr(3), ioldv(3), iolda(2) */
+};
+
+/* Context life cycle.  Replaces the allocations of dimen.f90 and the plans of fftini
+ * (Dynamics_TDDFT/fft.f90:5-91).  mode: HE_MODE_DYNAMICS (complex psi, Dynamics_TDDFT) or
+ * HE_MODE_STATICS (real psi, He_statics).  All device memory is allocated here.  *out is set
+ * whenever it is non-NULL, also on failure (so he_last_error can be read); destroy it. */
+int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, int precision,
+                  he_ctx_t** out);
+void he_ctx_destroy(he_ctx_t* ctx);
+const char* he_last_error(const he_ctx_t* ctx);
+/* Number of kernel launches this context has issued (all of them hand-written CUDA). */
+long long he_launch_count(const he_ctx_t* ctx);
+/* Device bytes held by the context. */
+size_t he_device_bytes(const he_ctx_t* ctx);
+/* Use an external CUDA stream (cudaStream_t); NULL selects the context's own stream. */
+int he_set_stream(he_ctx_t* ctx, void* stream);
+int he_synchronize(he_ctx_t* ctx);
+
+/* k-space kernels.  he_set_kernels uploads host arrays computed by the reference's fforma/initcg
+ * (fforma.f90:11-61, initcg.f90:32-49); kalfs may be NULL unless core4 = "OTC".
+ * he_compute_kernels evaluates the same kernels on the device (fforma with its sine integral,
+ * initcg, kalfs = exp(-(pi l p)^2) from DFT4He3d.f90:527-531). */
+int he_set_kernels(he_ctx_t* ctx, const double* fvlj4, const double* wcgk, const double* kalfs);
+int he_compute_kernels(he_ctx_t* ctx);
+
+int he_set_absorber(he_ctx_t* ctx, const he_absorber_t* abs);
+int he_set_impurities(he_ctx_t* ctx, const he_impurities_t* imp);
+
+/* Module-array transfer.  bytes must equal the field's size (see enum he_field). */
+int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes);
+int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes);
+
+/* ---- Dynamics_TDDFT call surface ---- */
+/* poten(): Dynamics_TDDFT/poten.f90:131-218 (pot4, dencg, delj4, fden from den). */
+int he_poten(he_ctx_t* ctx);
+/* potenimp() -> updatepoten(): potenimp.f90:1-19,83-123 (uimp from rimp).  Asynchronous; an
+ * impurity outside the interpolation table raises the sticky lstopimp flag read by he_lstopimp. */
+int he_potenimp(he_ctx_t* ctx);
+/* lstopimp (interpol module, modules.f90:393): *flag = 1 once an impurity left the table
+ * (potenimp.f90:104-109); the driver exits its loop on it (DFT4He3d.f90:895).  Synchronises. */
+int he_lstopimp(he_ctx_t* ctx, int* flag);
+/* forceimp(): potenimp.f90:23-67 (F from grad(den) and the impurity fields).  F may be NULL. */
+int he_forceimp(he_ctx_t* ctx, double* F);
+/* aimp = F/m_imp, as the driver does after forceimp (DFT4He3d.f90:571-573, :694-696). */
+int he_set_accel(he_ctx_t* ctx);
+/* steprk(deltat): steprk.f90:1-144.  steppc(deltat,errHe,errimp,errvimp): steppc.f90:1-180.
+ * The error pointers may be NULL (no synchronisation). */
+int he_steprk(he_ctx_t* ctx, double deltat);
+int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, double* errvimp);
+/* energy(): Dynamics_TDDFT/energy.f90:107-178; statics He_statics/energy.f90:36-150. */
+int he_energy(he_ctx_t* ctx, he_energies_t* out);
+/* derden(): derden.f90:26-28, materialises dxden/dyden/dzden. */
+int he_derden(he_ctx_t* ctx);
+
+/* ---- He_statics call surface ---- */
+/* The driver's per-iteration refresh (BCN4HeDFT.f90:1131-1155): derden, fftfw(den,fden),
+ * dencg = fftbk(fden*wcgk), and delj4 = fftbk(fden*fvlj4) which the statics poten() recomputes
+ * from that same fden until the next refresh (He_statics/poten.f90:27-31). */
+int he_refresh_density(he_ctx_t* ctx);
+/* evolo(0,mu4,mu4err,n4) as called once before the loop (BCN4HeDFT.f90:1050, evolo.f90:41-93). */
+int he_evolo0(he_ctx_t* ctx, double* mu4, double* mu4err, int n4);
+/* steprkr / steppcr (He_statics/steprkr.f90:1-96, steppcr.f90:1-108). errpc may be NULL. */
+int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4);
+int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4, double* errpc);
+/* varmu(npart,mu,errmu): He_statics/varmu.f90:31. */
+int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HE_DFT_H */

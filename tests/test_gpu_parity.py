@@ -1,0 +1,176 @@
+"""Device path (libhedft.so through the C-ABI) against the CPU oracle, on identical seeded inputs.
+
+Tolerances: the FP64 device path must agree with the oracle to 1e-10 relative in E/N, mu and the
+rho L2 norm per step (and field-wise to 1e-10 of the field's max); single transforms and field
+evaluations agree to ~1e-12.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from he_dft_2024_b200 import config as C
+from he_dft_2024_b200.context import Context
+from he_dft_2024_b200 import driver as D
+
+pytestmark = pytest.mark.gpu
+
+RTOL_STEP = 1e-10
+
+
+def small_dyn(n=32, n_imp=1, **kw):
+    w = C.tddft_1000(n=n, **kw)
+    w = C.replace(w, xmax=20.0, ymax=20.0, zmax=20.0, n4=300, n_imp=n_imp,
+                  m_imp_u=(85.0,) * n_imp, rimp0=((0.5, -0.3, 8.0),) * n_imp,
+                  vimp0_aps=((0.0, 0.0, -3.0),) * n_imp, deltatps=5e-4)
+    return w
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def test_library_runs_on_device():
+    w = small_dyn(n=16, n_imp=0)
+    with Context(w) as ctx:
+        assert ctx.device_bytes > 0
+
+
+@pytest.mark.parametrize("n", [(32, 32, 32), (48, 40, 36), (64, 64, 64)])
+def test_kernels_match_oracle(n):
+    w = C.replace(small_dyn(n_imp=0), nx=n[0], ny=n[1], nz=n[2])
+    d = w.as_dict()
+    with Context(w) as ctx:
+        fv = ctx.download("fvlj4").ravel(order="F")
+        wc = ctx.download("wcgk").ravel(order="F")
+    o = O.Dynamics(d)
+    assert rel(fv, o.get("fvlj4")) < 1e-13
+    assert rel(wc, o.get("wcgk")) < 1e-14
+
+
+@pytest.mark.parametrize("n", [(32, 32, 32), (48, 40, 36), (64, 64, 64), (40, 30, 24)])
+@pytest.mark.parametrize("icon", [13, 8])
+def test_poten_matches_oracle(n, icon):
+    w = C.replace(small_dyn(n_imp=0), nx=n[0], ny=n[1], nz=n[2], icon=icon, noise=0.05)
+    den = C.woods_saxon(w)
+    o = O.Dynamics(w.as_dict())
+    o.set("den", den)
+    o.poten()
+    with Context(w) as ctx:
+        ctx.upload("den", den)
+        ctx.poten()
+        for name in ("dencg", "delj4", "pot4"):
+            assert rel(ctx.download(name).ravel(order="F"), o.get(name)) < 1e-12, name
+        assert rel(ctx.download("fden").ravel(order="F"), o.get("fden")) < 1e-12
+
+
+def run_dynamics(w, steps, side):
+    den0 = C.woods_saxon(w)
+    psi0 = D.initial_wavefunction(w, den0, kick=(0.0, 0.0, 0.05))
+    D.dynamics_setup(side, psi0, w.n_imp)
+    out = []
+    for it in range(1, steps + 1):
+        D.dynamics_iteration(side, it, w.deltat, w.n_imp)
+        e = side.energy()
+        if hasattr(side, "download"):
+            den = side.download("den").ravel(order="F")
+            psi = side.download("psi").ravel(order="F")
+            rimp = side.download("rimp").ravel(order="F") if w.n_imp else np.zeros(0)
+        else:
+            den, psi = side.get("den"), side.get("psi")
+            rimp = side.get("rimp") if w.n_imp else np.zeros(0)
+        out.append(dict(e=e, den=den, psi=psi, rimp=rimp))
+    return out
+
+
+@pytest.mark.parametrize("n_imp", [0, 1, 2])
+def test_dynamics_steps_match_oracle(n_imp):
+    w = small_dyn(n=32, n_imp=n_imp)
+    if n_imp == 2:
+        w = C.replace(w, rimp0=((0.5, -0.3, 8.0), (-2.0, 1.0, -7.0)),
+                      vimp0_aps=((0.0, 0.0, -3.0), (1.0, 0.0, 2.0)), ii_kind=1, ii_D=5.0,
+                      ii_re=4.0, ii_a=1.0)
+    steps = 8
+    o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u)
+    ref = run_dynamics(w, steps, o)
+    with Context(w) as ctx:
+        got = run_dynamics(w, steps, ctx)
+    for k, (g, r) in enumerate(zip(got, ref)):
+        en_g, en_r = g["e"]["etot"] / w.n4, r["e"]["etot"] / w.n4
+        assert abs(en_g - en_r) <= RTOL_STEP * abs(en_r), (k, en_g, en_r)
+        for key in ("ekin4", "elj4", "ecor4", "esolid", "eHeX"):
+            assert abs(g["e"][key] - r["e"][key]) <= 1e-10 * max(abs(r["e"][key]), 1e-8), (k, key)
+        l2g, l2r = np.linalg.norm(g["den"]), np.linalg.norm(r["den"])
+        assert abs(l2g - l2r) <= RTOL_STEP * l2r
+        assert rel(g["psi"], r["psi"]) < 1e-10
+        if n_imp:
+            np.testing.assert_allclose(g["rimp"], r["rimp"], rtol=1e-12, atol=1e-12)
+
+
+def test_steppc_errors_and_ring_match_oracle():
+    w = small_dyn(n=32, n_imp=1)
+    o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u)
+    den0 = C.woods_saxon(w)
+    psi0 = D.initial_wavefunction(w, den0)
+    with Context(w) as ctx:
+        for side in (o, ctx):
+            D.dynamics_setup(side, psi0, 1)
+            for it in range(1, 4):
+                D.dynamics_iteration(side, it, w.deltat, 1)
+        for it in range(4, 8):
+            eo = o.steppc(w.deltat)
+            eg = ctx.steppc(w.deltat)
+            np.testing.assert_allclose(eg, eo, rtol=1e-9, atol=1e-15)
+            for side in (o, ctx):
+                side.potenimp(); side.poten(); side.forceimp(); side.set_accel()
+        for s in (1, 2, 3):
+            assert rel(ctx.download(f"psiold{s}").ravel(order="F"), o.get(f"psiold{s}")) < 1e-10
+        for s in (1, 2):
+            assert rel(ctx.download(f"hpsiold{s}").ravel(order="F"), o.get(f"hpsiold{s}")) < 1e-10
+        assert rel(ctx.download("pc").ravel(order="F"), o.get("pc")) < 1e-10
+        assert rel(ctx.download("q").ravel(order="F"), o.get("q")) < 1e-10
+        for name in ("vimp", "aimp", "F"):
+            np.testing.assert_allclose(ctx.download(name).ravel(order="F"), o.get(name),
+                                       rtol=1e-10, atol=1e-14)
+
+
+def test_short_axis_and_periodic_dynamics():
+    w = C.replace(small_dyn(n=32, n_imp=1), nz=12, zmax=6.0, icon=8,
+                  rimp0=((0.5, -0.3, 1.0),), vimp0_aps=((0.0, 0.0, 0.0),))
+    o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u)
+    ref = run_dynamics(w, 5, o)
+    with Context(w) as ctx:
+        got = run_dynamics(w, 5, ctx)
+    for g, r in zip(got, ref):
+        assert rel(g["psi"], r["psi"]) < 1e-10
+
+
+def run_statics(w, iters, side):
+    den0 = C.woods_saxon(w)
+    mu = D.statics_setup(side, den0, w.n4)
+    out = []
+    for it in range(1, iters + 1):
+        mu, err = D.statics_iteration(side, it, w.deltat_statics, mu, w.n4)
+        e = side.energy()
+        if hasattr(side, "download"):
+            den = side.download("den").ravel(order="F")
+            vm = side.varmu(w.n4, mu)
+        else:
+            den = side.get("den")
+            vm = side.varmu(w.n4, mu)
+        out.append(dict(mu=mu, err=err, e=e, den=den, varmu=vm))
+    return out
+
+
+@pytest.mark.parametrize("n", [32, 40])
+def test_statics_iterations_match_oracle(n):
+    w = C.replace(C.statics_500(), nx=n, ny=n, nz=n, xmax=0.35 * n, ymax=0.35 * n, zmax=0.35 * n)
+    o = O.Statics(w.as_dict())
+    ref = run_statics(w, 8, o)
+    with Context(w, mode="statics") as ctx:
+        got = run_statics(w, 8, ctx)
+    for k, (g, r) in enumerate(zip(got, ref)):
+        assert abs(g["mu"] - r["mu"]) <= RTOL_STEP * abs(r["mu"]), (k, g["mu"], r["mu"])
+        assert abs(g["e"]["etot"] - r["e"]["etot"]) <= RTOL_STEP * abs(r["e"]["etot"])
+        l2g, l2r = np.linalg.norm(g["den"]), np.linalg.norm(r["den"])
+        assert abs(l2g - l2r) <= RTOL_STEP * l2r
+        assert abs(g["varmu"] - r["varmu"]) <= 1e-8 * abs(r["varmu"])
