@@ -1,0 +1,394 @@
+"""Benchmark: real-time TDDFT grid-point-steps per second on the 128^3 classical-impurity workload.
+
+Workload (one "step" = one iteration of the Dynamics_TDDFT time loop body, DFT4He3d.f90:677-697:
+steppc (Hamming predictor-modifier-corrector with its inner potenimp/poten/forceimp) followed by
+potenimp, poten, forceimp and aimp = F/m): 4He_1000 on a 128^3 grid (h = 0.625 A, box +-40 A),
+one 85 u classical impurity with the capped Morse He-X potential, dt = 0.1 fs, binary64.  The
+droplet is a seeded synthetic Woods-Saxon profile (no reference data ships); the first three
+iterations (RK-Gill start) run before the timed region, as in the reference driver.
+
+value     device time (CUDA events on the context's stream) for K steps with all state resident
+          in HBM; the per-step working set (~0.45 GB) exceeds L2 (126 MB).
+e2e       the same K steps through the C-ABI the way the Fortran driver calls it every iteration:
+          steppc returning errHe/errimp/errvimp to the host, forceimp returning F to the host,
+          aimp = F/m computed on the host and uploaded, rimp/vimp read back for the per-step
+          output files (DFT4He3d.f90:677-707).
+roofline  the kernel with the largest share of device time, its algorithmic bytes per launch
+          (every input field read once, every output written once) over its mean CUDA-event time.
+cpu_baseline  the CPU oracle (C++ restatement, OpenMP on all host cores) on the identical
+          128^3 state copied from the device, a bounded sample of driver iterations.
+
+--impl reference times that CPU oracle alone on the same workload (the reference Fortran cannot be
+built in this image: no Fortran compiler, no FFTW).  Multi-GPU (torchrun): independent replicas,
+one trajectory per GPU, no collective on the data path; value = all ranks' grid-pt-steps over the
+max-over-ranks device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TDDFT grid-pt-steps/s (FP64, 128^3 classical-impurity steppc loop)"
+UNIT = "grid-pt-steps/s"
+
+# Algorithmic bytes per grid point of each kernel (binary64; N-sized field = 8 B real / 16 B
+# complex per point, half spectrum = (nx/2+1)/nx of that): reads + writes of the arrays the
+# kernel's reference counterpart consumes and produces.
+def kernel_bytes_per_point(nx):
+    hk = (nx // 2 + 1) / nx  # half-spectrum fraction
+    c, r = 16.0, 8.0
+    return {
+        # psi, pot4, uimp, psiold(ioldp3), hpsiold x2, pc -> psi_new, pc, hpsiold, den
+        "hpsi_pmc_predict": (c + r + r + c + 2 * c + c) + (c + c + c + r),
+        # psi, pot4, uimp, psiold x2, hpsiold x2, pc -> psi_new, pc, den
+        "hpsi_pmc_correct": (c + r + r + 2 * c + 2 * c + c) + (c + c + r),
+        # psi, pot4, uimp, q -> q, psi_new, den (+ hpsiold on stage 1)
+        "hpsi_rkgill_stage": (c + r + r + c) + (c + c + r),
+        # den -> uimp (+ force sums)
+        "impurity_field_force": r + r,
+        # psi, den, dencg, delj4, uimp -> sums
+        "energy_reduce": c + 4 * r,
+        "fft_x_r2c_den": r + c * hk,
+        "fft_x_r2c_corr": 2 * r + c * hk,
+        "fft_x_c2r_cg_lj": 2 * c * hk + 2 * r,
+        "fft_x_c2r_cg_lj_r2c_corr": 2 * c * hk + r + 2 * r + c * hk,
+        "fft_x_c2r_pot4": c * hk + 3 * r + r,
+        "fft_y": 2 * c * hk,
+        "fft_z_conv1": 2 * c * hk + r * hk,
+        "fft_z_conv2": c * hk + 3 * c * hk + 2 * r * hk,
+    }
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"he_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reduce_max(t, ws):
+    if ws == 1:
+        return t
+    import torch
+    import torch.distributed as dist
+    x = torch.tensor([t], dtype=torch.float64, device="cuda")
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_workload(args):
+    from he_dft_2024_b200 import config as C
+    return C.tddft_1000(n=args.n)
+
+
+def prepare_state(ctx, w):
+    """Set-up and RK-Gill start (iterations 1-3) of the driver."""
+    from he_dft_2024_b200 import config as C, driver as D
+    den0 = C.woods_saxon(w)
+    psi0 = D.initial_wavefunction(w, den0)
+    D.dynamics_setup(ctx, psi0, w.n_imp)
+    for it in range(1, 4):
+        D.dynamics_iteration(ctx, it, w.deltat, w.n_imp)
+
+
+def device_iteration(ctx, w, it):
+    from he_dft_2024_b200 import driver as D
+    D.dynamics_iteration(ctx, it, w.deltat, w.n_imp)
+
+
+def e2e_iteration(ctx, w, mass):
+    """One loop iteration as the Fortran driver issues it through the C-ABI."""
+    errs = ctx.steppc(w.deltat, errors=True)                 # D2H errHe, errimp, errvimp
+    ctx.potenimp()
+    ctx.poten()
+    F = ctx.forceimp(want=True)                              # D2H F(N_imp,3)
+    aimp = F / mass[:, None]                                 # host: aimp = F/m_imp
+    ctx.upload("aimp", aimp)                                 # H2D aimp
+    r = ctx.download("rimp")                                 # D2H for the rimp/vimp files
+    v = ctx.download("vimp")
+    return errs, r, v
+
+
+STATE_FIELDS = ("psi", "den", "pot4", "dencg", "delj4", "uimp", "pc", "q", "psiold1",
+                "psiold2", "psiold3", "hpsiold1", "hpsiold2", "fden")
+IMP_FIELDS = ("rimp", "vimp", "aimp", "F", "rimpold", "vimpold", "aimpold", "pcr", "pcv", "qr",
+              "qv")
+
+
+def copy_state_to_oracle(ctx, w, threads):
+    """Oracle holding the device's complete time-stepping state (fields, history, ring)."""
+    from oracle import oracle as O
+    o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u, nthreads=threads)
+    for name in STATE_FIELDS + (IMP_FIELDS if w.n_imp else ()):
+        o.set(name, ctx.download(name))
+    o.ring([int(v) for v in ctx.download("ring")])
+    return o
+
+
+def cpu_sample(ctx, w, iters, threads):
+    """Time `iters` driver iterations of the CPU oracle started from the device state, then run
+    the same iterations on the device and compare psi (a full-size parity spot check)."""
+    from he_dft_2024_b200 import driver as D
+    o = copy_state_to_oracle(ctx, w, threads)
+    t0 = time.perf_counter()
+    for k in range(iters):
+        D.dynamics_iteration(o, 4 + k, w.deltat, w.n_imp)
+    dt = time.perf_counter() - t0
+    for k in range(iters):
+        D.dynamics_iteration(ctx, 4 + k, w.deltat, w.n_imp)
+    pg = ctx.download("psi").ravel(order="F")
+    po = o.get("psi")
+    diff = float(np.max(np.abs(pg - po)) / np.max(np.abs(po)))
+    return dt, diff
+
+
+def run_ours(args):
+    import torch
+    from he_dft_2024_b200.context import Context
+    from he_dft_2024_b200.config import MP_U
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = build_workload(args)
+    N = w.n
+    ctx = Context(w)
+    # A dedicated (non-default) stream: the library's kernels and the timing events share it.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    prepare_state(ctx, w)
+    it = 4
+    for _ in range(args.warmup):
+        device_iteration(ctx, w, it)
+        it += 1
+    ctx.synchronize()
+
+    # ---- value: device-resident loop, CUDA events on the context's (torch's current) stream ----
+    launches0 = ctx.launches
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            device_iteration(ctx, w, it)
+            it += 1
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launches - launches0
+    t_max = reduce_max(ms / 1e3, ws)
+    value = N * args.steps * ws / t_max
+
+    # ---- e2e: the driver's host-facing calls every iteration ----
+    mass = np.asarray(w.m_imp_u, np.float64) * MP_U
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_iteration(ctx, w, mass)
+        it += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = reduce_max(e0.elapsed_time(e1) / 1e3, ws)
+    wall_e2e = time.perf_counter() - t0
+    e2e_value = N * args.steps * ws / e2e_s
+
+    # ---- per-kernel breakdown (separate short run with event timing) ----
+    ctx.timing(True)
+    for _ in range(max(3, min(args.steps, 10))):
+        device_iteration(ctx, w, it)
+        it += 1
+    rep = ctx.timing_report()
+    ctx.timing(False)
+    tot = sum(v[1] for v in rep.values())
+    bpp = kernel_bytes_per_point(w.nx)
+    top = max(rep.items(), key=lambda kv: kv[1][1])
+    name, (nl, kms) = top
+    peak, peak_kind = measured_peak()
+    alg = bpp.get(name, 0.0) * N
+    achieved = alg / (kms / nl / 1e3) / 1e9 if nl else 0.0
+    breakdown = {k: {"launches": v[0], "ms_per_launch": v[1] / v[0], "share": v[1] / tot,
+                     "GB/s": (bpp.get(k, 0.0) * N / (v[1] / v[0] / 1e3) / 1e9) if k in bpp else None}
+                 for k, v in sorted(rep.items(), key=lambda kv: -kv[1][1])}
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(name)
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "h_A": w.h[0], "n4": w.n4,
+                   "n_imp": w.n_imp, "deltat_ps": w.deltatps, "parallelism": f"replicas{ws}",
+                   "l2": "per-step working set 0.45 GB > 126 MB L2 (no flush)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * 3 * w.n_imp,
+                "d2h_bytes_per_step": 8 * (3 + 3 * w.n_imp * 3), "wall_s": wall_e2e},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "ms_per_launch": kms / nl},
+        "step_alg_bytes_per_point": 744.0,
+        "step_roofline_frac": (744.0 * N * args.steps / (t_max / ws)) / 1e9 / peak,
+        "kernels": breakdown,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        iters = args.cpu_iters
+        secs, diff = cpu_sample(ctx, w, iters, threads)
+        line["cpu_baseline"] = {"value": N * iters / secs, "unit": UNIT, "cores": threads,
+                                "kind": "port",
+                                "sample": f"{iters} driver iterations (steppc + field) of the "
+                                          f"{w.nx}^3 workload from the device state, "
+                                          f"{secs:.1f} s"}
+        line["parity_full_size"] = {"max_rel_psi_diff": diff, "iterations": iters,
+                                    "note": "device vs oracle from the identical 128^3 state"}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from he_dft_2024_b200 import config as C, driver as D
+    w = build_workload(args)
+    threads = os.cpu_count() or 1
+    o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u, nthreads=threads)
+    den0 = C.woods_saxon(w)
+    psi0 = D.initial_wavefunction(w, den0)
+    D.dynamics_setup(o, psi0, w.n_imp)
+    for it in range(1, 4):
+        D.dynamics_iteration(o, it, w.deltat, w.n_imp)
+    it = 4
+    for _ in range(args.warmup):
+        D.dynamics_iteration(o, it, w.deltat, w.n_imp)
+        it += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        D.dynamics_iteration(o, it, w.deltat, w.n_imp)
+        it += 1
+    secs = time.perf_counter() - t0
+    v = w.n * args.steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "n4": w.n4, "n_imp": w.n_imp,
+                   "deltat_ps": w.deltatps, "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} driver iterations of the {w.nx}^3 workload "
+                                   f"after the 3-iteration RK start and {args.warmup} warm-up "
+                                   "iterations (C++ restatement of the reference; the Fortran "
+                                   "reference cannot be built in this image)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--cpu-iters", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -62,6 +62,11 @@ class HeEnergies(ctypes.Structure):
                  "eimpu_impu", "eimpu", "etot")]
 
 
+class HeKernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 40), ("launches", ctypes.c_longlong),
+                ("ms", ctypes.c_double)]
+
+
 class HeError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"he_dft status {status}: {msg}")
@@ -118,6 +123,8 @@ def load():
         "he_steprkr": (ip, [vp, d, dp, dp, ip]),
         "he_steppcr": (ip, [vp, d, dp, dp, ip, dp]),
         "he_varmu": (ip, [vp, ip, d, dp]),
+        "he_timing": (ip, [vp, ip]),
+        "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

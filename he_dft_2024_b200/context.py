@@ -73,6 +73,17 @@ class Context:
     def device_bytes(self):
         return int(self.L.he_device_bytes(self.h))
 
+    def timing(self, enable=True):
+        self._ck(self.L.he_timing(self.h, 1 if enable else 0))
+
+    def timing_report(self):
+        """{kernel name: (launches, total ms)} of the launches recorded since timing(True)."""
+        buf = (_lib.HeKernelTime * 64)()
+        n = ctypes.c_int(0)
+        self._ck(self.L.he_timing_report(self.h, buf, 64, ctypes.byref(n)))
+        return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].ms))
+                for i in range(min(n.value, 64))}
+
     def synchronize(self):
         self._ck(self.L.he_synchronize(self.h))
 

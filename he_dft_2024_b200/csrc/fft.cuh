@@ -10,8 +10,14 @@
 // consecutive kx staged in shared memory).  The k-space kernel multiply is fused into the z pass
 // (forward z, multiply, inverse z), and the pointwise prologue/epilogue of poten is fused into
 // the x passes.  Lines are transformed by a mixed-radix (8,4,2,3,5) Stockham autosort in shared
-// memory (ping-pong buffers), twiddles from a per-length table built on the host in extended
-// precision.
+// memory (ping-pong buffers).
+//
+// Two instantiations of the line transform: for the common lengths the length N is a template
+// parameter, so the per-butterfly index arithmetic uses constant divisors, the stages unroll,
+// each stage reads its own twiddle table laid out [r-1][k] (consecutive threads read consecutive
+// twiddles), and line storage is swizzled (element i lives at i ^ ((i>>3)&7)) so that both the
+// strided and the contiguous side of every stage hit distinct shared-memory banks.  Other
+// admissible lengths use the same algorithm with run-time sizes.
 #pragma once
 #include "common.cuh"
 
@@ -24,7 +30,41 @@ struct LinePlan {
   int nst;               // number of radix stages
   int rad[kMaxStages];   // radix of each stage
   const double2* tw;     // device table exp(-2 pi i m / n), m = 0..n-1
+  const double2* stw;    // per-stage twiddles [stage][r-1][k], k < ns(stage)
+  int stw_len;           // entries in stw
 };
+
+// Greedy radix choice shared by host and device: 8, then 4, 2, 3, 5.
+HE_HD constexpr int radix_of(int m) {
+  return (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : 1;
+}
+HE_HD constexpr int radix_at(int n, int s) {
+  int m = n;
+  for (int st = 0; st < s; ++st) m /= radix_of(m);
+  return radix_of(m);
+}
+HE_HD constexpr int num_stages(int n) {
+  int m = n, s = 0;
+  while (m > 1 && radix_of(m) > 1) { m /= radix_of(m); ++s; }
+  return s;
+}
+// Offset of stage s's twiddles in the per-stage table: sum over earlier stages of (R-1)*ns.
+HE_HD constexpr int stw_offset(int n, int s) {
+  int off = 0, ns = 1, m = n;
+  for (int st = 0; st < s; ++st) {
+    const int R = radix_of(m);
+    off += (R - 1) * ns;
+    ns *= R;
+    m /= R;
+  }
+  return off;
+}
+// Line storage swizzle (identity unless N is a multiple of 8).
+template <int N>
+HE_HD constexpr int sw(int i) {
+  if constexpr (N > 0 && N % 8 == 0) return i ^ ((i >> 3) & 7);
+  else return i;
+}
 
 // Radix-R DFT in registers; inv selects exp(+i).
 template <int R>
@@ -102,13 +142,50 @@ HE_D void dft<5>(double2* v, bool inv) {
   v[3] = csub(a2, ib2);
 }
 
-// One Stockham stage of radix R over 'nlines' lines (line stride ls) from src to dst.
+// ---- compile-time length ------------------------------------------------------------------------
+template <int N, int R, int NS>
+HE_D void stage_t(const double2* __restrict__ src, double2* __restrict__ dst, int nlines, int ls,
+                  const double2* __restrict__ stw, bool inv, int tid, int nthr) {
+  constexpr int NR = N / R;
+  const int total = nlines * NR;
+  for (int w = tid; w < total; w += nthr) {
+    const int line = w / NR;
+    const int j = w - line * NR;
+    const int k = j % NS;
+    const double2* s = src + line * ls;
+    double2* d = dst + line * ls;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const double2 x = s[sw<N>(j + r * NR)];
+      if constexpr (NS == 1) v[r] = x;
+      else v[r] = (r == 0) ? x : cmul_conj_if(x, stw[(r - 1) * NS + k], inv);
+    }
+    dft<R>(v, inv);
+    const int base = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) d[sw<N>(base + r * NS)] = v[r];
+  }
+}
+
+template <int N, int S, int NS>
+HE_D double2* stages_t(double2* src, double2* dst, int nlines, int ls, const double2* stw,
+                       bool inv, int tid, int nthr) {
+  if constexpr (S >= num_stages(N)) {
+    return src;
+  } else {
+    constexpr int R = radix_at(N, S);
+    stage_t<N, R, NS>(src, dst, nlines, ls, stw + stw_offset(N, S), inv, tid, nthr);
+    __syncthreads();
+    return stages_t<N, S + 1, NS * R>(dst, src, nlines, ls, stw, inv, tid, nthr);
+  }
+}
+
+// ---- run-time length ------------------------------------------------------------------------------
 template <int R>
-HE_D void stockham_stage(const double2* __restrict__ src, double2* __restrict__ dst, int nlines,
-                         int ls, int n, int ns, const double2* __restrict__ tw, bool inv,
-                         int tid, int nthr) {
+HE_D void stage_rt(const double2* __restrict__ src, double2* __restrict__ dst, int nlines, int ls,
+                   int n, int ns, const double2* __restrict__ stw, bool inv, int tid, int nthr) {
   const int nr = n / R;
-  const int twstep = n / (ns * R);
   const int total = nlines * nr;
   for (int w = tid; w < total; w += nthr) {
     const int line = w / nr;
@@ -119,8 +196,8 @@ HE_D void stockham_stage(const double2* __restrict__ src, double2* __restrict__ 
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      double2 x = s[j + r * nr];
-      v[r] = (r == 0) ? x : cmul_conj_if(x, tw[r * k * twstep], inv);
+      const double2 x = s[j + r * nr];
+      v[r] = (r == 0 || ns == 1) ? x : cmul_conj_if(x, stw[(r - 1) * ns + k], inv);
     }
     dft<R>(v, inv);
     const int base = (j / ns) * ns * R + k;
@@ -129,37 +206,44 @@ HE_D void stockham_stage(const double2* __restrict__ src, double2* __restrict__ 
   }
 }
 
-// Transform 'nlines' lines held in buffer a (b is scratch of the same size).  Returns the buffer
-// holding the result.  Ends with __syncthreads().
+// Transform 'nlines' lines held in buffer a (b is scratch of the same size); N = 0 selects the
+// run-time length pl.n.  Returns the buffer holding the result; ends with __syncthreads().
+template <int N>
 HE_D double2* fft_lines(double2* a, double2* b, int nlines, int ls, const LinePlan& pl,
-                        const double2* tw_smem, bool inv) {
+                        const double2* stw_smem, bool inv) {
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthr = blockDim.x * blockDim.y;
-  double2* src = a;
-  double2* dst = b;
-  int ns = 1;
-  for (int s = 0; s < pl.nst; ++s) {
-    const int R = pl.rad[s];
-    switch (R) {
-      case 8: stockham_stage<8>(src, dst, nlines, ls, pl.n, ns, tw_smem, inv, tid, nthr); break;
-      case 4: stockham_stage<4>(src, dst, nlines, ls, pl.n, ns, tw_smem, inv, tid, nthr); break;
-      case 2: stockham_stage<2>(src, dst, nlines, ls, pl.n, ns, tw_smem, inv, tid, nthr); break;
-      case 3: stockham_stage<3>(src, dst, nlines, ls, pl.n, ns, tw_smem, inv, tid, nthr); break;
-      default: stockham_stage<5>(src, dst, nlines, ls, pl.n, ns, tw_smem, inv, tid, nthr); break;
+  if constexpr (N > 0) {
+    return stages_t<N, 0, 1>(a, b, nlines, ls, stw_smem, inv, tid, nthr);
+  } else {
+    double2* src = a;
+    double2* dst = b;
+    int ns = 1, off = 0;
+    for (int s = 0; s < pl.nst; ++s) {
+      const int R = pl.rad[s];
+      const double2* st = stw_smem + off;
+      switch (R) {
+        case 8: stage_rt<8>(src, dst, nlines, ls, pl.n, ns, st, inv, tid, nthr); break;
+        case 4: stage_rt<4>(src, dst, nlines, ls, pl.n, ns, st, inv, tid, nthr); break;
+        case 2: stage_rt<2>(src, dst, nlines, ls, pl.n, ns, st, inv, tid, nthr); break;
+        case 3: stage_rt<3>(src, dst, nlines, ls, pl.n, ns, st, inv, tid, nthr); break;
+        default: stage_rt<5>(src, dst, nlines, ls, pl.n, ns, st, inv, tid, nthr); break;
+      }
+      __syncthreads();
+      off += (R - 1) * ns;
+      ns *= R;
+      double2* t = src;
+      src = dst;
+      dst = t;
     }
-    __syncthreads();
-    ns *= R;
-    double2* t = src;
-    src = dst;
-    dst = t;
+    return src;
   }
-  return src;
 }
 
-HE_D void load_twiddles(double2* tw_smem, const LinePlan& pl) {
+HE_D void load_twiddles(double2* stw_smem, const LinePlan& pl) {
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthr = blockDim.x * blockDim.y;
-  for (int m = tid; m < pl.n; m += nthr) tw_smem[m] = pl.tw[m];
+  for (int m = tid; m < pl.stw_len; m += nthr) stw_smem[m] = pl.stw[m];
 }
 
 }  // namespace he

@@ -13,15 +13,23 @@
 //     X_C2R2_CORR  the same, then the R2C of the correlation source into A         (:166-171)
 //     X_C2R_POT    sto1 = C2R(A)*renor, penalty, pot4 assembly                     (:178-218)
 // y/z pass (k_ypass, k_zconv): CTA = TKX consecutive kx of one pencil family, staged transposed
-//   in shared memory (line stride n+1 to spread banks).  The z pass does forward z, the k-space
+//   in shared memory (odd line stride to spread banks).  The z pass does forward z, the k-space
 //   multiply by one or two real kernels (wcgk, fvlj4), and the inverse z, and can store the
 //   forward spectrum (fden) on the way.
+// Every kernel is instantiated for a compile-time line length N (the common grid sizes) and for
+// N = 0 (run-time length, other admissible sizes).
 #pragma once
 #include "fft.cuh"
 
 namespace he {
 
 enum XMode { X_R2C_DEN = 0, X_R2C_CORR = 1, X_C2R2 = 2, X_C2R2_CORR = 3, X_C2R_POT = 4 };
+
+// Rows per x-pass CTA and kx columns per y/z-pass CTA (host and device agree on these).
+HE_HD constexpr int tile_rows(int n) { return n <= 256 ? 16 : 8; }
+// Line stride in shared memory: the line length rounded up to a multiple of 8, plus one (odd, so
+// the transposing gathers of consecutive lines spread over the banks).
+HE_HD constexpr int line_stride(int n) { return ((n + 7) / 8) * 8 + 1; }
 
 struct XArgs {
   int nx, nxh;
@@ -56,93 +64,92 @@ HE_D double2 packed_c2r(const double2* ra, const double2* rb, int k, int n) {
   return make_double2(a.x + b.y, -a.y + b.x);
 }
 
-template <int MODE>
+// Split a transformed packed line into the half spectra of its real and imaginary rows.
+template <int N>
+HE_D double2 split_r2c(const double2* L, int k, int n, bool second) {
+  const double2 z = L[sw<N>(k)];
+  const double2 zc = cconj(L[sw<N>((n - k) % n)]);
+  if (!second) return make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
+  return make_double2(0.5 * (z.y - zc.y), -0.5 * (z.x - zc.x));
+}
+
+template <int MODE, int N>
 __global__ void __launch_bounds__(256) k_xpass(const XArgs a) {
   extern __shared__ double2 smem[];
-  const int n = a.nx, nxh = a.nxh, ls = n + 1;
+  const int n = (N > 0) ? N : a.nx;
+  const int nxh = n / 2 + 1;
+  const int ls = line_stride(n);
+  const int RB = (N > 0) ? tile_rows(N) : a.rb;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const long r0 = (long)blockIdx.x * a.rb;
-  const int rb = (int)min((long)a.rb, a.rows - r0);  // even by construction
+  const long r0 = (long)blockIdx.x * RB;
   double2* tw = smem;
-  double2* P0 = smem + n;
-  double2* P1 = P0 + a.rb * ls;
+  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  double2* P1 = P0 + RB * ls;
   load_twiddles(tw, a.pl);
 
   if constexpr (MODE == X_R2C_DEN || MODE == X_R2C_CORR) {
-    for (int e = tid; e < rb * n; e += nthr) {
+    const long g0 = r0 * n;
+    for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
-      const long g = (r0 + row) * n + x;
-      double v = a.den[g];
-      if constexpr (MODE == X_R2C_CORR) v = corr_source(v, a.dencg_in[g], a.cp4, a.cpp4);
-      reinterpret_cast<double*>(&P0[(row >> 1) * ls + x])[row & 1] = v;
+      double v = a.den[g0 + e];
+      if constexpr (MODE == X_R2C_CORR) v = corr_source(v, a.dencg_in[g0 + e], a.cp4, a.cpp4);
+      reinterpret_cast<double*>(&P0[(row >> 1) * ls + sw<N>(x)])[row & 1] = v;
     }
     __syncthreads();
-    double2* R = fft_lines(P0, P1, rb / 2, ls, a.pl, tw, false);
-    for (int e = tid; e < rb * nxh; e += nthr) {
+    double2* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, false);
+    for (int e = tid; e < RB * nxh; e += nthr) {
       const int row = e / nxh, k = e - row * nxh;
-      const double2* L = R + (row >> 1) * ls;
-      const double2 z = L[k];
-      const double2 zc = cconj(L[(n - k) % n]);
-      double2 o;
-      if ((row & 1) == 0) o = make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
-      else o = make_double2(0.5 * (z.y - zc.y), -0.5 * (z.x - zc.x));
-      a.specA[(r0 + row) * nxh + k] = o;
+      a.specA[(r0 + row) * nxh + k] = split_r2c<N>(R + (row >> 1) * ls, k, n, row & 1);
     }
     return;
   }
 
   if constexpr (MODE == X_C2R2 || MODE == X_C2R2_CORR) {
-    for (int e = tid; e < rb * n; e += nthr) {
+    for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, k = e - row * n;
       const double2* ra = a.specA + (r0 + row) * nxh;
       const double2* rbp = a.specB + (r0 + row) * nxh;
-      P0[row * ls + k] = packed_c2r(ra, rbp, k, n);
+      P0[row * ls + sw<N>(k)] = packed_c2r(ra, rbp, k, n);
     }
     __syncthreads();
-    double2* R = fft_lines(P0, P1, rb, ls, a.pl, tw, true);
+    double2* R = fft_lines<N>(P0, P1, RB, ls, a.pl, tw, true);
     double2* O = (R == P0) ? P1 : P0;
-    for (int e = tid; e < rb * n; e += nthr) {
+    for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
       const long g = (r0 + row) * n + x;
-      const double2 z = R[row * ls + x];
+      const double2 z = R[row * ls + sw<N>(x)];
       const double dcg = z.x * a.renor;
       a.out1[g] = dcg;
       a.out2[g] = z.y * a.renor;
       if constexpr (MODE == X_C2R2_CORR)
-        reinterpret_cast<double*>(&O[(row >> 1) * ls + x])[row & 1] =
+        reinterpret_cast<double*>(&O[(row >> 1) * ls + sw<N>(x)])[row & 1] =
             corr_source(a.den[g], dcg, a.cp4, a.cpp4);
     }
     if constexpr (MODE == X_C2R2) return;
     __syncthreads();
     double2* S = (O == P0) ? P1 : P0;
-    double2* R2 = fft_lines(O, S, rb / 2, ls, a.pl, tw, false);
-    for (int e = tid; e < rb * nxh; e += nthr) {
+    double2* R2 = fft_lines<N>(O, S, RB / 2, ls, a.pl, tw, false);
+    for (int e = tid; e < RB * nxh; e += nthr) {
       const int row = e / nxh, k = e - row * nxh;
-      const double2* L = R2 + (row >> 1) * ls;
-      const double2 z = L[k];
-      const double2 zc = cconj(L[(n - k) % n]);
-      double2 o;
-      if ((row & 1) == 0) o = make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
-      else o = make_double2(0.5 * (z.y - zc.y), -0.5 * (z.x - zc.x));
-      a.specA[(r0 + row) * nxh + k] = o;
+      a.specA[(r0 + row) * nxh + k] = split_r2c<N>(R2 + (row >> 1) * ls, k, n, row & 1);
     }
     return;
   }
 
   if constexpr (MODE == X_C2R_POT) {
-    // X_C2R_POT: rows 2p and 2p+1 share complex line p.
-    for (int e = tid; e < (rb / 2) * n; e += nthr) {
+    // rows 2p and 2p+1 share complex line p
+    for (int e = tid; e < (RB / 2) * n; e += nthr) {
       const int p = e / n, k = e - p * n;
       const double2* ra = a.specA + (r0 + 2 * p) * nxh;
       const double2* rbp = a.specA + (r0 + 2 * p + 1) * nxh;
-      P0[p * ls + k] = packed_c2r(ra, rbp, k, n);
+      P0[p * ls + sw<N>(k)] = packed_c2r(ra, rbp, k, n);
     }
     __syncthreads();
-    double2* R = fft_lines(P0, P1, rb / 2, ls, a.pl, tw, true);
-    for (int e = tid; e < rb * n; e += nthr) {
+    double2* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, true);
+    for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
       const long g = (r0 + row) * n + x;
-      const double2 z = R[(row >> 1) * ls + x];
+      const double2 z = R[(row >> 1) * ls + sw<N>(x)];
       const double sto1 = ((row & 1) ? z.y : z.x) * a.renor;
       const double dc = a.dencg_in[g];
       double pot = a.delj4_in[g] + dc * dc * (a.a0 + a.a1 * dc) + sto1;
@@ -170,86 +177,95 @@ struct YZArgs {
   const double* k2;          // null: single kernel
 };
 
+template <int N>
 __global__ void __launch_bounds__(256) k_ypass(const YZArgs a) {
   extern __shared__ double2 smem[];
-  const int n = a.ny, ls = n + 1, tkx = a.tkx, nxh = a.nxh;
+  const int n = (N > 0) ? N : a.ny;
+  const int ls = line_stride(n);
+  const int TK = (N > 0) ? tile_rows(N) : a.tkx;
+  const int nxh = a.nxh;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int kx0 = blockIdx.x * tkx;
+  const int kx0 = blockIdx.x * TK;
   const int z = blockIdx.y;
   double2* arr = a.arr[blockIdx.z];
   double2* tw = smem;
-  double2* P0 = smem + n;
-  double2* P1 = P0 + tkx * ls;
+  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  double2* P1 = P0 + TK * ls;
   load_twiddles(tw, a.pl);
   const long base = (long)nxh * n * z;
-  for (int e = tid; e < tkx * n; e += nthr) {
-    const int j = e / tkx, c = e - j * tkx;
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    P0[c * ls + j] = (kx < nxh) ? arr[base + kx + (long)nxh * j] : make_double2(0.0, 0.0);
+    P0[c * ls + sw<N>(j)] = (kx < nxh) ? arr[base + kx + (long)nxh * j] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  double2* R = fft_lines(P0, P1, tkx, ls, a.pl, tw, a.inv);
-  for (int e = tid; e < tkx * n; e += nthr) {
-    const int j = e / tkx, c = e - j * tkx;
+  double2* R = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, a.inv);
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) arr[base + kx + (long)nxh * j] = R[c * ls + j];
+    if (kx < nxh) arr[base + kx + (long)nxh * j] = R[c * ls + sw<N>(j)];
   }
 }
 
+template <int N>
 __global__ void __launch_bounds__(256) k_zconv(const YZArgs a) {
   extern __shared__ double2 smem[];
-  const int n = a.nz, ls = n + 1, tkx = a.tkx, nxh = a.nxh;
+  const int n = (N > 0) ? N : a.nz;
+  const int ls = line_stride(n);
+  const int TK = (N > 0) ? tile_rows(N) : a.tkx;
+  const int nxh = a.nxh;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int kx0 = blockIdx.x * tkx;
+  const int kx0 = blockIdx.x * TK;
   const int ky = blockIdx.y;
   double2* tw = smem;
-  double2* P0 = smem + n;
-  double2* P1 = P0 + tkx * ls;
-  double2* P2 = P1 + tkx * ls;
+  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  double2* P1 = P0 + TK * ls;
+  double2* P2 = P1 + TK * ls;
   load_twiddles(tw, a.pl);
   const long plane = (long)nxh * a.ny;
   const long base = (long)nxh * ky;
-  for (int e = tid; e < tkx * n; e += nthr) {
-    const int j = e / tkx, c = e - j * tkx;
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    P0[c * ls + j] = (kx < nxh) ? a.io[base + kx + plane * j] : make_double2(0.0, 0.0);
+    P0[c * ls + sw<N>(j)] = (kx < nxh) ? a.io[base + kx + plane * j] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  double2* F = fft_lines(P0, P1, tkx, ls, a.pl, tw, false);
+  double2* F = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, false);
   double2* O = (F == P0) ? P1 : P0;
-  for (int e = tid; e < tkx * n; e += nthr) {
-    const int j = e / tkx, c = e - j * tkx;
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
+    const int s = c * ls + sw<N>(j);
     if (kx >= nxh) {
-      F[c * ls + j] = make_double2(0.0, 0.0);
-      if (a.k2) P2[c * ls + j] = make_double2(0.0, 0.0);
+      F[s] = make_double2(0.0, 0.0);
+      if (a.k2) P2[s] = make_double2(0.0, 0.0);
       continue;
     }
     const long g = base + kx + plane * j;
-    const double2 f = F[c * ls + j];
+    const double2 f = F[s];
     if (a.fden_out) a.fden_out[g] = f;
     if (a.k2) {
       const double w2 = a.k2[g];
-      P2[c * ls + j] = make_double2(f.x * w2, f.y * w2);
+      P2[s] = make_double2(f.x * w2, f.y * w2);
     }
     const double w1 = a.k1[g];
-    F[c * ls + j] = make_double2(f.x * w1, f.y * w1);
+    F[s] = make_double2(f.x * w1, f.y * w1);
   }
   __syncthreads();
-  double2* R1 = fft_lines(F, O, tkx, ls, a.pl, tw, true);
-  for (int e = tid; e < tkx * n; e += nthr) {
-    const int j = e / tkx, c = e - j * tkx;
+  double2* R1 = fft_lines<N>(F, O, TK, ls, a.pl, tw, true);
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) a.io[base + kx + plane * j] = R1[c * ls + j];
+    if (kx < nxh) a.io[base + kx + plane * j] = R1[c * ls + sw<N>(j)];
   }
   if (!a.k2) return;
   __syncthreads();
   double2* S = (R1 == F) ? O : F;
-  double2* R2 = fft_lines(P2, S, tkx, ls, a.pl, tw, true);
-  for (int e = tid; e < tkx * n; e += nthr) {
-    const int j = e / tkx, c = e - j * tkx;
+  double2* R2 = fft_lines<N>(P2, S, TK, ls, a.pl, tw, true);
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) a.out2[base + kx + plane * j] = R2[c * ls + j];
+    if (kx < nxh) a.out2[base + kx + plane * j] = R2[c * ls + sw<N>(j)];
   }
 }
 

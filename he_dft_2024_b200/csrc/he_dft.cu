@@ -91,6 +91,15 @@ struct he_ctx {
   unsigned* counter = nullptr;
   double* sums = nullptr;
   double* hsum = nullptr;  // pinned host mirror of sums
+  // optional per-kernel CUDA-event timing (he_timing / he_timing_report)
+  struct TRec {
+    const char* name;
+    cudaEvent_t a, b;
+  };
+  bool timing = false;
+  std::vector<TRec> trec;
+  std::vector<cudaEvent_t> evpool;
+  size_t evnext = 0;
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -116,6 +125,7 @@ static int fail(he_ctx_t* c, int code, const char* fmt, ...) {
 #define LAUNCHED()                                                                       \
   do {                                                                                   \
     ++ctx->launches;                                                                     \
+    tstop(ctx);                                                                          \
     cudaError_t e_ = cudaGetLastError();                                                 \
     if (e_ != cudaSuccess)                                                               \
       return fail(ctx, HE_ERR_CUDA, "kernel launch failed (%s:%d): %s", __FILE__,      \
@@ -127,6 +137,27 @@ static int fail(he_ctx_t* c, int code, const char* fmt, ...) {
     int s_ = (expr);         \
     if (s_ != HE_OK) return s_; \
   } while (0)
+
+static cudaEvent_t tevent(he_ctx_t* ctx) {
+  if (ctx->evnext == ctx->evpool.size()) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    ctx->evpool.push_back(e);
+  }
+  return ctx->evpool[ctx->evnext++];
+}
+// Marks the start of the next launch (named) when timing is on; LAUNCHED() marks its end.
+static void tname(he_ctx_t* ctx, const char* name) {
+  if (!ctx->timing) return;
+  he_ctx::TRec r{name, tevent(ctx), nullptr};
+  cudaEventRecord(r.a, ctx->stream);
+  ctx->trec.push_back(r);
+}
+static void tstop(he_ctx_t* ctx) {
+  if (!ctx->timing || ctx->trec.empty() || ctx->trec.back().b) return;
+  ctx->trec.back().b = tevent(ctx);
+  cudaEventRecord(ctx->trec.back().b, ctx->stream);
+}
 
 static int dalloc(he_ctx_t* ctx, void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
@@ -163,24 +194,34 @@ static bool tstgrid_ok(int n) {  // tstgrid.f90:9-13
 
 static int make_plan(he_ctx_t* ctx, int n, LinePlan* pl) {
   pl->n = n;
-  pl->nst = 0;
+  pl->nst = num_stages(n);
   int m = n;
-  while (m % 8 == 0 && pl->nst < kMaxStages) { pl->rad[pl->nst++] = 8; m /= 8; }
-  while (m % 4 == 0 && pl->nst < kMaxStages) { pl->rad[pl->nst++] = 4; m /= 4; }
-  while (m % 2 == 0 && pl->nst < kMaxStages) { pl->rad[pl->nst++] = 2; m /= 2; }
-  while (m % 3 == 0 && pl->nst < kMaxStages) { pl->rad[pl->nst++] = 3; m /= 3; }
-  while (m % 5 == 0 && pl->nst < kMaxStages) { pl->rad[pl->nst++] = 5; m /= 5; }
-  if (m != 1) return fail(ctx, HE_ERR_ARG, "FFT length %d is not 2^a 3^b 5^c", n);
-  std::vector<double2> tw(n);
-  for (int k = 0; k < n; ++k) {
-    long double a = -2.0L * 3.14159265358979323846264338327950288L * k / n;
-    tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+  for (int s = 0; s < pl->nst; ++s) {
+    pl->rad[s] = radix_of(m);
+    m /= pl->rad[s];
   }
+  if (m != 1 || pl->nst > kMaxStages) return fail(ctx, HE_ERR_ARG, "FFT length %d is not 2^a 3^b 5^c", n);
+  // Per-stage twiddles: stage s (radix R, ns = product of earlier radices) holds
+  // exp(-2 pi i r k / (ns R)) at [(r-1)*ns + k], r = 1..R-1, k = 0..ns-1.
+  std::vector<double2> stw;
+  int ns = 1;
+  for (int s = 0; s < pl->nst; ++s) {
+    const int R = pl->rad[s];
+    for (int r = 1; r < R; ++r)
+      for (int k = 0; k < ns; ++k) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * r * k / ((long double)ns * R);
+        stw.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+      }
+    ns *= R;
+  }
+  if (stw.empty()) stw.push_back(make_double2(1.0, 0.0));
   double2* d = nullptr;
-  TRY(dalloc_t(ctx, &d, n));
-  CK(cudaMemcpyAsync(d, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  TRY(dalloc_t(ctx, &d, stw.size()));
+  CK(cudaMemcpyAsync(d, stw.data(), stw.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   pl->tw = d;
+  pl->stw = d;
+  pl->stw_len = (int)stw.size();
   return HE_OK;
 }
 
@@ -234,20 +275,23 @@ static ReduceTail tail(he_ctx_t* ctx, int slot) {
 }
 
 template <class Op>
-static int run_stencil(he_ctx_t* ctx, const StencilGeom& g, const typename Op::T* f, const Op& op) {
+static int run_stencil(he_ctx_t* ctx, const StencilGeom& g, const typename Op::T* f, const Op& op,
+                       int slot = -1) {
   dim3 grid = stencil_grid(ctx, g), block(kTX, kTY);
-  k_stencil<Op, kTX, kTY><<<grid, block, 0, ctx->stream>>>(f, g, op);
+  ReduceTail rt{};
+  if (Op::NV > 0) {
+    TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
+    rt = tail(ctx, slot);
+  }
+  tname(ctx, Op::kname());
+  k_stencil<Op, kTX, kTY><<<grid, block, 0, ctx->stream>>>(f, g, op, rt);
   LAUNCHED();
   return HE_OK;
 }
 template <class Op>
 static int run_stencil_red(he_ctx_t* ctx, const StencilGeom& g, const typename Op::T* f,
                            const Op& op, int slot) {
-  dim3 grid = stencil_grid(ctx, g), block(kTX, kTY);
-  TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
-  k_stencil_red<Op, kTX, kTY><<<grid, block, 0, ctx->stream>>>(f, g, op, tail(ctx, slot));
-  LAUNCHED();
-  return HE_OK;
+  return run_stencil(ctx, g, f, op, slot);
 }
 
 static Timec timec_view(const he_ctx_t* ctx) {
@@ -271,10 +315,65 @@ static XArgs xargs(he_ctx_t* ctx) {
   a.C = ctx->fn.C; a.beta = ctx->fn.beta; a.den_m = ctx->fn.den_m;
   return a;
 }
+// Line lengths with a compile-time FFT instantiation; other admissible lengths run the same
+// kernels with run-time sizes (N = 0).
+#define HE_FFT_SIZES(X) X(32) X(64) X(96) X(128) X(160) X(192) X(256)
+
+static size_t fft_smem(const LinePlan& pl, int lines, int nbuf) {
+  return sizeof(double2) * (((size_t)pl.stw_len + 1) / 2 * 2 + (size_t)nbuf * lines * line_stride(pl.n));
+}
+static bool x_fast(const he_ctx_t* ctx) {
+  switch (ctx->nx) {
+#define HE_CASE(N) case N:
+    HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    return ((long)ctx->ny * ctx->nz) % tile_rows(ctx->nx) == 0;
+    default: return false;
+  }
+}
+static bool yz_fast(int n) {
+  switch (n) {
+#define HE_CASE(N) case N:
+    HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    return true;
+    default: return false;
+  }
+}
+
+template <int MODE, int N>
+static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
+  const int rb = (N > 0) ? tile_rows(N) : a.rb;
+  const unsigned nb = (unsigned)((a.rows + rb - 1) / rb);
+  const size_t smem = fft_smem(ctx->plx, rb, 2);
+  static const char* names[5] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
+                                 "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4"};
+  CK(cudaFuncSetAttribute(k_xpass<MODE, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tname(ctx, names[MODE]);
+  k_xpass<MODE, N><<<nb, 256, smem, ctx->stream>>>(a);
+  LAUNCHED();
+  return HE_OK;
+}
 template <int MODE>
 static int xpass(he_ctx_t* ctx, const XArgs& a) {
-  const unsigned nb = (unsigned)((a.rows + a.rb - 1) / a.rb);
-  k_xpass<MODE><<<nb, 256, ctx->smem_x, ctx->stream>>>(a);
+  if (x_fast(ctx)) {
+    switch (ctx->nx) {
+#define HE_CASE(N) case N: return xpass_n<MODE, N>(ctx, a);
+      HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    }
+  }
+  return xpass_n<MODE, 0>(ctx, a);
+}
+
+template <int N>
+static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
+  const int tk = (N > 0) ? tile_rows(N) : ctx->tkx;
+  const size_t smem = fft_smem(ctx->ply, tk, 2);
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->nz, narr);
+  CK(cudaFuncSetAttribute(k_ypass<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tname(ctx, "fft_y");
+  k_ypass<N><<<grid, 256, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
@@ -284,8 +383,25 @@ static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
   a.pl = ctx->ply;
   a.arr[0] = a0; a.arr[1] = a1 ? a1 : a0;
   a.inv = inv;
-  dim3 grid((ctx->nxh + ctx->tkx - 1) / ctx->tkx, ctx->nz, a1 ? 2 : 1);
-  k_ypass<<<grid, 256, ctx->smem_y, ctx->stream>>>(a);
+  const int narr = a1 ? 2 : 1;
+  if (yz_fast(ctx->ny)) {
+    switch (ctx->ny) {
+#define HE_CASE(N) case N: return ypass_n<N>(ctx, a, narr);
+      HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    }
+  }
+  return ypass_n<0>(ctx, a, narr);
+}
+
+template <int N>
+static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
+  const int tk = (N > 0) ? tile_rows(N) : ctx->tkx;
+  const size_t smem = fft_smem(ctx->plz, tk, 3);
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
+  CK(cudaFuncSetAttribute(k_zconv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
+  k_zconv<N><<<grid, 256, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
@@ -295,10 +411,14 @@ static int zconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, co
   a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
   a.pl = ctx->plz;
   a.io = io; a.out2 = out2; a.fden_out = fden_out; a.k1 = k1; a.k2 = k2;
-  dim3 grid((ctx->nxh + ctx->tkx - 1) / ctx->tkx, ctx->ny, 1);
-  k_zconv<<<grid, 256, ctx->smem_z, ctx->stream>>>(a);
-  LAUNCHED();
-  return HE_OK;
+  if (yz_fast(ctx->nz)) {
+    switch (ctx->nz) {
+#define HE_CASE(N) case N: return zconv_n<N>(ctx, a);
+      HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    }
+  }
+  return zconv_n<0>(ctx, a);
 }
 
 // fden = R2C(den); wA <- fden*wcgk and wB <- fden*fvlj4 back in (x-transformed) row space.
@@ -588,6 +708,7 @@ static int stat_hpsi(he_ctx_t* ctx, double* out, int slot) {
 }
 
 static int stat_normalize(he_ctx_t* ctx, int n4) {
+  tname(ctx, "statics_normalize");
   k_stat_normalize<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
                                                             ctx->sums, (double)n4, ctx->dxyz);
   LAUNCHED();
@@ -668,23 +789,17 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   TRY(make_plan(ctx, ctx->ny, &ctx->ply));
   TRY(make_plan(ctx, ctx->nz, &ctx->plz));
   const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
-  ctx->tkx = (nmax <= 256) ? 16 : 8;
-  ctx->x_rb = (ctx->nx <= 256) ? 16 : 8;
+  ctx->tkx = tile_rows(nmax);
+  ctx->x_rb = tile_rows(ctx->nx);
   while (ctx->x_rb > 2 && ((long)ctx->ny * ctx->nz) % ctx->x_rb) ctx->x_rb -= 2;
-  ctx->smem_x = sizeof(double2) * (ctx->nx + 2 * (size_t)ctx->x_rb * (ctx->nx + 1));
-  ctx->smem_y = sizeof(double2) * (ctx->ny + 2 * (size_t)ctx->tkx * (ctx->ny + 1));
-  ctx->smem_z = sizeof(double2) * (ctx->nz + 3 * (size_t)ctx->tkx * (ctx->nz + 1));
-  int maxsm = 0;
-  CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
+  ctx->smem_x = fft_smem(ctx->plx, tile_rows(ctx->nx), 2);
+  ctx->smem_y = fft_smem(ctx->ply, ctx->tkx, 2);
+  ctx->smem_z = fft_smem(ctx->plz, ctx->tkx, 3);
+  int maxsm = 0, dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   if ((int)ctx->smem_x > maxsm || (int)ctx->smem_y > maxsm || (int)ctx->smem_z > maxsm)
     return fail(ctx, HE_ERR_ARG, "grid too large for the shared-memory FFT passes");
-  CK(cudaFuncSetAttribute(k_xpass<X_R2C_DEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_x));
-  CK(cudaFuncSetAttribute(k_xpass<X_R2C_CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_x));
-  CK(cudaFuncSetAttribute(k_xpass<X_C2R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_x));
-  CK(cudaFuncSetAttribute(k_xpass<X_C2R2_CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_x));
-  CK(cudaFuncSetAttribute(k_xpass<X_C2R_POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_x));
-  CK(cudaFuncSetAttribute(k_ypass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_y));
-  CK(cudaFuncSetAttribute(k_zconv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_z));
 
   const size_t N = ctx->N, Nk = ctx->Nk;
   TRY(dalloc_t(ctx, &ctx->fden, Nk));
@@ -731,6 +846,7 @@ void he_ctx_destroy(he_ctx_t* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->hsum) cudaFreeHost(ctx->hsum);
+  for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -770,6 +886,7 @@ int he_compute_kernels(he_ctx_t* ctx) {
   a.op_core = ctx->op_core; a.otc = 0;
   a.eps = ctx->fn.eps4; a.sigma = ctx->fn.sigma4; a.hc = ctx->fn.h4; a.l = ctx->fn.l;
   a.fvlj4 = ctx->fvlj4; a.wcgk = ctx->wcgk; a.kalfs = ctx->kalfs;
+  tname(ctx, "kspace_kernels");
   k_kernels<<<kPwBlocks, 256, 0, ctx->stream>>>(a);
   LAUNCHED();
   CK(cudaStreamSynchronize(ctx->stream));
@@ -937,6 +1054,7 @@ int he_forceimp(he_ctx_t* ctx, double* F) {
   // The fused field pass of he_potenimp accumulated sum(grad den * uimp_k) for the current den and
   // rimp; redo it if either changed since.
   if (!ctx->force_fresh) TRY(he_potenimp(ctx));
+  tname(ctx, "impurity_force");
   k_imp_force<<<1, 32, 0, ctx->stream>>>(ctx->imp, ctx->sums + S_FORCE, ctx->dxyz);
   LAUNCHED();
   if (F) {
@@ -951,6 +1069,7 @@ int he_set_accel(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "dynamics routine");
   if (ctx->n_imp == 0) return HE_OK;
+  tname(ctx, "impurity_accel");
   k_imp_accel<<<1, 32, 0, ctx->stream>>>(ctx->imp);
   LAUNCHED();
   return HE_OK;
@@ -989,6 +1108,7 @@ int he_steprk(he_ctx_t* ctx, double deltat) {
     }
     ctx->force_fresh = false;
     if (ctx->n_imp > 0) {
+      tname(ctx, "impurity_rk");
       k_imp_rk<<<1, 32, 0, ctx->stream>>>(ctx->imp, jr, arun[jr], brun[jr], crun[jr], deltat);
       LAUNCHED();
     }
@@ -1021,6 +1141,7 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   }
   ctx->force_fresh = false;
   if (ctx->n_imp > 0) {
+    tname(ctx, "impurity_predict");
     k_imp_predict<<<1, 32, 0, ctx->stream>>>(ctx->imp, deltat);
     LAUNCHED();
   }
@@ -1048,6 +1169,7 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   }
   ctx->force_fresh = false;
   if (ctx->n_imp > 0) {
+    tname(ctx, "impurity_correct");
     k_imp_correct<<<1, 32, 0, ctx->stream>>>(ctx->imp, deltat);
     LAUNCHED();
   }
@@ -1159,6 +1281,7 @@ int he_evolo0(he_ctx_t* ctx, double* mu4, double* mu4err, int n4) {
   if (!ctx || !mu4 || !mu4err) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
   TRY(stat_hpsi(ctx, ctx->hpsi, S_STAT_H));
+  tname(ctx, "statics_sumsq");
   k_sumsq<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double*)ctx->psi, ctx->N, tail(ctx, S_STAT_N));
   LAUNCHED();
   TRY(stat_normalize(ctx, n4));
@@ -1179,7 +1302,9 @@ int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
   for (int jr = 0; jr < 4; ++jr) {
     TRY(stat_hpsi(ctx, ctx->hpsi, S_STAT_H));
     if (jr == 0) {
-      k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H);
+      tname(ctx, "copy_slot");
+      tname(ctx, "copy_slot");
+  k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H);
       LAUNCHED();
     }
     StatPW s = statpw(ctx, deltat, n4);
@@ -1190,6 +1315,7 @@ int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
     s.hsave = jr == 0 ? (double*)ctx->hpsiold[1] : nullptr;
     s.a = arun[jr]; s.b = brun[jr]; s.c = crun[jr];
     s.jr = jr;
+    tname(ctx, "statics_rk_update");
     k_stat_rk<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
     LAUNCHED();
     if (jr == 0) {
@@ -1226,6 +1352,7 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
     s.h1 = (const double*)ctx->hpsiold[ctx->ioldh[0] - 1];
     s.h2 = (double*)ctx->hpsiold[ctx->ioldh[1] - 1];
     s.pc = (double*)ctx->pc;
+    tname(ctx, "statics_predict");
     k_stat_predict<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
     LAUNCHED();
     std::swap(ctx->psi, ctx->psiold[ctx->ioldp[2] - 1]);
@@ -1245,11 +1372,13 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
     s.pc = (double*)ctx->pc;
     s.out = (double*)ctx->scratch;
     ReduceTail rt = tail(ctx, S_STAT_PC);
+    tname(ctx, "statics_correct");
     k_stat_correct<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, rt);
     LAUNCHED();
     std::swap(ctx->psi, ctx->scratch);
   }
   // k_stat_correct leaves sum psi^2 in S_STAT_PC+1; the normalisation reads S_STAT_N.
+  tname(ctx, "copy_slot");
   k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_STAT_N, S_STAT_PC + 1);
   LAUNCHED();
   TRY(stat_normalize(ctx, n4));
@@ -1268,11 +1397,51 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
 int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu) {
   if (!ctx || !errmu) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
+  tname(ctx, "statics_varmu");
   k_varmu<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(ctx->hpsi, (const double*)ctx->psi, ctx->N, mu,
                                                    tail(ctx, S_VARMU));
   LAUNCHED();
   TRY(read_sums(ctx));
   *errmu = ctx->hsum[S_VARMU] * ctx->dxyz / (double)npart;
+  return HE_OK;
+}
+
+int he_timing(he_ctx_t* ctx, int enable) {
+  if (!ctx) return HE_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->trec.clear();
+  ctx->evnext = 0;
+  ctx->timing = enable != 0;
+  // Create the events up front so that recording never waits on event creation.
+  while (enable && ctx->evpool.size() < 8192) {
+    cudaEvent_t e = nullptr;
+    CK(cudaEventCreate(&e));
+    ctx->evpool.push_back(e);
+  }
+  return HE_OK;
+}
+
+int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n) {
+  if (!ctx || !n) return fail(ctx, HE_ERR_ARG, "null argument");
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<he_kernel_time_t> agg;
+  for (const auto& r : ctx->trec) {
+    if (!r.b) continue;
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    size_t k = 0;
+    for (; k < agg.size(); ++k)
+      if (std::strncmp(agg[k].name, r.name, sizeof(agg[k].name)) == 0) break;
+    if (k == agg.size()) {
+      he_kernel_time_t t{};
+      std::strncpy(t.name, r.name, sizeof(t.name) - 1);
+      agg.push_back(t);
+    }
+    agg[k].launches += 1;
+    agg[k].ms += ms;
+  }
+  *n = (int)agg.size();
+  for (int i = 0; i < (int)agg.size() && i < max; ++i) out[i] = agg[i];
   return HE_OK;
 }
 

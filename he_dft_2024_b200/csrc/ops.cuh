@@ -5,100 +5,6 @@
 
 namespace he {
 
-// ---- deterministic grid reduction: per-block partials, the last CTA to finish sums them ------
-struct ReduceTail {
-  double* partials;
-  unsigned* counter;
-  double* out;
-};
-
-template <int NV>
-__device__ void reduce_tail(const ReduceTail& rt, long nb) {
-  __shared__ bool s_last;
-  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-  const int nthr = blockDim.x * blockDim.y * blockDim.z;
-  if (tid == 0) {
-    __threadfence();
-    const unsigned t = atomicAdd(rt.counter, 1u);
-    s_last = (t == (unsigned)(nb - 1));
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  double v[NV];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-    double s = 0.0;
-    for (long b = tid; b < nb; b += nthr) s += __ldcg(rt.partials + b * NV + k);
-    v[k] = s;
-  }
-  block_reduce_store<NV>(v, rt.out);
-  if (tid == 0) *rt.counter = 0u;
-}
-
-// Stencil kernel with the reduction tail (ops with NV > 0).
-template <class Op, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY)
-    k_stencil_red(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
-                  const ReduceTail rt) {
-  using T = typename Op::T;
-  constexpr int NV = Op::NV;
-  __shared__ T tile[TY + 12][TX + 12];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = tx + TX * ty;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int ix = x0 + tx, iy = y0 + ty;
-  const int z0 = blockIdx.z * g.zc;
-  const int z1 = min(z0 + g.zc, g.nz);
-  const bool inside = (ix < g.nx) && (iy < g.ny);
-  double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-  T q[13];
-#pragma unroll
-  for (int m = 0; m < 12; ++m)
-    q[m + 1] = inside ? load_bc(f, g, ix, iy, z0 - 6 + m) : zero_of(T());
-  for (int iz = z0; iz < z1; ++iz) {
-#pragma unroll
-    for (int m = 0; m < 12; ++m) q[m] = q[m + 1];
-    q[12] = inside ? load_bc(f, g, ix, iy, iz + 6) : zero_of(T());
-    tile[ty + 6][tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
-    for (int e = tid; e < 12 * TY; e += TX * TY) {
-      const int r = e / 12, c = e - r * 12;
-      const int sx = (c < 6) ? c : TX + c;
-      tile[r + 6][sx] = load_bc(f, g, x0 + sx - 6, y0 + r, iz);
-    }
-    for (int e = tid; e < 12 * TX; e += TX * TY) {
-      const int r = e / TX, c = e - r * TX;
-      const int sy = (r < 6) ? r : TY + r;
-      tile[sy][c + 6] = load_bc(f, g, x0 + c, y0 + sy - 6, iz);
-    }
-    __syncthreads();
-    if (inside) {
-      T dx = zero_of(T()), dy = zero_of(T()), dz = zero_of(T());
-      if (g.axis_on[0]) {
-#pragma unroll
-        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tile[ty + 6][tx + m], dx);
-      }
-      if (g.axis_on[1]) {
-#pragma unroll
-        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tile[ty + m][tx + 6], dy);
-      }
-      if (g.axis_on[2]) {
-#pragma unroll
-        for (int m = 0; m < 13; ++m) dz = axpy(g.w[2][m], q[m], dz);
-      }
-      const long idx = (long)ix + (long)g.nx * ((long)iy + (long)g.ny * iz);
-      op.at(ix, iy, iz, idx, dx, dy, dz, q[6], acc);
-    }
-    __syncthreads();
-  }
-  const long nb = (long)gridDim.x * gridDim.y * gridDim.z;
-  const long b = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
-  block_reduce_store<NV>(acc, rt.partials + b * NV);
-  reduce_tail<NV>(rt, nb);
-}
-
 // ---- absorbing mask: timec = (Lambdah*(1+tx+1+ty+1+tz), 1)  (DFT4He3d.f90:592-601) -----------
 struct Timec {
   const double* ax;  // tanh((|x_i|-txmean)/txsurf), host-evaluated per axis
@@ -126,6 +32,7 @@ HE_D double2 hpsi_rt(double2 dx, double2 dy, double2 dz, double2 c, double pot, 
 // steppc predictor + modifier (steppc.f90:51-61).  po3 = psiold(ioldp(3)) is read and receives
 // the new psi (the host then swaps it with the psi buffer, so psiold(ioldp(3)) holds the old psi).
 struct OpPredict {
+  static const char* kname() { return "hpsi_pmc_predict"; }
   using T = double2;
   static constexpr int NV = 0;
   const double* pot4;
@@ -137,14 +44,19 @@ struct OpPredict {
   double* den;
   Timec tm;
   double h2o2m, s43, c112;
+  struct In {
+    double pot, u;
+    double2 p3, h1, h2, pc;
+  };
+  HE_D In load(long i) const { return In{pot4[i], uimp[i], po3[i], h1[i], h2[i], pc[i]}; }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               double*) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, pot4[i], uimp[i], tm.re(ix, iy, iz), h2o2m);
-    const double2 hh1 = h1[i], hh2 = h2[i];
+               const In& v, double*) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, v.pot, v.u, tm.re(ix, iy, iz), h2o2m);
+    const double2 hh1 = v.h1, hh2 = v.h2;
     const double2 t = make_double2(2.0 * s4.x - hh1.x + 2.0 * hh2.x, 2.0 * s4.y - hh1.y + 2.0 * hh2.y);
-    const double2 p3 = po3[i];
+    const double2 p3 = v.p3;
     const double2 sto1 = make_double2(p3.x + s43 * t.x, p3.y + s43 * t.y);
-    const double2 pcv = pc[i];
+    const double2 pcv = v.pc;
     const double2 pn = make_double2(sto1.x - c112 * pcv.x, sto1.y - c112 * pcv.y);
     pc[i] = sto1;
     h2[i] = s4;
@@ -155,6 +67,7 @@ struct OpPredict {
 
 // steppc corrector + final value (steppc.f90:118-127); accumulates sum |pc|.
 struct OpCorrect {
+  static const char* kname() { return "hpsi_pmc_correct"; }
   using T = double2;
   static constexpr int NV = 1;
   const double* pot4;
@@ -168,14 +81,19 @@ struct OpCorrect {
   double* den;
   Timec tm;
   double h2o2m, s3, c9;
+  struct In {
+    double pot, u;
+    double2 p3, p2, h1, h2, pc;
+  };
+  HE_D In load(long i) const { return In{pot4[i], uimp[i], po3[i], po2[i], h1[i], h2[i], pc[i]}; }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               double* acc) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, pot4[i], uimp[i], tm.re(ix, iy, iz), h2o2m);
-    const double2 a3 = po3[i], a2 = po2[i], b1 = h1[i], b2 = h2[i];
+               const In& v, double* acc) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, v.pot, v.u, tm.re(ix, iy, iz), h2o2m);
+    const double2 a3 = v.p3, a2 = v.p2, b1 = v.h1, b2 = v.h2;
     const double2 inner = make_double2(s4.x + 2.0 * b1.x - b2.x, s4.y + 2.0 * b1.y - b2.y);
     const double2 s5 = make_double2(0.125 * (9.0 * a3.x - a2.x + s3 * inner.x),
                                     0.125 * (9.0 * a3.y - a2.y + s3 * inner.y));
-    const double2 p = pc[i];
+    const double2 p = v.pc;
     const double2 pn = make_double2(p.x - s5.x, p.y - s5.y);
     pc[i] = pn;
     const double2 o = make_double2(s5.x + c9 * pn.x, s5.y + c9 * pn.y);
@@ -187,6 +105,7 @@ struct OpCorrect {
 
 // One RK-Gill stage (steprk.f90:67-79).  hsave (stage 1 only) receives H psi for hpsiold(1).
 struct OpRK {
+  static const char* kname() { return "hpsi_rkgill_stage"; }
   using T = double2;
   static constexpr int NV = 0;
   const double* pot4;
@@ -197,10 +116,15 @@ struct OpRK {
   double* den;
   Timec tm;
   double h2o2m, a, b, cc, dt;
+  struct In {
+    double pot, u;
+    double2 q;
+  };
+  HE_D In load(long i) const { return In{pot4[i], uimp[i], q[i]}; }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               double*) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, pot4[i], uimp[i], tm.re(ix, iy, iz), h2o2m);
-    const double2 qq = q[i];
+               const In& v, double*) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, v.pot, v.u, tm.re(ix, iy, iz), h2o2m);
+    const double2 qq = v.q;
     const double2 s1 = make_double2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
     q[i] = make_double2(qq.x + 3.0 * s1.x - cc * s4.x, qq.y + 3.0 * s1.y - cc * s4.y);
     if (hsave) hsave[i] = s4;
@@ -215,6 +139,7 @@ struct OpRK {
 //          sum den*(1+tanh(beta*(den-den_m))), sum uimp*den}
 template <typename TT>
 struct OpEnergy {
+  static const char* kname() { return "energy_reduce"; }
   using T = TT;
   static constexpr int NV = 5;
   const double* den;
@@ -225,24 +150,32 @@ struct OpEnergy {
   int lsolid;
   HE_D static double n2(double v) { return v * v; }
   HE_D static double n2(double2 v) { return v.x * v.x + v.y * v.y; }
-  HE_D void at(int, int, int, long i, T dx, T dy, T dz, T, double* acc) const {
-    const double a3 = den[i], a4 = dencg[i];
+  struct In {
+    double den, dcg, dlj, u;
+  };
+  HE_D In load(long i) const { return In{den[i], dencg[i], delj4[i], uimp ? uimp[i] : 0.0}; }
+  HE_D void at(int, int, int, long, T dx, T dy, T dz, T, const In& v, double* acc) const {
+    const double a3 = v.den, a4 = v.dcg;
     acc[0] += n2(dx) + n2(dy) + n2(dz);
-    acc[1] += delj4[i] * a3;
+    acc[1] += v.dlj * a3;
     acc[2] += a3 * a4 * a4 * (aux1 + aux2 * a4);
     if (lsolid) acc[3] += a3 * (1.0 + tanh(beta * (a3 - den_m)));
-    if (uimp) acc[4] += uimp[i] * a3;
+    acc[4] += v.u * a3;
   }
 };
 
 // derden(): dxden, dyden, dzden (derden.f90:26-28).
 struct OpDerden {
+  static const char* kname() { return "derden"; }
   using T = double;
   static constexpr int NV = 0;
   double* gx;
   double* gy;
   double* gz;
-  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double, double*) const {
+  struct In {};
+  HE_D In load(long) const { return In{}; }
+  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double, const In&,
+               double*) const {
     gx[i] = dx;
     gy[i] = dy;
     gz[i] = dz;
@@ -273,6 +206,7 @@ struct ImpDev {
 // radius is clamped to the table end and the index is taken after the clamp.
 template <int NI>
 struct OpImpField {
+  static const char* kname() { return "impurity_field_force"; }
   using T = double;
   static constexpr int NV = 3 * NI;
   const double* tab;  // (npot) per impurity, impurity-major
@@ -281,8 +215,10 @@ struct OpImpField {
   int n, npot;
   double delinter, rmax;
   double xmax, ymax, zmax, hx, hy, hz;
+  struct In {};
+  HE_D In load(long) const { return In{}; }
   HE_D void at(int ix, int iy, int iz, long i, double dx, double dy, double dz, double,
-               double* acc) const {
+               const In&, double* acc) const {
     const double x = -xmax + hx * ix, y = -ymax + hy * iy, z = -zmax + hz * iz;
     double u = 0.0;
 #pragma unroll
@@ -297,8 +233,13 @@ struct OpImpField {
           r = rmax;
         }
         int i0 = (int)(r / delinter);
+        // mod(r,DelInter) is exact: r - q*DelInter with q = trunc(r/DelInter) taken exactly.
+        // One fma gives that value exactly whenever the rounded quotient i0 equals q (the
+        // remainder is then representable); otherwise fall back to fmod.
+        double rm = fma(-(double)i0, delinter, r);
+        if (rm < 0.0 || rm >= delinter) rm = fmod(r, delinter);
         if (i0 > npot - 2) i0 = npot - 2;
-        const double rmod = fmod(r, delinter) / delinter;
+        const double rmod = rm / delinter;
         const double* t = tab + (long)k * npot;
         const double uk = t[i0] * (1.0 - rmod) + t[i0 + 1] * rmod;
         u = u + uk;
@@ -456,14 +397,19 @@ __global__ void k_imp_correct(ImpDev* s, double dt) {
 // ---- statics (real psi) ------------------------------------------------------------------------
 // hpsi = -(d2x+d2y+d2z)*h2o2m4 + pot4*psi; acc = sum psi*hpsi  (steppcr.f90:40-42).
 struct OpHpsiR {
+  static const char* kname() { return "statics_hpsi"; }
   using T = double;
   static constexpr int NV = 1;
   const double* pot4;
   double* out;
   double h2o2m;
-  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double c,
+  struct In {
+    double pot;
+  };
+  HE_D In load(long i) const { return In{pot4[i]}; }
+  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double c, const In& v,
                double* acc) const {
-    const double h = -((dx + dy) + dz) * h2o2m + pot4[i] * c;
+    const double h = -((dx + dy) + dz) * h2o2m + v.pot * c;
     out[i] = h;
     acc[0] += c * h;
   }

@@ -7,12 +7,15 @@
 // shorter than npd gives a zero derivative (init_deriv_parallel.f90:949-953).  The weights are
 // the Bickley rows times Sto = 1/h**id.
 //
-// Kernel shape (2.5-D streaming): a CTA owns a TX x TY tile of the x-y plane and marches through a
-// chunk of z.  Each thread keeps the 13 values f(x,y,z-6..z+6) of its column in registers (the z
-// derivative), and the CTA stages the current plane with a 6-point halo in shared memory (the x
-// and y derivatives).  Every field value is read from HBM once per chunk; halo re-reads hit L2.
-// The consumer ('Op') receives the three derivatives and the centre value and does the fused
-// pointwise work (H psi, predictor/corrector, reductions) in the same pass.
+// Kernel shape (2.5-D streaming, software pipelined): a CTA owns a TX x TY tile of the x-y plane
+// and marches through a chunk of z.  Each thread keeps f(x,y,z-6..z+6) of its column in registers
+// (the z derivative); the CTA stages the current plane with its 6-point x/y halo in shared memory
+// (the x and y derivatives).  While plane z is being consumed, the next plane is already in
+// flight: its halo by cp.async into the other half of a double-buffered tile (zero-filled
+// outside the grid for icon=13), its z+7 column value and the consumer's pointwise operands by
+// register prefetch.  Every field value is read from HBM once per chunk; halo re-reads hit L2.
+// The consumer ('Op') receives the three derivatives, the centre value and its prefetched
+// operands and does the fused pointwise work (H psi, predictor/corrector, reductions).
 #pragma once
 #include "common.cuh"
 
@@ -26,36 +29,97 @@ struct StencilGeom {
   double w[3][13];   // scaled weights per axis
 };
 
+// Resolve (ix,iy,iz) under the boundary condition: returns false for a zero-padded point
+// (icon=13), otherwise the in-range index and whether the value is negated (icon=18).
+HE_D bool resolve_bc(const StencilGeom& g, int& ix, int& iy, int& iz, bool& neg) {
+  neg = false;
+  if (g.icon == 13)
+    return !(ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny || iz < 0 || iz >= g.nz);
+  const bool anti = (g.icon == 18);
+  if (ix < 0) { ix += g.nx; neg ^= anti; } else if (ix >= g.nx) { ix -= g.nx; neg ^= anti; }
+  if (iy < 0) { iy += g.ny; neg ^= anti; } else if (iy >= g.ny) { iy -= g.ny; neg ^= anti; }
+  if (iz < 0) { iz += g.nz; neg ^= anti; } else if (iz >= g.nz) { iz -= g.nz; neg ^= anti; }
+  // Axes shorter than 6 points (whose derivative is off) can still be out of range after one
+  // wrap; keep the unused load inside the array.
+  ix = min(max(ix, 0), g.nx - 1);
+  iy = min(max(iy, 0), g.ny - 1);
+  iz = min(max(iz, 0), g.nz - 1);
+  return true;
+}
+
 template <typename T>
 HE_D T load_bc(const T* __restrict__ f, const StencilGeom& g, int ix, int iy, int iz) {
-  bool neg = false;
-  if (g.icon == 13) {
-    if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny || iz < 0 || iz >= g.nz) return zero_of(T());
-  } else {
-    const bool anti = (g.icon == 18);
-    if (ix < 0) { ix += g.nx; neg ^= anti; } else if (ix >= g.nx) { ix -= g.nx; neg ^= anti; }
-    if (iy < 0) { iy += g.ny; neg ^= anti; } else if (iy >= g.ny) { iy -= g.ny; neg ^= anti; }
-    if (iz < 0) { iz += g.nz; neg ^= anti; } else if (iz >= g.nz) { iz -= g.nz; neg ^= anti; }
-    // Axes shorter than 6 points (whose derivative is off) can still be out of range after one
-    // wrap; keep the unused load inside the array.
-    ix = min(max(ix, 0), g.nx - 1);
-    iy = min(max(iy, 0), g.ny - 1);
-    iz = min(max(iz, 0), g.nz - 1);
-  }
+  bool neg;
+  if (!resolve_bc(g, ix, iy, iz, neg)) return zero_of(T());
   T v = f[(long)ix + (long)g.nx * ((long)iy + (long)g.ny * iz)];
   return neg_if(v, neg);
 }
 
+// Asynchronous global -> shared copy of one element (cp.async, zero fill when src_bytes = 0).
+template <typename T>
+HE_D void cp_async_elem(T* dst_smem, const T* src, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_smem);
+  const int nbytes = valid ? (int)sizeof(T) : 0;
+  if constexpr (sizeof(T) == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src),
+                 "r"(nbytes));
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src),
+                 "r"(nbytes));
+  }
+}
+HE_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+HE_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Reductions: per-block partials, the last CTA to finish sums them in a fixed order.
+struct ReduceTail {
+  double* partials;
+  unsigned* counter;
+  double* out;
+};
+
+template <int NV>
+__device__ void reduce_tail(const ReduceTail& rt, long nb) {
+  __shared__ bool s_last;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthr = blockDim.x * blockDim.y * blockDim.z;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(rt.counter, 1u);
+    s_last = (t == (unsigned)(nb - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = 0.0;
+    for (long b = tid; b < nb; b += nthr) s += __ldcg(rt.partials + b * NV + k);
+    v[k] = s;
+  }
+  block_reduce_store<NV>(v, rt.out);
+  if (tid == 0) *rt.counter = 0u;
+}
+
 // Op interface:
-//   using T;                        field element type (double or double2)
-//   static constexpr int NV;        number of FP64 block reductions (0 = none)
-//   HE_D void at(int ix,int iy,int iz,long idx,T dx,T dy,T dz,T c,double* acc) const;
-// k_stencil serves ops without reductions; ops.cuh adds k_stencil_red with the grid reduction.
+//   using T;                      field element type (double or double2)
+//   static constexpr int NV;      number of FP64 block reductions (0 = none)
+//   struct In;                    the pointwise operands of one grid point
+//   HE_D In load(long idx) const; issue their loads (prefetched one plane ahead)
+//   HE_D void at(int ix,int iy,int iz,long idx,T dx,T dy,T dz,T c,const In&,double* acc) const;
 template <class Op, int TX, int TY>
 __global__ void __launch_bounds__(TX* TY)
-    k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op) {
+    k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
+              const ReduceTail rt) {
   using T = typename Op::T;
-  __shared__ T tile[TY + 12][TX + 12];
+  using In = typename Op::In;
+  constexpr int NT = TX * TY;
+  constexpr int NH = 12 * (TX + TY);       // halo elements per plane
+  constexpr int HK = (NH + NT - 1) / NT;   // halo elements per thread
+  constexpr int NV = Op::NV > 0 ? Op::NV : 1;
+  __shared__ __align__(16) T tile[2][TY + 12][TX + 12];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + TX * ty;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -63,51 +127,109 @@ __global__ void __launch_bounds__(TX* TY)
   const int z0 = blockIdx.z * g.zc;
   const int z1 = min(z0 + g.zc, g.nz);
   const bool inside = (ix < g.nx) && (iy < g.ny);
-  double acc[1] = {0.0};
+  const long plane = (long)g.nx * g.ny;
+  const long idx0 = (long)min(ix, g.nx - 1) + (long)g.nx * min(iy, g.ny - 1);
 
+  // This thread's halo elements: shared-memory slot and grid position.
+  int hsy[HK], hsx[HK];
+#pragma unroll
+  for (int k = 0; k < HK; ++k) {
+    const int e = tid + k * NT;
+    if (e < 12 * TY) {  // x halo: 6 columns each side of the TY rows
+      const int r = e / 12, c = e - r * 12;
+      hsy[k] = r + 6;
+      hsx[k] = (c < 6) ? c : TX + c;
+    } else if (e < NH) {  // y halo: 6 rows each side of the TX columns
+      const int e2 = e - 12 * TY;
+      const int r = e2 / TX, c = e2 - r * TX;
+      hsy[k] = (r < 6) ? r : TY + r;
+      hsx[k] = c + 6;
+    } else {
+      hsy[k] = -1;
+      hsx[k] = 0;
+    }
+  }
+  auto issue_halo = [&](int buf, int iz) {
+#pragma unroll
+    for (int k = 0; k < HK; ++k) {
+      if (hsy[k] < 0) continue;
+      int gx = x0 + hsx[k] - 6, gy = y0 + hsy[k] - 6, gz = iz;
+      bool neg;
+      const bool ok = resolve_bc(g, gx, gy, gz, neg);
+      const T* src = ok ? f + (long)gx + (long)g.nx * ((long)gy + (long)g.ny * gz) : f;
+      cp_async_elem(&tile[buf][hsy[k]][hsx[k]], src, ok);
+    }
+    cp_async_commit();
+  };
+  // Antiperiodic wrap: negate this thread's wrapped halo elements once they have landed.
+  auto fix_halo_sign = [&](int buf, int iz) {
+    if (g.icon != 18) return;
+#pragma unroll
+    for (int k = 0; k < HK; ++k) {
+      if (hsy[k] < 0) continue;
+      int gx = x0 + hsx[k] - 6, gy = y0 + hsy[k] - 6, gz = iz;
+      bool neg;
+      resolve_bc(g, gx, gy, gz, neg);
+      if (neg) tile[buf][hsy[k]][hsx[k]] = neg_if(tile[buf][hsy[k]][hsx[k]], true);
+    }
+  };
+
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+
+  // Prologue: z-queue f(z0-6 .. z0+5), the next column value f(z0+6), plane z0's halo and
+  // operands.
   T q[13];
 #pragma unroll
   for (int m = 0; m < 12; ++m)
     q[m + 1] = inside ? load_bc(f, g, ix, iy, z0 - 6 + m) : zero_of(T());
+  T qn = inside ? load_bc(f, g, ix, iy, z0 + 6) : zero_of(T());
+  issue_halo(0, z0);
+  In cur = op.load(idx0 + plane * z0);
 
   for (int iz = z0; iz < z1; ++iz) {
+    const int b = (iz - z0) & 1;
 #pragma unroll
     for (int m = 0; m < 12; ++m) q[m] = q[m + 1];
-    q[12] = inside ? load_bc(f, g, ix, iy, iz + 6) : zero_of(T());
-    // Centre: threads past the grid edge (partial tiles) stage the boundary value instead
-    // (zero for icon=13, the wrapped value for icon=8/18).
-    tile[ty + 6][tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
-    // x halo: 6 columns each side for the TY rows
-    for (int e = tid; e < 12 * TY; e += TX * TY) {
-      const int r = e / 12, c = e - r * 12;
-      const int sx = (c < 6) ? c : TX + c;
-      tile[r + 6][sx] = load_bc(f, g, x0 + sx - 6, y0 + r, iz);
+    q[12] = qn;
+    // Centre of plane iz: from the queue (threads past the grid edge stage the boundary value).
+    tile[b][ty + 6][tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
+    In nxt = cur;
+    if (iz + 1 < z1) {
+      issue_halo(b ^ 1, iz + 1);
+      if (inside) qn = load_bc(f, g, ix, iy, iz + 7);
+      nxt = op.load(idx0 + plane * (iz + 1));
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
-    // y halo: 6 rows each side for the TX columns
-    for (int e = tid; e < 12 * TX; e += TX * TY) {
-      const int r = e / TX, c = e - r * TX;
-      const int sy = (r < 6) ? r : TY + r;
-      tile[sy][c + 6] = load_bc(f, g, x0 + c, y0 + sy - 6, iz);
-    }
+    fix_halo_sign(b, iz);
     __syncthreads();
     if (inside) {
       T dx = zero_of(T()), dy = zero_of(T()), dz = zero_of(T());
       if (g.axis_on[0]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tile[ty + 6][tx + m], dx);
+        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tile[b][ty + 6][tx + m], dx);
       }
       if (g.axis_on[1]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tile[ty + m][tx + 6], dy);
+        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tile[b][ty + m][tx + 6], dy);
       }
       if (g.axis_on[2]) {
 #pragma unroll
         for (int m = 0; m < 13; ++m) dz = axpy(g.w[2][m], q[m], dz);
       }
-      const long idx = (long)ix + (long)g.nx * ((long)iy + (long)g.ny * iz);
-      op.at(ix, iy, iz, idx, dx, dy, dz, q[6], acc);
+      op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], cur, acc);
     }
+    cur = nxt;
     __syncthreads();
+  }
+  if constexpr (Op::NV > 0) {
+    const long nb = (long)gridDim.x * gridDim.y * gridDim.z;
+    const long blk = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
+    block_reduce_store<NV>(acc, rt.partials + blk * NV);
+    reduce_tail<NV>(rt, nb);
   }
 }
 

@@ -188,6 +188,18 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
 /* varmu(npart,mu,errmu): He_statics/varmu.f90:31. */
 int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu);
 
+/* ---- per-kernel timing (CUDA events on the context's stream) ---- */
+/* The reference only times whole runs (Dynamics_TDDFT/DFT4He3d.f90:662-664,905-911; timer.f90);
+ * these calls add per-kernel device times.  he_timing(ctx,1) clears and starts recording,
+ * he_timing(ctx,0) stops; he_timing_report aggregates by kernel (synchronises). */
+typedef struct {
+  char name[40];
+  long long launches;
+  double ms;
+} he_kernel_time_t;
+int he_timing(he_ctx_t* ctx, int enable);
+int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
+
 #ifdef __cplusplus
 }
 #endif

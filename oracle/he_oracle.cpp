@@ -1110,6 +1110,13 @@ static double* dyn_field(Dyn* d, const char* name, long* n) {
   if (s == "aimp") return R(d->aimp, 3 * d->ni);
   if (s == "F") return R(d->F, 3 * d->ni);
   if (s == "potion") return R(d->potion, (long)d->ni * d->npot);
+  if (s == "rimpold") return R(d->rimpold, 9 * d->ni);
+  if (s == "vimpold") return R(d->vimpold, 9 * d->ni);
+  if (s == "aimpold") return R(d->aimpold, 6 * d->ni);
+  if (s == "pcr") return R(d->pcr, 3 * d->ni);
+  if (s == "pcv") return R(d->pcv, 3 * d->ni);
+  if (s == "qr") return R(d->qr, 3 * d->ni);
+  if (s == "qv") return R(d->qv, 3 * d->ni);
   return nullptr;
 }
 static double* stat_field(Stat* d, const char* name, long* n) {
@@ -1182,6 +1189,17 @@ void ho_dyn_steppc(void* h, double dt, double* err3) {
 }
 void ho_dyn_energy(void* h, double* out) { ((Dyn*)h)->energy(out); }
 int ho_dyn_lstopimp(void* h) { return ((Dyn*)h)->lstopimp ? 1 : 0; }
+// Ring indices ioldp(3), ioldh(2), ioldr(3), ioldv(3), iolda(2): set != 0 writes them.
+void ho_dyn_ring(void* h, int* r, int set) {
+  Dyn* d = (Dyn*)h;
+  int* dst[13] = {&d->ioldp[0], &d->ioldp[1], &d->ioldp[2], &d->ioldh[0], &d->ioldh[1],
+                  &d->ioldr[0], &d->ioldr[1], &d->ioldr[2], &d->ioldv[0], &d->ioldv[1],
+                  &d->ioldv[2], &d->iolda[0], &d->iolda[1]};
+  for (int i = 0; i < 13; ++i) {
+    if (set) *dst[i] = r[i];
+    else r[i] = *dst[i];
+  }
+}
 
 void* ho_stat_create(const ho_params* p) {
   Stat* d = new Stat();

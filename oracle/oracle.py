@@ -92,6 +92,7 @@ def lib():
         L.ho_dyn_energy.argtypes = [vp, dp]
         L.ho_dyn_lstopimp.restype = ctypes.c_int
         L.ho_dyn_lstopimp.argtypes = [vp]
+        L.ho_dyn_ring.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.ho_stat_create.restype = vp
         L.ho_stat_create.argtypes = [P]
         L.ho_stat_destroy.argtypes = [vp]
@@ -183,6 +184,17 @@ class Dynamics(_Fields):
         return dict(zip(ENERGY_KEYS, e))
 
     def lstopimp(self): return bool(self.L.ho_dyn_lstopimp(self.h))
+
+    def ring(self, values=None):
+        """Get (or set) ioldp(3), ioldh(2), ioldr(3), ioldv(3), iolda(2)."""
+        r = (ctypes.c_int * 13)()
+        if values is not None:
+            for i, v in enumerate(values):
+                r[i] = int(v)
+            self.L.ho_dyn_ring(self.h, r, 1)
+            return list(values)
+        self.L.ho_dyn_ring(self.h, r, 0)
+        return list(r)
 
 
 class Statics(_Fields):

@@ -70,7 +70,11 @@ def test_potion_table_follows_potenimpini():
     assert delinter == rmax / (npot - 1)
     r = np.arange(npot) * delinter
     e = 1 - np.exp(-0.8 * (r - 6.5))
-    np.testing.assert_allclose(potion[0], 2.0 * (e * e - 1), rtol=1e-15)
+    morse = 2.0 * (e * e - 1)
+    # Select_Pot contract: r < r_cutoff gives umax (the capped Morse core, umax = V(r_cutoff))
+    expect = np.where(r < C.MORSE_RCUT, C.MORSE_UMAX, morse)
+    np.testing.assert_allclose(potion[0], expect, rtol=1e-15)
+    assert C.MORSE_UMAX == pytest.approx(2.0 * ((1 - np.exp(-0.8 * (2.0 - 6.5))) ** 2 - 1))
     assert potion.shape == (1, npot)
 
 
