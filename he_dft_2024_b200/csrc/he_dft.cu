@@ -283,8 +283,11 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g, const typename Op::T
     TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
     rt = tail(ctx, slot);
   }
+  constexpr size_t smem = stencil_smem<Op, kTX, kTY>();
+  CK(cudaFuncSetAttribute(k_stencil<Op, kTX, kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)smem));
   tname(ctx, Op::kname());
-  k_stencil<Op, kTX, kTY><<<grid, block, 0, ctx->stream>>>(f, g, op, rt);
+  k_stencil<Op, kTX, kTY><<<grid, block, smem, ctx->stream>>>(f, g, op, rt);
   LAUNCHED();
   return HE_OK;
 }
@@ -664,7 +667,7 @@ static int pw_blocks(const he_ctx_t* ctx) {
 
 template <int NI>
 static int launch_impfield(he_ctx_t* ctx) {
-  OpImpField<NI> op;
+  OpImpField<NI> op{};
   op.tab = ctx->pot_tab; op.imp = ctx->imp; op.uimp = ctx->uimp;
   op.n = ctx->n_imp; op.npot = ctx->npot;
   op.delinter = ctx->delinter; op.rmax = ctx->rmaxinterpol;
@@ -700,8 +703,8 @@ static StatPW statpw(he_ctx_t* ctx, double dt, int n4) {
 }
 
 static int stat_hpsi(he_ctx_t* ctx, double* out, int slot) {
-  OpHpsiR op;
-  op.pot4 = ctx->pot4;
+  OpHpsiR op{};
+  op.s8[0] = ctx->pot4;
   op.out = out;
   op.h2o2m = ctx->fn.h2o2m4;
   return run_stencil_red(ctx, ctx->g2, (const double*)ctx->psi, op, slot);
@@ -1084,8 +1087,9 @@ int he_steprk(he_ctx_t* ctx, double deltat) {
   const double brun[4] = {2.0, 1.0, 1.0, 2.0};
   const double crun[4] = {0.5, 1.0 - r2, 1.0 + r2, 0.5};
   for (int jr = 0; jr < 4; ++jr) {
-    OpRK op;
-    op.pot4 = ctx->pot4; op.uimp = ctx->uimp;
+    OpRK op{};
+    op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
+    op.s16[0] = (const double2*)ctx->q;
     op.q = (double2*)ctx->q;
     op.out = (double2*)(jr == 0 ? ctx->psiold[2] : ctx->scratch);
     op.hsave = jr == 0 ? (double2*)ctx->hpsiold[1] : nullptr;
@@ -1124,12 +1128,15 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "steppc is a dynamics routine");
   const double c112 = 112.0 / 121.0, c9 = 9.0 / 121.0, c4o3 = 4.0 / 3.0;
   {
-    OpPredict op;
-    op.pot4 = ctx->pot4; op.uimp = ctx->uimp;
+    OpPredict op{};
+    op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
     op.po3 = (double2*)ctx->psiold[ctx->ioldp[2] - 1];
-    op.h1 = (const double2*)ctx->hpsiold[ctx->ioldh[0] - 1];
     op.h2 = (double2*)ctx->hpsiold[ctx->ioldh[1] - 1];
     op.pc = (double2*)ctx->pc;
+    op.s16[0] = op.po3;
+    op.s16[1] = (const double2*)ctx->hpsiold[ctx->ioldh[0] - 1];
+    op.s16[2] = op.h2;
+    op.s16[3] = op.pc;
     op.den = ctx->den;
     op.tm = timec_view(ctx);
     op.h2o2m = ctx->fn.h2o2m4;
@@ -1147,12 +1154,13 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   }
   TRY(field_eval(ctx));
   {
-    OpCorrect op;
-    op.pot4 = ctx->pot4; op.uimp = ctx->uimp;
-    op.po3 = (const double2*)ctx->psiold[ctx->ioldp[2] - 1];
-    op.po2 = (const double2*)ctx->psiold[ctx->ioldp[1] - 1];
-    op.h1 = (const double2*)ctx->hpsiold[ctx->ioldh[0] - 1];
-    op.h2 = (const double2*)ctx->hpsiold[ctx->ioldh[1] - 1];
+    OpCorrect op{};
+    op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
+    op.s16[0] = (const double2*)ctx->psiold[ctx->ioldp[2] - 1];
+    op.s16[1] = (const double2*)ctx->psiold[ctx->ioldp[1] - 1];
+    op.s16[2] = (const double2*)ctx->hpsiold[ctx->ioldh[0] - 1];
+    op.s16[3] = (const double2*)ctx->hpsiold[ctx->ioldh[1] - 1];
+    op.s16[4] = (const double2*)ctx->pc;
     op.pc = (double2*)ctx->pc;
     op.out = (double2*)ctx->scratch;
     op.den = ctx->den;
@@ -1189,14 +1197,16 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
 int he_energy(he_ctx_t* ctx, he_energies_t* out) {
   if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode == HE_MODE_DYNAMICS) {
-    OpEnergy<double2> op;
-    op.den = ctx->den; op.dencg = ctx->dencg; op.delj4 = ctx->delj4; op.uimp = ctx->uimp;
+    OpEnergy<double2> op{};
+    op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->uimp;
+    op.has_u = 1;
     op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
     op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
     TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_EN));
   } else {
-    OpEnergy<double> op;
-    op.den = ctx->den; op.dencg = ctx->dencg; op.delj4 = ctx->delj4; op.uimp = nullptr;
+    OpEnergy<double> op{};
+    op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->den;
+    op.has_u = 0;
     op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
     op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
     TRY(run_stencil_red(ctx, ctx->g1, (const double*)ctx->psi, op, S_EN));
@@ -1245,7 +1255,7 @@ int he_derden(he_ctx_t* ctx) {
     TRY(dalloc_t(ctx, &ctx->dyden, ctx->N));
     TRY(dalloc_t(ctx, &ctx->dzden, ctx->N));
   }
-  OpDerden op;
+  OpDerden op{};
   op.gx = ctx->dxden; op.gy = ctx->dyden; op.gz = ctx->dzden;
   return run_stencil(ctx, ctx->g1, ctx->den, op);
 }

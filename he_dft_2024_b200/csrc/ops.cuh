@@ -34,29 +34,21 @@ HE_D double2 hpsi_rt(double2 dx, double2 dy, double2 dz, double2 c, double pot, 
 struct OpPredict {
   static const char* kname() { return "hpsi_pmc_predict"; }
   using T = double2;
-  static constexpr int NV = 0;
-  const double* pot4;
-  const double* uimp;
+  static constexpr int NV = 0, N8 = 2, N16 = 4;
+  const double* s8[N8];      // pot4, uimp
+  const double2* s16[N16];   // psiold(ioldp(3)), hpsiold(ioldh(1)), hpsiold(ioldh(2)), pc
   double2* po3;
-  const double2* h1;
   double2* h2;
   double2* pc;
   double* den;
   Timec tm;
   double h2o2m, s43, c112;
-  struct In {
-    double pot, u;
-    double2 p3, h1, h2, pc;
-  };
-  HE_D In load(long i) const { return In{pot4[i], uimp[i], po3[i], h1[i], h2[i], pc[i]}; }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               const In& v, double*) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, v.pot, v.u, tm.re(ix, iy, iz), h2o2m);
-    const double2 hh1 = v.h1, hh2 = v.h2;
+               const double* v8, const double2* v16, int vs, double*) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tm.re(ix, iy, iz), h2o2m);
+    const double2 p3 = v16[0], hh1 = v16[vs], hh2 = v16[2 * vs], pcv = v16[3 * vs];
     const double2 t = make_double2(2.0 * s4.x - hh1.x + 2.0 * hh2.x, 2.0 * s4.y - hh1.y + 2.0 * hh2.y);
-    const double2 p3 = v.p3;
     const double2 sto1 = make_double2(p3.x + s43 * t.x, p3.y + s43 * t.y);
-    const double2 pcv = v.pc;
     const double2 pn = make_double2(sto1.x - c112 * pcv.x, sto1.y - c112 * pcv.y);
     pc[i] = sto1;
     h2[i] = s4;
@@ -69,31 +61,21 @@ struct OpPredict {
 struct OpCorrect {
   static const char* kname() { return "hpsi_pmc_correct"; }
   using T = double2;
-  static constexpr int NV = 1;
-  const double* pot4;
-  const double* uimp;
-  const double2* po3;
-  const double2* po2;
-  const double2* h1;
-  const double2* h2;
+  static constexpr int NV = 1, N8 = 2, N16 = 5;
+  const double* s8[N8];      // pot4, uimp
+  const double2* s16[N16];   // psiold(ioldp(3)), psiold(ioldp(2)), hpsiold(ioldh(1)), (ioldh(2)), pc
   double2* pc;
   double2* out;
   double* den;
   Timec tm;
   double h2o2m, s3, c9;
-  struct In {
-    double pot, u;
-    double2 p3, p2, h1, h2, pc;
-  };
-  HE_D In load(long i) const { return In{pot4[i], uimp[i], po3[i], po2[i], h1[i], h2[i], pc[i]}; }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               const In& v, double* acc) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, v.pot, v.u, tm.re(ix, iy, iz), h2o2m);
-    const double2 a3 = v.p3, a2 = v.p2, b1 = v.h1, b2 = v.h2;
+               const double* v8, const double2* v16, int vs, double* acc) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tm.re(ix, iy, iz), h2o2m);
+    const double2 a3 = v16[0], a2 = v16[vs], b1 = v16[2 * vs], b2 = v16[3 * vs], p = v16[4 * vs];
     const double2 inner = make_double2(s4.x + 2.0 * b1.x - b2.x, s4.y + 2.0 * b1.y - b2.y);
     const double2 s5 = make_double2(0.125 * (9.0 * a3.x - a2.x + s3 * inner.x),
                                     0.125 * (9.0 * a3.y - a2.y + s3 * inner.y));
-    const double2 p = v.pc;
     const double2 pn = make_double2(p.x - s5.x, p.y - s5.y);
     pc[i] = pn;
     const double2 o = make_double2(s5.x + c9 * pn.x, s5.y + c9 * pn.y);
@@ -107,24 +89,19 @@ struct OpCorrect {
 struct OpRK {
   static const char* kname() { return "hpsi_rkgill_stage"; }
   using T = double2;
-  static constexpr int NV = 0;
-  const double* pot4;
-  const double* uimp;
+  static constexpr int NV = 0, N8 = 2, N16 = 1;
+  const double* s8[N8];      // pot4, uimp
+  const double2* s16[N16];   // q
   double2* q;
   double2* out;
   double2* hsave;
   double* den;
   Timec tm;
   double h2o2m, a, b, cc, dt;
-  struct In {
-    double pot, u;
-    double2 q;
-  };
-  HE_D In load(long i) const { return In{pot4[i], uimp[i], q[i]}; }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               const In& v, double*) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, v.pot, v.u, tm.re(ix, iy, iz), h2o2m);
-    const double2 qq = v.q;
+               const double* v8, const double2* v16, int vs, double*) const {
+    const double2 s4 = hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tm.re(ix, iy, iz), h2o2m);
+    const double2 qq = v16[0];
     const double2 s1 = make_double2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
     q[i] = make_double2(qq.x + 3.0 * s1.x - cc * s4.x, qq.y + 3.0 * s1.y - cc * s4.y);
     if (hsave) hsave[i] = s4;
@@ -141,26 +118,21 @@ template <typename TT>
 struct OpEnergy {
   static const char* kname() { return "energy_reduce"; }
   using T = TT;
-  static constexpr int NV = 5;
-  const double* den;
-  const double* dencg;
-  const double* delj4;
-  const double* uimp;  // may be null (statics)
+  static constexpr int NV = 5, N8 = 4, N16 = 0;
+  const double* s8[N8];      // den, dencg, delj4, uimp (den again when there is no uimp)
+  const double2* s16[1];
   double aux1, aux2, beta, den_m;
-  int lsolid;
+  int lsolid, has_u;
   HE_D static double n2(double v) { return v * v; }
   HE_D static double n2(double2 v) { return v.x * v.x + v.y * v.y; }
-  struct In {
-    double den, dcg, dlj, u;
-  };
-  HE_D In load(long i) const { return In{den[i], dencg[i], delj4[i], uimp ? uimp[i] : 0.0}; }
-  HE_D void at(int, int, int, long, T dx, T dy, T dz, T, const In& v, double* acc) const {
-    const double a3 = v.den, a4 = v.dcg;
+  HE_D void at(int, int, int, long, T dx, T dy, T dz, T, const double* v8, const double2*, int vs,
+               double* acc) const {
+    const double a3 = v8[0], a4 = v8[vs];
     acc[0] += n2(dx) + n2(dy) + n2(dz);
-    acc[1] += v.dlj * a3;
+    acc[1] += v8[2 * vs] * a3;
     acc[2] += a3 * a4 * a4 * (aux1 + aux2 * a4);
     if (lsolid) acc[3] += a3 * (1.0 + tanh(beta * (a3 - den_m)));
-    acc[4] += v.u * a3;
+    if (has_u) acc[4] += v8[3 * vs] * a3;
   }
 };
 
@@ -168,14 +140,14 @@ struct OpEnergy {
 struct OpDerden {
   static const char* kname() { return "derden"; }
   using T = double;
-  static constexpr int NV = 0;
+  static constexpr int NV = 0, N8 = 0, N16 = 0;
+  const double* s8[1];
+  const double2* s16[1];
   double* gx;
   double* gy;
   double* gz;
-  struct In {};
-  HE_D In load(long) const { return In{}; }
-  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double, const In&,
-               double*) const {
+  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double, const double*,
+               const double2*, int, double*) const {
     gx[i] = dx;
     gy[i] = dy;
     gz[i] = dz;
@@ -215,10 +187,11 @@ struct OpImpField {
   int n, npot;
   double delinter, rmax;
   double xmax, ymax, zmax, hx, hy, hz;
-  struct In {};
-  HE_D In load(long) const { return In{}; }
+  static constexpr int N8 = 0, N16 = 0;
+  const double* s8[1];
+  const double2* s16[1];
   HE_D void at(int ix, int iy, int iz, long i, double dx, double dy, double dz, double,
-               const In&, double* acc) const {
+               const double*, const double2*, int, double* acc) const {
     const double x = -xmax + hx * ix, y = -ymax + hy * iy, z = -zmax + hz * iz;
     double u = 0.0;
 #pragma unroll
@@ -399,17 +372,14 @@ __global__ void k_imp_correct(ImpDev* s, double dt) {
 struct OpHpsiR {
   static const char* kname() { return "statics_hpsi"; }
   using T = double;
-  static constexpr int NV = 1;
-  const double* pot4;
+  static constexpr int NV = 1, N8 = 1, N16 = 0;
+  const double* s8[N8];      // pot4
+  const double2* s16[1];
   double* out;
   double h2o2m;
-  struct In {
-    double pot;
-  };
-  HE_D In load(long i) const { return In{pot4[i]}; }
-  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double c, const In& v,
-               double* acc) const {
-    const double h = -((dx + dy) + dz) * h2o2m + v.pot * c;
+  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double c, const double* v8,
+               const double2*, int, double* acc) const {
+    const double h = -((dx + dy) + dz) * h2o2m + v8[0] * c;
     out[i] = h;
     acc[0] += c * h;
   }

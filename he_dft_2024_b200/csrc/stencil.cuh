@@ -11,11 +11,12 @@
 // and marches through a chunk of z.  Each thread keeps f(x,y,z-6..z+6) of its column in registers
 // (the z derivative); the CTA stages the current plane with its 6-point x/y halo in shared memory
 // (the x and y derivatives).  While plane z is being consumed, the next plane is already in
-// flight: its halo by cp.async into the other half of a double-buffered tile (zero-filled
-// outside the grid for icon=13), its z+7 column value and the consumer's pointwise operands by
-// register prefetch.  Every field value is read from HBM once per chunk; halo re-reads hit L2.
-// The consumer ('Op') receives the three derivatives, the centre value and its prefetched
-// operands and does the fused pointwise work (H psi, predictor/corrector, reductions).
+// flight: its halo and the consumer's pointwise operands by cp.async into the other half of
+// double-buffered shared-memory stages (the halo zero-filled outside the grid for icon=13), and
+// its z+7 column value by register prefetch.  Every field value is read from HBM once per chunk;
+// halo re-reads hit L2.
+// The consumer ('Op') receives the three derivatives, the centre value and its staged operands
+// and does the fused pointwise work (H psi, predictor/corrector, reductions).
 #pragma once
 #include "common.cuh"
 
@@ -106,20 +107,39 @@ __device__ void reduce_tail(const ReduceTail& rt, long nb) {
 // Op interface:
 //   using T;                      field element type (double or double2)
 //   static constexpr int NV;      number of FP64 block reductions (0 = none)
-//   struct In;                    the pointwise operands of one grid point
-//   HE_D In load(long idx) const; issue their loads (prefetched one plane ahead)
-//   HE_D void at(int ix,int iy,int iz,long idx,T dx,T dy,T dz,T c,const In&,double* acc) const;
+//   static constexpr int N8, N16; number of real / complex pointwise operand fields
+//   const double* s8[N8]; const double2* s16[N16];  the operand fields (set by the host)
+//   HE_D void at(int ix,int iy,int iz,long idx,T dx,T dy,T dz,T c,const double* v8,
+//                const double2* v16,int vs,double* acc) const;
+//   where v8[k*vs] and v16[k*vs] are this point's operands of field k (staged in shared memory).
+// Minimum resident CTAs per SM for a stencil instantiation (caps registers at 64K/(256*m)).
+template <typename T>
+constexpr int stencil_min_blocks() {
+  return sizeof(T) == 16 ? 2 : 3;
+}
+
+// Dynamic shared memory of one stencil CTA: the double-buffered halo tile and the
+// double-buffered operand stages.
 template <class Op, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY)
+HE_HD constexpr size_t stencil_smem() {
+  return 2 * (size_t)(TY + 12) * (TX + 12) * sizeof(typename Op::T) +
+         2 * (size_t)Op::N16 * TX * TY * sizeof(double2) + 2 * (size_t)Op::N8 * TX * TY * sizeof(double);
+}
+
+template <class Op, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY, stencil_min_blocks<typename Op::T>())
     k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
               const ReduceTail rt) {
   using T = typename Op::T;
-  using In = typename Op::In;
   constexpr int NT = TX * TY;
   constexpr int NH = 12 * (TX + TY);       // halo elements per plane
   constexpr int HK = (NH + NT - 1) / NT;   // halo elements per thread
   constexpr int NV = Op::NV > 0 ? Op::NV : 1;
-  __shared__ __align__(16) T tile[2][TY + 12][TX + 12];
+  constexpr int TILE = (TY + 12) * (TX + 12);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tiles = reinterpret_cast<T*>(smem_raw);                                     // [2][TILE]
+  double2* st16 = reinterpret_cast<double2*>(smem_raw + 2 * TILE * sizeof(T));  // [2][N16][NT]
+  double* st8 = reinterpret_cast<double*>(st16 + 2 * Op::N16 * NT);             // [2][N8][NT]
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + TX * ty;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -129,77 +149,103 @@ __global__ void __launch_bounds__(TX* TY)
   const bool inside = (ix < g.nx) && (iy < g.ny);
   const long plane = (long)g.nx * g.ny;
   const long idx0 = (long)min(ix, g.nx - 1) + (long)g.nx * min(iy, g.ny - 1);
+  const bool anti = (g.icon == 18), wrap = (g.icon != 13);
 
-  // This thread's halo elements: shared-memory slot and grid position.
-  int hsy[HK], hsx[HK];
+  // This thread's halo elements: shared-memory slot, in-plane offset and x/y boundary status
+  // (resolved once; only the z part changes per plane).
+  int hslot[HK];
+  long hoff[HK];
+  bool hok[HK], hneg[HK];
 #pragma unroll
   for (int k = 0; k < HK; ++k) {
     const int e = tid + k * NT;
+    int sy = -1, sx = 0;
     if (e < 12 * TY) {  // x halo: 6 columns each side of the TY rows
       const int r = e / 12, c = e - r * 12;
-      hsy[k] = r + 6;
-      hsx[k] = (c < 6) ? c : TX + c;
+      sy = r + 6;
+      sx = (c < 6) ? c : TX + c;
     } else if (e < NH) {  // y halo: 6 rows each side of the TX columns
       const int e2 = e - 12 * TY;
       const int r = e2 / TX, c = e2 - r * TX;
-      hsy[k] = (r < 6) ? r : TY + r;
-      hsx[k] = c + 6;
-    } else {
-      hsy[k] = -1;
-      hsx[k] = 0;
+      sy = (r < 6) ? r : TY + r;
+      sx = c + 6;
     }
+    hslot[k] = (sy < 0) ? -1 : sy * (TX + 12) + sx;
+    int gx = x0 + sx - 6, gy = y0 + sy - 6, gz = 0;
+    bool neg = false;
+    hok[k] = (sy >= 0) && resolve_bc(g, gx, gy, gz, neg);
+    hneg[k] = neg;
+    hoff[k] = (long)gx + (long)g.nx * gy;
   }
-  auto issue_halo = [&](int buf, int iz) {
+  // Resolve plane index iz: false for a zero plane (icon=13), else the wrapped plane and sign.
+  auto zplane = [&](int iz, int& zz, bool& zneg) -> bool {
+    zneg = false;
+    zz = iz;
+    if (!wrap) return iz >= 0 && iz < g.nz;
+    if (zz < 0) { zz += g.nz; zneg = anti; } else if (zz >= g.nz) { zz -= g.nz; zneg = anti; }
+    zz = min(max(zz, 0), g.nz - 1);
+    return true;
+  };
+  // Plane iz's halo and this thread's operands into stage buf (one cp.async group).
+  auto issue_plane = [&](int buf, int iz) {
+    int zz;
+    bool zneg;
+    const bool zok = zplane(iz, zz, zneg);
+    T* tb = tiles + buf * TILE;
 #pragma unroll
     for (int k = 0; k < HK; ++k) {
-      if (hsy[k] < 0) continue;
-      int gx = x0 + hsx[k] - 6, gy = y0 + hsy[k] - 6, gz = iz;
-      bool neg;
-      const bool ok = resolve_bc(g, gx, gy, gz, neg);
-      const T* src = ok ? f + (long)gx + (long)g.nx * ((long)gy + (long)g.ny * gz) : f;
-      cp_async_elem(&tile[buf][hsy[k]][hsx[k]], src, ok);
+      if (hslot[k] < 0) continue;
+      const bool ok = zok && hok[k];
+      cp_async_elem(tb + hslot[k], ok ? f + hoff[k] + plane * zz : f, ok);
     }
+    const long pi = idx0 + plane * iz;
+#pragma unroll
+    for (int k = 0; k < Op::N16; ++k)
+      cp_async_elem(st16 + (buf * Op::N16 + k) * NT + tid, op.s16[k] + pi, true);
+#pragma unroll
+    for (int k = 0; k < Op::N8; ++k)
+      cp_async_elem(st8 + (buf * Op::N8 + k) * NT + tid, op.s8[k] + pi, true);
     cp_async_commit();
   };
-  // Antiperiodic wrap: negate this thread's wrapped halo elements once they have landed.
   auto fix_halo_sign = [&](int buf, int iz) {
-    if (g.icon != 18) return;
+    if (!anti) return;
+    int zz;
+    bool zneg;
+    zplane(iz, zz, zneg);
+    T* tb = tiles + buf * TILE;
 #pragma unroll
-    for (int k = 0; k < HK; ++k) {
-      if (hsy[k] < 0) continue;
-      int gx = x0 + hsx[k] - 6, gy = y0 + hsy[k] - 6, gz = iz;
-      bool neg;
-      resolve_bc(g, gx, gy, gz, neg);
-      if (neg) tile[buf][hsy[k]][hsx[k]] = neg_if(tile[buf][hsy[k]][hsx[k]], true);
-    }
+    for (int k = 0; k < HK; ++k)
+      if (hslot[k] >= 0 && (hneg[k] ^ zneg)) tb[hslot[k]] = neg_if(tb[hslot[k]], true);
+  };
+  auto column = [&](int iz) -> T {  // f at (ix, iy, iz) under the boundary condition
+    int zz;
+    bool zneg;
+    if (!inside || !zplane(iz, zz, zneg)) return zero_of(T());
+    return neg_if(f[idx0 + plane * zz], zneg);
   };
 
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
 
-  // Prologue: z-queue f(z0-6 .. z0+5), the next column value f(z0+6), plane z0's halo and
-  // operands.
+  // Prologue: z-queue f(z0-6 .. z0+5), the next column value f(z0+6) and plane z0's stage.
   T q[13];
 #pragma unroll
-  for (int m = 0; m < 12; ++m)
-    q[m + 1] = inside ? load_bc(f, g, ix, iy, z0 - 6 + m) : zero_of(T());
-  T qn = inside ? load_bc(f, g, ix, iy, z0 + 6) : zero_of(T());
-  issue_halo(0, z0);
-  In cur = op.load(idx0 + plane * z0);
+  for (int m = 0; m < 12; ++m) q[m + 1] = column(z0 - 6 + m);
+  T qn = column(z0 + 6);
+  issue_plane(0, z0);
 
   for (int iz = z0; iz < z1; ++iz) {
     const int b = (iz - z0) & 1;
+    T* tb = tiles + b * TILE;
 #pragma unroll
     for (int m = 0; m < 12; ++m) q[m] = q[m + 1];
     q[12] = qn;
     // Centre of plane iz: from the queue (threads past the grid edge stage the boundary value).
-    tile[b][ty + 6][tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
-    In nxt = cur;
+    tb[(ty + 6) * (TX + 12) + tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
     if (iz + 1 < z1) {
-      issue_halo(b ^ 1, iz + 1);
-      if (inside) qn = load_bc(f, g, ix, iy, iz + 7);
-      nxt = op.load(idx0 + plane * (iz + 1));
+      issue_plane(b ^ 1, iz + 1);
+      qn = column(iz + 7);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -210,19 +256,19 @@ __global__ void __launch_bounds__(TX* TY)
       T dx = zero_of(T()), dy = zero_of(T()), dz = zero_of(T());
       if (g.axis_on[0]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tile[b][ty + 6][tx + m], dx);
+        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tb[(ty + 6) * (TX + 12) + tx + m], dx);
       }
       if (g.axis_on[1]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tile[b][ty + m][tx + 6], dy);
+        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tb[(ty + m) * (TX + 12) + tx + 6], dy);
       }
       if (g.axis_on[2]) {
 #pragma unroll
         for (int m = 0; m < 13; ++m) dz = axpy(g.w[2][m], q[m], dz);
       }
-      op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], cur, acc);
+      op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
+            st16 + b * Op::N16 * NT + tid, NT, acc);
     }
-    cur = nxt;
     __syncthreads();
   }
   if constexpr (Op::NV > 0) {
