@@ -125,6 +125,9 @@ def load():
         "he_varmu": (ip, [vp, ip, d, dp]),
         "he_timing": (ip, [vp, ip]),
         "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
+        "he_energy_noalloc": (ip, [ctypes.POINTER(HeGrid), ctypes.POINTER(HeFunctional), ip, vp,
+                                   vp, vp, vp, vp, vp, ctypes.POINTER(HeEnergies),
+                                   ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -238,7 +238,7 @@ HE_D double pair_dpot(const ImpDev& s, double r) {
 }
 
 // forceimp: F(k,c) = -sum(d_c den * uimp_k)*dxyz + sum_m F_ij(k,m,c)  (potenimp.f90:40-58).
-__global__ void k_imp_force(ImpDev* s, const double* sums, double dxyz) {
+static __global__ void k_imp_force(ImpDev* s, const double* sums, double dxyz) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int n = s->n;
   for (int k = 0; k < n; ++k)
@@ -255,7 +255,7 @@ __global__ void k_imp_force(ImpDev* s, const double* sums, double dxyz) {
 }
 
 // aimp = F / m_imp (DFT4He3d.f90:571-573).
-__global__ void k_imp_accel(ImpDev* s) {
+static __global__ void k_imp_accel(ImpDev* s) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int n = s->n;
   for (int k = 0; k < n; ++k)
@@ -263,7 +263,7 @@ __global__ void k_imp_accel(ImpDev* s) {
 }
 
 // Impurity part of one RK-Gill stage (steprk.f90:92-125).
-__global__ void k_imp_rk(ImpDev* s, int jr, double a, double b, double cc, double dt) {
+static __global__ void k_imp_rk(ImpDev* s, int jr, double a, double b, double cc, double dt) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int n = s->n;
   double stor[3 * kMaxImp];
@@ -299,7 +299,7 @@ __global__ void k_imp_rk(ImpDev* s, int jr, double a, double b, double cc, doubl
 
 // Impurity predictor + modifier (steppc.f90:80-99).  The velocity prediction is stored in
 // vimpold(:,:,ioldv(3)) and vimp keeps v_n, as in the reference.
-__global__ void k_imp_predict(ImpDev* s, double dt) {
+static __global__ void k_imp_predict(ImpDev* s, double dt) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int n = s->n;
   const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
@@ -329,7 +329,7 @@ __global__ void k_imp_predict(ImpDev* s, double dt) {
 
 // Impurity corrector (steppc.f90:149-174).  aimp is the value set by the driver before the step
 // (the forceimp inside steppc refreshes F but not aimp), as in the reference.
-__global__ void k_imp_correct(ImpDev* s, double dt) {
+static __global__ void k_imp_correct(ImpDev* s, double dt) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int n = s->n;
   const double c9 = 9.0 / 121.0;

@@ -200,6 +200,25 @@ typedef struct {
 int he_timing(he_ctx_t* ctx, int enable);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
+/* ---- energy sums without device allocation ----
+ * No counterpart in the reference.  For callers that cannot let a library allocate device
+ * memory because all of it belongs to them (a Fortran driver whose arrays live in OpenACC or
+ * CUDA Fortran data regions sized at start-up, a job that reserves the GPU's memory in its own
+ * pool): computes energy()'s He sums (ekin4, elj4, ecor4, esolid, etot4, and eHeX when uimp is
+ * given) from the caller's device arrays psi (complex in HE_MODE_DYNAMICS, real in
+ * HE_MODE_STATICS), den, dencg, delj4 and uimp (may be NULL), in the reference layout.  Calls no
+ * cudaMalloc/cudaFree: the reduction scratch is a fixed 328,000-byte device array inside the
+ * library (room for grids up to 256^3; larger grids return HE_ERR_ARG), held on every GPU that
+ * loads the library until exit.  The first call on a device looks up that array's address (set-up
+ * once per device); make the first call before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU race.  Synchronises `stream` (cudaStream_t, NULL = default);
+ * fills *out (impurity fields other than eHeX/eimpu are zero); on error writes a message to
+ * err[errlen] when given. */
+int he_energy_noalloc(const he_grid_t* grid, const he_functional_t* fun, int mode,
+                      const void* psi, const double* den, const double* dencg,
+                      const double* delj4, const double* uimp, void* stream,
+                      he_energies_t* out, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
