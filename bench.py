@@ -277,6 +277,7 @@ def run_ours(args):
     rep = ctx.timing_report()
     ctx.timing(False)
     tot = sum(v[1] for v in rep.values())
+    tiles = ctx.tuned_tiles()
     bpp = kernel_bytes_per_point(w.nx)
     top = max(rep.items(), key=lambda kv: kv[1][1])
     name, (nl, kms) = top
@@ -311,6 +312,7 @@ def run_ours(args):
         "step_alg_bytes_per_point": 744.0,
         "step_roofline_frac": (744.0 * N * args.steps / (t_max / ws)) / 1e9 / peak,
         "kernels": breakdown,
+        "fft_tiles_xyz": list(tiles),
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu:

@@ -124,6 +124,7 @@ def load():
         "he_steppcr": (ip, [vp, d, dp, dp, ip, dp]),
         "he_varmu": (ip, [vp, ip, d, dp]),
         "he_timing": (ip, [vp, ip]),
+        "he_tuned_tiles": (ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
         "he_energy_noalloc": (ip, [ctypes.POINTER(HeGrid), ctypes.POINTER(HeFunctional), ip, vp,
                                    vp, vp, vp, vp, vp, ctypes.POINTER(HeEnergies),

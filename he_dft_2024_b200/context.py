@@ -84,6 +84,12 @@ class Context:
         return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].ms))
                 for i in range(min(n.value, 64))}
 
+    def tuned_tiles(self):
+        """FFT tile sizes (x, y, z) chosen by the context's autotuner."""
+        v = [ctypes.c_int(0) for _ in range(3)]
+        self._ck(self.L.he_tuned_tiles(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
     def synchronize(self):
         self._ck(self.L.he_synchronize(self.h))
 

@@ -25,8 +25,11 @@ namespace he {
 
 enum XMode { X_R2C_DEN = 0, X_R2C_CORR = 1, X_C2R2 = 2, X_C2R2_CORR = 3, X_C2R_POT = 4 };
 
-// Rows per x-pass CTA and kx columns per y/z-pass CTA (host and device agree on these).
+// Rows per x-pass CTA and kx columns per y/z-pass CTA for the run-time-length kernels (the
+// compile-time kernels take the tile as a template parameter, 16 or 8, picked per context by
+// the autotuner; a CTA has 16 threads per tile line).
 HE_HD constexpr int tile_rows(int n) { return n <= 256 ? 16 : 8; }
+HE_HD constexpr int tile_threads(int tile) { return tile * 16; }
 // Line stride in shared memory: the line length rounded up to a multiple of 8, plus one (odd, so
 // the transposing gathers of consecutive lines spread over the banks).
 HE_HD constexpr int line_stride(int n) { return ((n + 7) / 8) * 8 + 1; }
@@ -73,13 +76,13 @@ HE_D double2 split_r2c(const double2* L, int k, int n, bool second) {
   return make_double2(0.5 * (z.y - zc.y), -0.5 * (z.x - zc.x));
 }
 
-template <int MODE, int N>
-__global__ void __launch_bounds__(256) k_xpass(const XArgs a) {
+template <int MODE, int N, int TILE>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
   extern __shared__ double2 smem[];
   const int n = (N > 0) ? N : a.nx;
   const int nxh = n / 2 + 1;
   const int ls = line_stride(n);
-  const int RB = (N > 0) ? tile_rows(N) : a.rb;
+  const int RB = (N > 0) ? TILE : a.rb;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const long r0 = (long)blockIdx.x * RB;
   double2* tw = smem;
@@ -177,12 +180,12 @@ struct YZArgs {
   const double* k2;          // null: single kernel
 };
 
-template <int N>
-__global__ void __launch_bounds__(256) k_ypass(const YZArgs a) {
+template <int N, int TILE>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
   extern __shared__ double2 smem[];
   const int n = (N > 0) ? N : a.ny;
   const int ls = line_stride(n);
-  const int TK = (N > 0) ? tile_rows(N) : a.tkx;
+  const int TK = (N > 0) ? TILE : a.tkx;
   const int nxh = a.nxh;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;
@@ -207,12 +210,12 @@ __global__ void __launch_bounds__(256) k_ypass(const YZArgs a) {
   }
 }
 
-template <int N>
-__global__ void __launch_bounds__(256) k_zconv(const YZArgs a) {
+template <int N, int TILE>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a) {
   extern __shared__ double2 smem[];
   const int n = (N > 0) ? N : a.nz;
   const int ls = line_stride(n);
-  const int TK = (N > 0) ? tile_rows(N) : a.tkx;
+  const int TK = (N > 0) ? TILE : a.tkx;
   const int nxh = a.nxh;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;

@@ -62,6 +62,7 @@ struct he_ctx {
   // FFT
   LinePlan plx{}, ply{}, plz{};
   int x_rb = 16, tkx = 16;
+  int tile_x = 16, tile_y = 16, tile_z = 16;  // autotuned tile variants (16 or 8 lines)
   size_t smem_x = 0, smem_y = 0, smem_z = 0;
   // k space
   double2 *fden = nullptr, *wA = nullptr, *wB = nullptr;
@@ -325,12 +326,12 @@ static XArgs xargs(he_ctx_t* ctx) {
 static size_t fft_smem(const LinePlan& pl, int lines, int nbuf) {
   return sizeof(double2) * (((size_t)pl.stw_len + 1) / 2 * 2 + (size_t)nbuf * lines * line_stride(pl.n));
 }
-static bool x_fast(const he_ctx_t* ctx) {
+static bool x_fast(const he_ctx_t* ctx, int tile) {
   switch (ctx->nx) {
 #define HE_CASE(N) case N:
     HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
-    return ((long)ctx->ny * ctx->nz) % tile_rows(ctx->nx) == 0;
+    return ((long)ctx->ny * ctx->nz) % tile == 0;
     default: return false;
   }
 }
@@ -344,39 +345,45 @@ static bool yz_fast(int n) {
   }
 }
 
-template <int MODE, int N>
+// Tile variants of the compile-time kernels: 16 lines per CTA (256 threads) or 8 (128 threads).
+// he_ctx_create times both for each pass family on the context's grid and keeps the faster.
+template <int MODE, int N, int TILE>
 static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
-  const int rb = (N > 0) ? tile_rows(N) : a.rb;
+  const int rb = (N > 0) ? TILE : a.rb;
   const unsigned nb = (unsigned)((a.rows + rb - 1) / rb);
   const size_t smem = fft_smem(ctx->plx, rb, 2);
+  const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   static const char* names[5] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
                                  "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4"};
-  CK(cudaFuncSetAttribute(k_xpass<MODE, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, names[MODE]);
-  k_xpass<MODE, N><<<nb, 256, smem, ctx->stream>>>(a);
+  k_xpass<MODE, N, TILE><<<nb, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
 template <int MODE>
 static int xpass(he_ctx_t* ctx, const XArgs& a) {
-  if (x_fast(ctx)) {
+  const int tile = ctx->tile_x;
+  if (x_fast(ctx, tile)) {
     switch (ctx->nx) {
-#define HE_CASE(N) case N: return xpass_n<MODE, N>(ctx, a);
+#define HE_CASE(N) \
+  case N: return tile == 8 ? xpass_n<MODE, N, 8>(ctx, a) : xpass_n<MODE, N, 16>(ctx, a);
       HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
     }
   }
-  return xpass_n<MODE, 0>(ctx, a);
+  return xpass_n<MODE, 0, 16>(ctx, a);
 }
 
-template <int N>
+template <int N, int TILE>
 static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
-  const int tk = (N > 0) ? tile_rows(N) : ctx->tkx;
+  const int tk = (N > 0) ? TILE : ctx->tkx;
   const size_t smem = fft_smem(ctx->ply, tk, 2);
+  const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->nz, narr);
-  CK(cudaFuncSetAttribute(k_ypass<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_ypass<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, "fft_y");
-  k_ypass<N><<<grid, 256, smem, ctx->stream>>>(a);
+  k_ypass<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
@@ -387,24 +394,27 @@ static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
   a.arr[0] = a0; a.arr[1] = a1 ? a1 : a0;
   a.inv = inv;
   const int narr = a1 ? 2 : 1;
+  const int tile = ctx->tile_y;
   if (yz_fast(ctx->ny)) {
     switch (ctx->ny) {
-#define HE_CASE(N) case N: return ypass_n<N>(ctx, a, narr);
+#define HE_CASE(N) \
+  case N: return tile == 8 ? ypass_n<N, 8>(ctx, a, narr) : ypass_n<N, 16>(ctx, a, narr);
       HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
     }
   }
-  return ypass_n<0>(ctx, a, narr);
+  return ypass_n<0, 16>(ctx, a, narr);
 }
 
-template <int N>
+template <int N, int TILE>
 static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
-  const int tk = (N > 0) ? tile_rows(N) : ctx->tkx;
+  const int tk = (N > 0) ? TILE : ctx->tkx;
   const size_t smem = fft_smem(ctx->plz, tk, 3);
+  const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
-  CK(cudaFuncSetAttribute(k_zconv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_zconv<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
-  k_zconv<N><<<grid, 256, smem, ctx->stream>>>(a);
+  k_zconv<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
@@ -414,14 +424,16 @@ static int zconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, co
   a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
   a.pl = ctx->plz;
   a.io = io; a.out2 = out2; a.fden_out = fden_out; a.k1 = k1; a.k2 = k2;
+  const int tile = ctx->tile_z;
   if (yz_fast(ctx->nz)) {
     switch (ctx->nz) {
-#define HE_CASE(N) case N: return zconv_n<N>(ctx, a);
+#define HE_CASE(N) \
+  case N: return tile == 8 ? zconv_n<N, 8>(ctx, a) : zconv_n<N, 16>(ctx, a);
       HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
     }
   }
-  return zconv_n<0>(ctx, a);
+  return zconv_n<0, 16>(ctx, a);
 }
 
 // fden = R2C(den); wA <- fden*wcgk and wB <- fden*fvlj4 back in (x-transformed) row space.
@@ -724,6 +736,52 @@ static int read_sums(he_ctx_t* ctx) {
   return HE_OK;
 }
 
+// Tile autotuner: times the 16-line and 8-line variants of each FFT pass family on this
+// context's grid (zero-filled work arrays, one warm-up and three timed launches each) and keeps
+// the faster.  Runs once in he_ctx_create.
+static int autotune_tiles(he_ctx_t* ctx) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto timed = [&](int (*fn)(he_ctx_t*), float* ms) -> int {
+    TRY(fn(ctx));
+    CK(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < 3; ++r) TRY(fn(ctx));
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return HE_OK;
+  };
+  auto pick = [&](int* knob, int (*fn)(he_ctx_t*)) -> int {
+    float t16 = 0.0f, t8 = 0.0f;
+    *knob = 16;
+    TRY(timed(fn, &t16));
+    *knob = 8;
+    TRY(timed(fn, &t8));
+    *knob = (t8 < t16) ? 8 : 16;
+    return HE_OK;
+  };
+  int st = HE_OK;
+  if (x_fast(ctx, 16) && x_fast(ctx, 8))
+    st = pick(&ctx->tile_x, [](he_ctx_t* c) -> int {
+      XArgs a = xargs(c);
+      a.specA = c->wA; a.specB = c->wB; a.den = c->den;
+      a.out1 = c->dencg; a.out2 = c->delj4;
+      return xpass<X_C2R2_CORR>(c, a);
+    });
+  if (st == HE_OK && yz_fast(ctx->ny))
+    st = pick(&ctx->tile_y, [](he_ctx_t* c) -> int { return ypass(c, c->wA, c->wB, true); });
+  if (st == HE_OK && yz_fast(ctx->nz))
+    st = pick(&ctx->tile_z, [](he_ctx_t* c) -> int {
+      return zconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, nullptr);
+    });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st == HE_OK) CK(cudaMemsetAsync(ctx->wA, 0, 16 * ctx->Nk, ctx->stream));
+  if (st == HE_OK) CK(cudaMemsetAsync(ctx->wB, 0, 16 * ctx->Nk, ctx->stream));
+  return st;
+}
+
 // ------------------------------------------------------------------------------------------------
 // C-ABI
 // ------------------------------------------------------------------------------------------------
@@ -840,6 +898,7 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   TRY(dalloc_t(ctx, &ctx->counter, 1));
   TRY(dalloc_t(ctx, &ctx->sums, S_COUNT));
   CK(cudaMallocHost(&ctx->hsum, S_COUNT * sizeof(double)));
+  TRY(autotune_tiles(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   return HE_OK;
 }
@@ -1058,7 +1117,7 @@ int he_forceimp(he_ctx_t* ctx, double* F) {
   // rimp; redo it if either changed since.
   if (!ctx->force_fresh) TRY(he_potenimp(ctx));
   tname(ctx, "impurity_force");
-  k_imp_force<<<1, 32, 0, ctx->stream>>>(ctx->imp, ctx->sums + S_FORCE, ctx->dxyz);
+  k_imp_force<<<1, 128, 0, ctx->stream>>>(ctx->imp, ctx->sums + S_FORCE, ctx->dxyz);
   LAUNCHED();
   if (F) {
     ImpDev h;
@@ -1073,7 +1132,7 @@ int he_set_accel(he_ctx_t* ctx) {
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "dynamics routine");
   if (ctx->n_imp == 0) return HE_OK;
   tname(ctx, "impurity_accel");
-  k_imp_accel<<<1, 32, 0, ctx->stream>>>(ctx->imp);
+  k_imp_accel<<<1, 128, 0, ctx->stream>>>(ctx->imp);
   LAUNCHED();
   return HE_OK;
 }
@@ -1113,7 +1172,7 @@ int he_steprk(he_ctx_t* ctx, double deltat) {
     ctx->force_fresh = false;
     if (ctx->n_imp > 0) {
       tname(ctx, "impurity_rk");
-      k_imp_rk<<<1, 32, 0, ctx->stream>>>(ctx->imp, jr, arun[jr], brun[jr], crun[jr], deltat);
+      k_imp_rk<<<1, 128, 0, ctx->stream>>>(ctx->imp, jr, arun[jr], brun[jr], crun[jr], deltat);
       LAUNCHED();
     }
     if (jr <= 2) TRY(field_eval(ctx));
@@ -1149,7 +1208,7 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   ctx->force_fresh = false;
   if (ctx->n_imp > 0) {
     tname(ctx, "impurity_predict");
-    k_imp_predict<<<1, 32, 0, ctx->stream>>>(ctx->imp, deltat);
+    k_imp_predict<<<1, 128, 0, ctx->stream>>>(ctx->imp, deltat);
     LAUNCHED();
   }
   TRY(field_eval(ctx));
@@ -1178,7 +1237,7 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   ctx->force_fresh = false;
   if (ctx->n_imp > 0) {
     tname(ctx, "impurity_correct");
-    k_imp_correct<<<1, 32, 0, ctx->stream>>>(ctx->imp, deltat);
+    k_imp_correct<<<1, 128, 0, ctx->stream>>>(ctx->imp, deltat);
     LAUNCHED();
   }
   if (errHe || errimp || errvimp) {
@@ -1452,6 +1511,14 @@ int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n) {
   }
   *n = (int)agg.size();
   for (int i = 0; i < (int)agg.size() && i < max; ++i) out[i] = agg[i];
+  return HE_OK;
+}
+
+int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z) {
+  if (!ctx || !x || !y || !z) return HE_ERR_ARG;
+  *x = ctx->tile_x;
+  *y = ctx->tile_y;
+  *z = ctx->tile_z;
   return HE_OK;
 }
 

@@ -176,6 +176,11 @@ struct ImpDev {
 // den: uimp = sum_k V_k(|r-R_k|) by linear interpolation of the potenimpini table, and
 // acc[3k+c] = sum d_c(den) * V_k.  Off-table radii set lstopimp (potenimp.f90:104-109); the
 // radius is clamped to the table end and the index is taken after the clamp.
+// The table index is int(r/DelInter) with the rounded IEEE quotient and the fraction is
+// mod(r,DelInter)/DelInter with the exact remainder, as in the reference: when r/DelInter rounds
+// up to an integer k although the exact quotient is below k, the reference takes bin k with a
+// fraction of ~1 (it interpolates one bin further out), and so does this kernel.  The remainder
+// r - i0*DelInter is one exact fma when i0 is the exact floor, else r - (i0-1)*DelInter.
 template <int NI>
 struct OpImpField {
   static const char* kname() { return "impurity_field_force"; }
@@ -193,11 +198,12 @@ struct OpImpField {
   HE_D void at(int ix, int iy, int iz, long i, double dx, double dy, double dz, double,
                const double*, const double2*, int, double* acc) const {
     const double x = -xmax + hx * ix, y = -ymax + hy * iy, z = -zmax + hz * iz;
+    const double* __restrict__ rp = imp->rimp;
     double u = 0.0;
 #pragma unroll
     for (int k = 0; k < NI; ++k) {
       if (k < n) {
-        const double rx = imp->rimp[k], ry = imp->rimp[k + n], rz = imp->rimp[k + 2 * n];
+        const double rx = __ldg(rp + k), ry = __ldg(rp + k + n), rz = __ldg(rp + k + 2 * n);
         const double zt = (z - rz) * (z - rz);
         const double yt = (y - ry) * (y - ry) + zt;
         double r = sqrt((x - rx) * (x - rx) + yt);
@@ -206,15 +212,13 @@ struct OpImpField {
           r = rmax;
         }
         int i0 = (int)(r / delinter);
-        // mod(r,DelInter) is exact: r - q*DelInter with q = trunc(r/DelInter) taken exactly.
-        // One fma gives that value exactly whenever the rounded quotient i0 equals q (the
-        // remainder is then representable); otherwise fall back to fmod.
         double rm = fma(-(double)i0, delinter, r);
-        if (rm < 0.0 || rm >= delinter) rm = fmod(r, delinter);
+        if (rm < 0.0) rm = fma(-(double)(i0 - 1), delinter, r);
+        else if (rm >= delinter) rm = fmod(r, delinter);
         if (i0 > npot - 2) i0 = npot - 2;
         const double rmod = rm / delinter;
-        const double* t = tab + (long)k * npot;
-        const double uk = t[i0] * (1.0 - rmod) + t[i0 + 1] * rmod;
+        const double* __restrict__ t = tab + (long)k * npot;
+        const double uk = __ldg(t + i0) * (1.0 - rmod) + __ldg(t + i0 + 1) * rmod;
         u = u + uk;
         acc[3 * k + 0] += dx * uk;
         acc[3 * k + 1] += dy * uk;
@@ -224,6 +228,21 @@ struct OpImpField {
     uimp[i] = u;
   }
 };
+
+// The impurity kernels run on one CTA: the ImpDev struct is copied into shared memory by the
+// whole CTA, updated by thread 0 (the integrator is a few dozen scalars), and copied back.
+HE_D void imp_stage_in(ImpDev* dst, const ImpDev* src) {
+  const unsigned* a = reinterpret_cast<const unsigned*>(src);
+  unsigned* b = reinterpret_cast<unsigned*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(ImpDev) / 4); i += blockDim.x) b[i] = a[i];
+  __syncthreads();
+}
+HE_D void imp_stage_out(ImpDev* dst, const ImpDev* src) {
+  __syncthreads();
+  const unsigned* a = reinterpret_cast<const unsigned*>(src);
+  unsigned* b = reinterpret_cast<unsigned*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(ImpDev) / 4); i += blockDim.x) b[i] = a[i];
+}
 
 HE_D double pair_pot(const ImpDev& s, double r) {
   if (s.ii_kind == 0) return (r < s.ii_rcut) ? s.ii_umax : 0.0;
@@ -238,8 +257,7 @@ HE_D double pair_dpot(const ImpDev& s, double r) {
 }
 
 // forceimp: F(k,c) = -sum(d_c den * uimp_k)*dxyz + sum_m F_ij(k,m,c)  (potenimp.f90:40-58).
-static __global__ void k_imp_force(ImpDev* s, const double* sums, double dxyz) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+HE_D void imp_force_body(ImpDev* s, const double* sums, double dxyz) {
   const int n = s->n;
   for (int k = 0; k < n; ++k)
     for (int c = 0; c < 3; ++c) s->F[k + n * c] = -sums[3 * k + c] * dxyz;
@@ -253,18 +271,28 @@ static __global__ void k_imp_force(ImpDev* s, const double* sums, double dxyz) {
       for (int c = 0; c < 3; ++c) s->F[k + n * c] = s->F[k + n * c] + (-dv * d[c] / a1);
     }
 }
+static __global__ void k_imp_force(ImpDev* g, const double* sums, double dxyz) {
+  __shared__ ImpDev st;
+  imp_stage_in(&st, g);
+  if (threadIdx.x == 0) imp_force_body(&st, sums, dxyz);
+  imp_stage_out(g, &st);
+}
 
 // aimp = F / m_imp (DFT4He3d.f90:571-573).
-static __global__ void k_imp_accel(ImpDev* s) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+HE_D void imp_accel_body(ImpDev* s) {
   const int n = s->n;
   for (int k = 0; k < n; ++k)
     for (int c = 0; c < 3; ++c) s->aimp[k + n * c] = s->F[k + n * c] / s->m[k];
 }
+static __global__ void k_imp_accel(ImpDev* g) {
+  __shared__ ImpDev st;
+  imp_stage_in(&st, g);
+  if (threadIdx.x == 0) imp_accel_body(&st);
+  imp_stage_out(g, &st);
+}
 
 // Impurity part of one RK-Gill stage (steprk.f90:92-125).
-static __global__ void k_imp_rk(ImpDev* s, int jr, double a, double b, double cc, double dt) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+HE_D void imp_rk_body(ImpDev* s, int jr, double a, double b, double cc, double dt) {
   const int n = s->n;
   double stor[3 * kMaxImp];
   for (int i = 0; i < 3 * n; ++i) {
@@ -296,11 +324,16 @@ static __global__ void k_imp_rk(ImpDev* s, int jr, double a, double b, double cc
     for (int i = 0; i < 2; ++i) s->iolda[i] = i + 1;
   }
 }
+static __global__ void k_imp_rk(ImpDev* g, int jr, double a, double b, double cc, double dt) {
+  __shared__ ImpDev st;
+  imp_stage_in(&st, g);
+  if (threadIdx.x == 0) imp_rk_body(&st, jr, a, b, cc, dt);
+  imp_stage_out(g, &st);
+}
 
 // Impurity predictor + modifier (steppc.f90:80-99).  The velocity prediction is stored in
 // vimpold(:,:,ioldv(3)) and vimp keeps v_n, as in the reference.
-static __global__ void k_imp_predict(ImpDev* s, double dt) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+HE_D void imp_predict_body(ImpDev* s, double dt) {
   const int n = s->n;
   const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
   const double sd = c4o3 * dt;
@@ -326,11 +359,16 @@ static __global__ void k_imp_predict(ImpDev* s, double dt) {
   s->iolda[1] = s->iolda[0];
   s->iolda[0] = t;
 }
+static __global__ void k_imp_predict(ImpDev* g, double dt) {
+  __shared__ ImpDev st;
+  imp_stage_in(&st, g);
+  if (threadIdx.x == 0) imp_predict_body(&st, dt);
+  imp_stage_out(g, &st);
+}
 
 // Impurity corrector (steppc.f90:149-174).  aimp is the value set by the driver before the step
 // (the forceimp inside steppc refreshes F but not aimp), as in the reference.
-static __global__ void k_imp_correct(ImpDev* s, double dt) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+HE_D void imp_correct_body(ImpDev* s, double dt) {
   const int n = s->n;
   const double c9 = 9.0 / 121.0;
   const double s3 = 3.0 * dt;
@@ -365,6 +403,12 @@ static __global__ void k_imp_correct(ImpDev* s, double dt) {
   s->ioldv[2] = s->ioldv[1];
   s->ioldv[1] = s->ioldv[0];
   s->ioldv[0] = t;
+}
+static __global__ void k_imp_correct(ImpDev* g, double dt) {
+  __shared__ ImpDev st;
+  imp_stage_in(&st, g);
+  if (threadIdx.x == 0) imp_correct_body(&st, dt);
+  imp_stage_out(g, &st);
 }
 
 // ---- statics (real psi) ------------------------------------------------------------------------

@@ -198,6 +198,9 @@ typedef struct {
   double ms;
 } he_kernel_time_t;
 int he_timing(he_ctx_t* ctx, int enable);
+/* Tile sizes (lines per CTA, 16 or 8) the context's autotuner chose for the x, y and z FFT
+ * passes at creation. */
+int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
 /* ---- energy sums without device allocation ----

@@ -77,6 +77,38 @@ def test_poten_matches_oracle(n, icon):
         assert rel(ctx.download("fden").ravel(order="F"), o.get("fden")) < 1e-12
 
 
+def test_potenimp_matches_oracle_including_rounded_bins():
+    """uimp and F against the oracle.  The geometry contains radii r whose quotient r/DelInter
+    rounds up to an integer k while the exact quotient is below k (e.g. r = 7.8 A with
+    DelInter = 0.025 A): the reference then interpolates from bin k with a fraction ~1
+    (int(r/DelInter) with mod(r,DelInter), Dynamics_TDDFT/potenimp.f90:102,111), one bin further
+    out than the exact floor would; the device path must do the same."""
+    from fractions import Fraction
+    w = small_dyn(n=32, n_imp=1)
+    _, npot, d, _ = C.potion_table(w)
+    x, y, z = C.grid_axes(w)
+    rx, ry, rz = w.rimp0[0]
+    quirk = 0
+    for xi in x:
+        for yi in y:
+            for zi in z:
+                r = float(np.sqrt((xi - rx) ** 2 + ((yi - ry) ** 2 + (zi - rz) ** 2)))
+                if int(r / d) != int(Fraction(r) / Fraction(d)):
+                    quirk += 1
+    o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u)
+    den = C.woods_saxon(w)
+    o.set("den", den)
+    o.potenimp(); o.poten(); o.forceimp()
+    with Context(w) as ctx:
+        oracle_kernels(ctx, o)
+        ctx.upload("den", den)
+        ctx.potenimp(); ctx.poten()
+        F = ctx.forceimp(want=True)
+        assert rel(ctx.download("uimp").ravel(order="F"), o.get("uimp")) < 1e-14
+    np.testing.assert_allclose(F.ravel(order="F"), o.get("F"), rtol=1e-11, atol=1e-14)
+    assert quirk > 0  # the geometry does exercise the rounded-bin case
+
+
 def run_dynamics(w, steps, side):
     den0 = C.woods_saxon(w)
     psi0 = D.initial_wavefunction(w, den0, kick=(0.0, 0.0, 0.05))
