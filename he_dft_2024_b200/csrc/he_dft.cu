@@ -62,6 +62,7 @@ struct he_ctx {
   // FFT
   LinePlan plx{}, ply{}, plz{};
   int x_rb = 16, tkx = 16;
+  int num_sms = 148;
   int tile_x = 16, tile_y = 16, tile_z = 16;  // autotuned tile variants (16 or 8 lines)
   size_t smem_x = 0, smem_y = 0, smem_z = 0;
   // k space
@@ -275,16 +276,42 @@ static ReduceTail tail(he_ctx_t* ctx, int slot) {
   return r;
 }
 
+// z-chunk of a stencil launch.  A CTA marches one x-y tile through `zc` planes after a
+// 12-plane prologue; the grid is (x tiles) x (y tiles) x ceil(nz/zc).  The chunk minimises
+// waves x (zc + 6): waves = ceil(CTAs / (SMs x resident CTAs per SM)), and the prologue costs
+// about half a step per plane.  The resident-CTA count is the kernel's occupancy, queried once
+// per kernel and device.
+static int choose_zc(const he_ctx_t* ctx, int occ) {
+  const long tiles = (long)((ctx->nx + kTX - 1) / kTX) * ((ctx->ny + kTY - 1) / kTY);
+  const long slots = (long)ctx->num_sms * (occ > 0 ? occ : 1);
+  int best = ctx->nz, bestcost = 1 << 30;
+  for (int zc = 4; zc <= ctx->nz; ++zc) {
+    const long ctas = tiles * ((ctx->nz + zc - 1) / zc);
+    const long waves = (ctas + slots - 1) / slots;
+    const int cost = (int)(waves * (zc + 6));
+    if (cost < bestcost) { bestcost = cost; best = zc; }
+  }
+  return std::max(1, std::min(best, ctx->nz));
+}
+
 template <class Op>
-static int run_stencil(he_ctx_t* ctx, const StencilGeom& g, const typename Op::T* f, const Op& op,
+static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::T* f, const Op& op,
                        int slot = -1) {
+  constexpr size_t smem = stencil_smem<Op, kTX, kTY>();
+  static int occ = -1;  // resident CTAs per SM of this instantiation
+  if (occ < 0) {
+    CK(cudaFuncSetAttribute(k_stencil<Op, kTX, kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<Op, kTX, kTY>, kTX * kTY, smem));
+  }
+  StencilGeom g = g0;
+  g.zc = choose_zc(ctx, occ);
   dim3 grid = stencil_grid(ctx, g), block(kTX, kTY);
   ReduceTail rt{};
   if (Op::NV > 0) {
     TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
     rt = tail(ctx, slot);
   }
-  constexpr size_t smem = stencil_smem<Op, kTX, kTY>();
   CK(cudaFuncSetAttribute(k_stencil<Op, kTX, kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)smem));
   tname(ctx, Op::kname());
@@ -840,6 +867,11 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   make_geom(ctx, 2, &ctx->g2);
   *out = ctx;
 
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
   if (e != cudaSuccess)
     return fail(ctx, HE_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
@@ -892,7 +924,9 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
     TRY(dalloc_t(ctx, &ctx->t4, N));
     TRY(dalloc_t(ctx, &ctx->timec, N));
   }
-  dim3 sg = stencil_grid(ctx, ctx->g2);
+  StencilGeom g4 = ctx->g2;
+  g4.zc = 4;  // the smallest z-chunk choose_zc can pick
+  dim3 sg = stencil_grid(ctx, g4);
   ctx->partials_cap = std::max((size_t)sg.x * sg.y * sg.z, (size_t)kPwBlocks) * (3 * kMaxImp);
   TRY(dalloc_t(ctx, &ctx->partials, ctx->partials_cap));
   TRY(dalloc_t(ctx, &ctx->counter, 1));
