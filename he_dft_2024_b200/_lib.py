@@ -15,14 +15,16 @@ LIB_PATH = os.path.join(PKG, "libhedft.so")
 HEADER = os.path.join(ROOT, "include", "he_dft.h")
 
 HE_OK, HE_ERR_ARG, HE_ERR_CUDA, HE_ERR_STATE, HE_ERR_NOMEM = 0, 1, 2, 3, 4
-HE_MODE_DYNAMICS, HE_MODE_STATICS = 0, 1
+HE_MODE_DYNAMICS, HE_MODE_STATICS, HE_MODE_QUANTUM = 0, 1, 2
+HE_MAX_QIMP = 4
 HE_PREC_F64 = 0
 
 FIELDS = dict(
     psi=0, den=1, pot4=2, dencg=3, delj4=4, uimp=5, fden=6, pc=7, q=8, psiold1=9, psiold2=10,
     psiold3=11, hpsiold1=12, hpsiold2=13, dxden=14, dyden=15, dzden=16, hpsi=17, fvlj4=18,
     wcgk=19, rimp=20, vimp=21, aimp=22, F=23, rimpold=24, vimpold=25, aimpold=26, pcr=27, pcv=28,
-    qr=29, qv=30, ring=31)
+    qr=29, qv=30, ring=31, psix=32, upotx=33, potx4=34, denx=35, pcx=36, qx=37, psixold=38,
+    hpsixold=39, uimpk=40, uimpkk=41)
 
 
 class HeGrid(ctypes.Structure):
@@ -54,6 +56,22 @@ class HeImpurities(ctypes.Structure):
                 ("ii_kind", ctypes.c_int),
                 ("ii_D", ctypes.c_double), ("ii_re", ctypes.c_double), ("ii_a", ctypes.c_double),
                 ("ii_rcut", ctypes.c_double), ("ii_umax", ctypes.c_double)]
+
+
+class HePairPot(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("D", ctypes.c_double), ("re", ctypes.c_double),
+                ("a", ctypes.c_double), ("rcut", ctypes.c_double), ("umax", ctypes.c_double)]
+
+
+class HeQImpurities(ctypes.Structure):
+    _fields_ = [("n_imp", ctypes.c_int),
+                ("m_imp_u", ctypes.POINTER(ctypes.c_double)),
+                ("mu4", ctypes.c_double),
+                ("he_x", HePairPot * HE_MAX_QIMP),
+                ("x_x", HePairPot * (HE_MAX_QIMP * HE_MAX_QIMP)),
+                ("uimp_k", ctypes.POINTER(ctypes.c_double)),
+                ("uimp_k_k", ctypes.POINTER(ctypes.c_double)),
+                ("n_spline", ctypes.c_int), ("nq", ctypes.c_int), ("parabolic", ctypes.c_int)]
 
 
 class HeEnergies(ctypes.Structure):
@@ -126,6 +144,10 @@ def load():
         "he_timing": (ip, [vp, ip]),
         "he_tuned_tiles": (ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
+        "he_set_quantum_impurities": (ip, [vp, ctypes.POINTER(HeQImpurities)]),
+        "he_qimp_moments": (ip, [vp, dp]),
+        "he_ft_v_spline_table": (ip, [ctypes.POINTER(HePairPot), d, d, ip, ip, dp, ip,
+                                      ctypes.c_char_p, ctypes.c_size_t]),
         "he_energy_noalloc": (ip, [ctypes.POINTER(HeGrid), ctypes.POINTER(HeFunctional), ip, vp,
                                    vp, vp, vp, vp, vp, ctypes.POINTER(HeEnergies),
                                    ctypes.c_char_p, ctypes.c_size_t]),

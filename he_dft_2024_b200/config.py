@@ -69,6 +69,17 @@ class Workload:
     ii_umax: float = 0.0
     rimp0: Tuple[Tuple[float, float, float], ...] = ()
     vimp0_aps: Tuple[Tuple[float, float, float], ...] = ()   # A/ps, as in imp.input
+    # quantum impurities (Dynamics_quantum_impurities): the He-X kernel is FT_V_spline of the
+    # pot_* pair potential, the X-X kernel of the ii_* one ('null' = kind 0)
+    nq_imp: int = 0
+    mq_imp_u: Tuple[float, ...] = ()
+    mu4: float = 0.0          # chemical-potential shift of H psi (0 unless Lbulk)
+    nq: int = 1000            # potenimpini's Nq (modules.f90:165); effective max(10001, nq)
+    n_spline: int = 100001    # N_FT_V_spline (FT_V_spline.f90:2)
+    parabolic: int = 0        # Lparabolic_fit_FT_V_spline
+    psix_width: float = 1.5   # Gaussian initial impurity wave function, A
+    psix_center: Tuple[Tuple[float, float, float], ...] = ()
+    psix_kick_aps: Tuple[Tuple[float, float, float], ...] = ()  # impurity velocity, A/ps
     # statics local time step (He_statics/modules.f90:299)
     dtmin: float = 1.0e-10
     sdmu: float = 1.0e-1
@@ -191,3 +202,63 @@ def tddft_5000_256(**kw):
     """4He_5000 on 256^3 (h = 0.5 A), same impurity and step as tddft_1000."""
     return replace(tddft_1000(), name="tddft-4He5000-256^3-classical", nx=256, ny=256, nz=256,
                    xmax=64.0, ymax=64.0, zmax=64.0, n4=5000, **kw)
+
+
+def quantum_2000(n=192, speed_ms=200.0, direction=(0.0, 0.0, 1.0), **kw):
+    """4He_2000 on 192^3 (h = 0.5 A) with one quantum impurity of 23 u (h2o2mx = h2o2m4 *
+    4.002603/23) and the Morse He-X potential; the impurity starts as a normalised Gaussian of
+    width 1.5 A at the droplet centre, kicked by exp(i k.r), k = v*7.63822291/(2 h2o2mx), with
+    speed speed_ms (m/s) along direction."""
+    xm = 48.0 * n / 192
+    d = np.asarray(direction, dtype=np.float64)
+    d = d / np.linalg.norm(d)
+    v = tuple(float(c) for c in d * speed_ms / 100.0)  # m/s -> A/ps
+    return replace(Workload(name=f"tddft-4He2000-{n}^3-quantum", nx=n, ny=n, nz=n, xmax=xm,
+                            ymax=xm, zmax=xm, n4=2000, nq_imp=1, mq_imp_u=(23.0,),
+                            pot_rcut=MORSE_RCUT, pot_umax=MORSE_UMAX,
+                            psix_center=((0.0, 0.0, 0.0),), psix_kick_aps=(v,),
+                            deltatps=1.0e-4, steps=1000), **kw)
+
+
+def quantum_batch(count=16, n=192, seed=1234, **kw):
+    """The batched quantum workload: count trajectories of quantum_2000 whose impurity speeds are
+    U(0, 400) m/s and directions uniform on the sphere (numpy PCG64 seeded with seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        speed = rng.uniform(0.0, 400.0)
+        d = rng.normal(size=3)
+        out.append(quantum_2000(n=n, speed_ms=speed, direction=tuple(d / np.linalg.norm(d)), **kw))
+    return out
+
+
+def psix_initial(w: Workload, k: int = 0):
+    """Impurity k's initial wave function: exp(-|r-c|^2/(2 width^2)) * exp(i kv.r), normalised
+    to 1 (sum |psix|^2 dxyz = 1), kv = v[A/ps]*7.63822291/(2*h2o2mx)."""
+    x, y, z = grid_axes(w)
+    c = w.psix_center[k] if w.psix_center else (0.0, 0.0, 0.0)
+    r2 = ((x[:, None, None] - c[0]) ** 2 + (y[None, :, None] - c[1]) ** 2 +
+          (z[None, None, :] - c[2]) ** 2)
+    f = np.exp(-r2 / (2.0 * w.psix_width ** 2)).astype(np.complex128)
+    if w.psix_kick_aps:
+        h2o2mx = w.h2o2m4 * 4.002603 / w.mq_imp_u[k]
+        kv = np.asarray(w.psix_kick_aps[k], dtype=np.float64) * KTOPS / (2.0 * h2o2mx)
+        ph = kv[0] * x[:, None, None] + kv[1] * y[None, :, None] + kv[2] * z[None, None, :]
+        f = f * np.exp(1j * ph)
+    f /= np.sqrt((np.abs(f) ** 2).sum() * w.dxyz)
+    return np.asfortranarray(f)
+
+
+def pair_rows(w: Workload):
+    """FT_V_spline pair potentials as rows {kind, D, re, a, r_cutoff, umax}: He-X for each quantum
+    impurity and X-X for each ordered pair (i + n*j; i == j and 'null' pairs are kind 0)."""
+    n = w.nq_imp
+    hex_ = np.array([[w.pot_kind, w.pot_D, w.pot_re, w.pot_a, w.pot_rcut, w.pot_umax]] * n,
+                    dtype=np.float64).reshape(n, 6)
+    xx = np.zeros((n * n, 6))
+    for i in range(n):
+        for j in range(n):
+            if i != j and w.ii_kind:
+                xx[i + n * j] = [w.ii_kind, w.ii_D, w.ii_re, w.ii_a, w.ii_rcut, w.ii_umax]
+    return hex_, xx
+

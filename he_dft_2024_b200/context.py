@@ -14,13 +14,16 @@ from ._lib import FIELDS, HeError, dptr
 from .config import MP_U, KTOPS, Workload, potion_table
 
 COMPLEX_DYN = {"psi", "pc", "q", "psiold1", "psiold2", "psiold3", "hpsiold1", "hpsiold2"}
+COMPLEX_Q = {"psix", "pcx", "qx", "psixold", "hpsixold"}
+MODES = {"dynamics": _lib.HE_MODE_DYNAMICS, "statics": _lib.HE_MODE_STATICS,
+         "quantum": _lib.HE_MODE_QUANTUM}
 
 
 class Context:
     def __init__(self, w: Workload, mode="dynamics", compute_kernels=True):
         self.L = _lib.load()
         self.w = w
-        self.mode = _lib.HE_MODE_DYNAMICS if mode == "dynamics" else _lib.HE_MODE_STATICS
+        self.mode = MODES[mode]
         g = _lib.HeGrid(w.nx, w.ny, w.nz, w.xmax, w.ymax, w.zmax, w.npd, w.icon)
         core = {"OT": b"OT ", "OP": b"OP ", "OTC": b"OTC"}[w.core]
         f = _lib.HeFunctional(core, w.h4, w.eps4, w.sigma4, w.cp4, w.cpp4, w.den4c, w.alphas,
@@ -35,12 +38,14 @@ class Context:
             raise HeError(st, msg)
         if compute_kernels:
             self._ck(self.L.he_compute_kernels(self.h))
-        if self.mode == _lib.HE_MODE_DYNAMICS:
+        if self.mode != _lib.HE_MODE_STATICS:
             ab = _lib.HeAbsorber(w.lambdah, w.txmean, w.txsurf, w.tymean, w.tysurf, w.tzmean,
                                  w.tzsurf)
             self._ck(self.L.he_set_absorber(self.h, ctypes.byref(ab)))
-            if w.n_imp > 0:
-                self.set_impurities(w)
+        if self.mode == _lib.HE_MODE_DYNAMICS and w.n_imp > 0:
+            self.set_impurities(w)
+        if self.mode == _lib.HE_MODE_QUANTUM and w.nq_imp > 0:
+            self.set_quantum_impurities(w)
 
     # ---- plumbing -------------------------------------------------------------------------------
     def _ck(self, st):
@@ -108,10 +113,22 @@ class Context:
             return (w.n_imp, 3, 2)
         if name == "ring":
             return (13,)
+        n = w.nq_imp
+        if name in ("psix", "upotx", "pcx", "qx"):
+            return (w.nx, w.ny, w.nz, n)
+        if name == "psixold":
+            return (w.nx, w.ny, w.nz, 3, n)
+        if name == "hpsixold":
+            return (w.nx, w.ny, w.nz, 2, n)
+        if name == "uimpk":
+            return (w.nx // 2 + 1, w.ny, w.nz, n)
+        if name == "uimpkk":
+            return (w.nx // 2 + 1, w.ny, w.nz, n, n)
         return (w.nx, w.ny, w.nz)
 
     def _is_complex(self, name):
-        return name == "fden" or (self.mode == _lib.HE_MODE_DYNAMICS and name in COMPLEX_DYN)
+        return (name == "fden" or name in COMPLEX_Q or
+                (self.mode != _lib.HE_MODE_STATICS and name in COMPLEX_DYN))
 
     def upload(self, name, arr):
         dt = np.complex128 if self._is_complex(name) else np.float64
@@ -146,6 +163,39 @@ class Context:
         if w.vimp0_aps:
             # imp.input gives A/ps; the driver converts to A K (DFT4He3d.f90:313)
             self.upload("vimp", np.array(w.vimp0_aps, dtype=np.float64) * KTOPS)
+
+    def set_quantum_impurities(self, w: Workload, uimp_k=None, uimp_k_k=None):
+        """he_set_quantum_impurities: masses, mu4 and the He-X / X-X pair potentials of the
+        workload; uimp_k / uimp_k_k host tables replace the device FT_V_spline when given."""
+        from .config import pair_rows
+        n = w.nq_imp
+        hex_, xx = pair_rows(w)
+        q = _lib.HeQImpurities()
+        q.n_imp = n
+        self._mq = np.ascontiguousarray(np.asarray(w.mq_imp_u, np.float64))
+        q.m_imp_u = dptr(self._mq)
+        q.mu4 = w.mu4
+        for i in range(n):
+            q.he_x[i] = _lib.HePairPot(int(hex_[i, 0]), *hex_[i, 1:])
+            for j in range(n):
+                r = xx[i + n * j]
+                q.x_x[i + n * j] = _lib.HePairPot(int(r[0]), *r[1:])
+        self._uk = self._ukk = None
+        if uimp_k is not None:
+            self._uk = np.ascontiguousarray(np.asarray(uimp_k, np.float64).ravel(order="F"))
+            q.uimp_k = dptr(self._uk)
+        if uimp_k_k is not None:
+            self._ukk = np.ascontiguousarray(np.asarray(uimp_k_k, np.float64).ravel(order="F"))
+            q.uimp_k_k = dptr(self._ukk)
+        q.n_spline, q.nq, q.parabolic = w.n_spline, w.nq, w.parabolic
+        self._ck(self.L.he_set_quantum_impurities(self.h, ctypes.byref(q)))
+
+    def qimp_moments(self):
+        """(N_imp, 4): norm, <x>, <y>, <z> of each impurity density."""
+        n = self.w.nq_imp
+        out = np.zeros(4 * n)
+        self._ck(self.L.he_qimp_moments(self.h, dptr(out)))
+        return out.reshape(n, 4)
 
     # ---- Dynamics_TDDFT routines ----------------------------------------------------------------
     def poten(self):
@@ -218,3 +268,18 @@ class Context:
 
 def mass_of(w: Workload):
     return np.asarray(w.m_imp_u, np.float64) * MP_U
+
+
+def ft_v_spline_table(pot, pmax, hp, n_spline=100001, parabolic=0):
+    """FT_V_spline's momentum table V(i*hp), i < int(pmax/hp + 1.5), computed on the device."""
+    L = _lib.load()
+    n_p = int(pmax / hp + 1.5)
+    out = np.zeros(n_p)
+    err = ctypes.create_string_buffer(256)
+    pp = _lib.HePairPot(int(pot[0]), *[float(v) for v in pot[1:6]])
+    st = L.he_ft_v_spline_table(ctypes.byref(pp), pmax, hp, n_spline, parabolic, dptr(out), n_p,
+                                err, 256)
+    if st != 0:
+        raise HeError(st, err.value.decode())
+    return out
+

@@ -11,7 +11,9 @@
 //     X_R2C_CORR   spectrum of den*dencg*(cp4+cpp4*dencg)                          (:166-168)
 //     X_C2R2       dencg = C2R(A)*renor, delj4 = C2R(B)*renor                      (:142,:154)
 //     X_C2R2_CORR  the same, then the R2C of the correlation source into A         (:166-171)
-//     X_C2R_POT    sto1 = C2R(A)*renor, penalty, pot4 assembly                     (:178-218)
+//     X_C2R_POT    sto1 = C2R(A)*renor, penalty, pot4 assembly (+ potx4 of the quantum
+//                  impurities when extra is set)                                   (:178-218)
+//     X_C2R1       out1 = C2R(A)*renor (rows 2p, 2p+1 packed in one line)
 // y/z pass (k_ypass, k_zconv): CTA = TKX consecutive kx of one pencil family, staged transposed
 //   in shared memory (odd line stride to spread banks).  The z pass does forward z, the k-space
 //   multiply by one or two real kernels (wcgk, fvlj4), and the inverse z, and can store the
@@ -23,7 +25,7 @@
 
 namespace he {
 
-enum XMode { X_R2C_DEN = 0, X_R2C_CORR = 1, X_C2R2 = 2, X_C2R2_CORR = 3, X_C2R_POT = 4 };
+enum XMode { X_R2C_DEN = 0, X_R2C_CORR = 1, X_C2R2 = 2, X_C2R2_CORR = 3, X_C2R_POT = 4, X_C2R1 = 5 };
 
 // Rows per x-pass CTA and kx columns per y/z-pass CTA for the run-time-length kernels (the
 // compile-time kernels take the tile as a template parameter, 16 or 8, picked per context by
@@ -46,6 +48,7 @@ struct XArgs {
   const double2* specB;
   double* out1;              // dencg  (C2R2*) or pot4 (C2R_POT)
   double* out2;              // delj4  (C2R2*)
+  const double* extra;       // C2R_POT: potx4 added after the correlation term (null: none)
   double renor, cp4, cpp4, a0, a1;
   int lsolid;
   double C, beta, den_m;
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
     return;
   }
 
-  if constexpr (MODE == X_C2R_POT) {
+  if constexpr (MODE == X_C2R_POT || MODE == X_C2R1) {
     // rows 2p and 2p+1 share complex line p
     for (int e = tid; e < (RB / 2) * n; e += nthr) {
       const int p = e / n, k = e - p * n;
@@ -154,8 +157,13 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
       const long g = (r0 + row) * n + x;
       const double2 z = R[(row >> 1) * ls + sw<N>(x)];
       const double sto1 = ((row & 1) ? z.y : z.x) * a.renor;
+      if constexpr (MODE == X_C2R1) {
+        a.out1[g] = sto1;
+        continue;
+      }
       const double dc = a.dencg_in[g];
       double pot = a.delj4_in[g] + dc * dc * (a.a0 + a.a1 * dc) + sto1;
+      if (a.extra) pot = pot + a.extra[g];
       if (a.lsolid) {
         const double d = a.den[g];
         const double t = tanh(a.beta * (d - a.den_m));

@@ -19,6 +19,7 @@
 #include "fft_kernels.cuh"
 #include "ops.cuh"
 #include "setup.cuh"
+#include "quantum.cuh"
 
 using namespace he;
 
@@ -39,7 +40,12 @@ enum Slot {
   S_VARMU = 44,
   S_HMEAN0 = 45,
   S_STAT_PC = 46,   // k_stat_correct writes {sum |pc|, sum psi^2} to slots 46, 47
-  S_COUNT = 64
+  S_ERRX = 48,      // quantum: sum |pcx_i|, kMaxQImp slots
+  S_QEK = 52,       // quantum: sum |grad psix_i|^2, kMaxQImp slots
+  S_QHEX = 56,      // quantum: sum sto2*den (eHeX)
+  S_QII = 57,       // quantum: impurity-pair sums (eimpu_impu), 6 slots
+  S_QMOM = 64,      // quantum: moments, 4 per impurity
+  S_COUNT = 96
 };
 
 }  // namespace
@@ -87,6 +93,16 @@ struct he_ctx {
   size_t pot_tab_cap = 0;
   double delinter = 0.0, rmaxinterpol = 0.0;
   bool force_fresh = false;
+  // quantum impurities (HE_MODE_QUANTUM); psixold[i][s-1] is Fortran slot s of impurity i
+  int nq = 0;
+  double mu4 = 0.0, h2o2mx[kMaxQImp] = {};
+  void *psix[kMaxQImp] = {}, *pcx[kMaxQImp] = {}, *qx[kMaxQImp] = {}, *xscratch = nullptr;
+  void *psixold[kMaxQImp][3] = {}, *hpsixold[kMaxQImp][2] = {};
+  double *denx[kMaxQImp] = {}, *upotx[kMaxQImp] = {}, *uimpk[kMaxQImp] = {};
+  double* uimpkk[kMaxQImp * kMaxQImp] = {};  // (i,j) at i + kMaxQImp*j; null = no kernel
+  double* potx4 = nullptr;
+  double2 *wC = nullptr, *wD = nullptr, *sx[kMaxQImp] = {};
+  bool cglj_pending = false;  // wA/wB hold fden*wcgk, fden*fvlj4 of the current fden (x,y domain)
   // reductions
   double* partials = nullptr;
   size_t partials_cap = 0;
@@ -380,8 +396,8 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   const unsigned nb = (unsigned)((a.rows + rb - 1) / rb);
   const size_t smem = fft_smem(ctx->plx, rb, 2);
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
-  static const char* names[5] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
-                                 "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4"};
+  static const char* names[6] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
+                                 "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4", "fft_x_c2r"};
   CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, names[MODE]);
   k_xpass<MODE, N, TILE><<<nb, nthr, smem, ctx->stream>>>(a);
@@ -474,8 +490,9 @@ static int spectrum_cg_lj(he_ctx_t* ctx) {
   TRY(ypass(ctx, ctx->wA, ctx->wB, true));
   return HE_OK;
 }
-// Correlation convolution of the spectrum in wA (already x-transformed) and pot4 assembly.
-static int correlation_tail(he_ctx_t* ctx) {
+// Correlation convolution of the spectrum in wA (already x-transformed) and pot4 assembly
+// (extra: potx4 of the quantum impurities, or null).
+static int correlation_tail(he_ctx_t* ctx, const double* extra = nullptr) {
   TRY(ypass(ctx, ctx->wA, nullptr, false));
   TRY(zconv(ctx, ctx->wA, ctx->wcgk, nullptr, nullptr, nullptr));
   TRY(ypass(ctx, ctx->wA, nullptr, true));
@@ -483,12 +500,13 @@ static int correlation_tail(he_ctx_t* ctx) {
   a.specA = ctx->wA;
   a.den = ctx->den; a.dencg_in = ctx->dencg; a.delj4_in = ctx->delj4;
   a.out1 = ctx->pot4;
+  a.extra = extra;
   return xpass<X_C2R_POT>(ctx, a);
 }
 
 // ---- module-array access -----------------------------------------------------------------------
 static size_t wf_elem(const he_ctx_t* ctx) {
-  return ctx->mode == HE_MODE_DYNAMICS ? sizeof(double2) : sizeof(double);
+  return ctx->mode == HE_MODE_STATICS ? sizeof(double) : sizeof(double2);
 }
 
 static int imp_pull(he_ctx_t* ctx, ImpDev* h) {
@@ -812,6 +830,574 @@ static int autotune_tiles(he_ctx_t* ctx) {
 // ------------------------------------------------------------------------------------------------
 // C-ABI
 // ------------------------------------------------------------------------------------------------
+// ------------------------------------------------------------------------------------------------
+// quantum impurities (HE_MODE_QUANTUM, Dynamics_quantum_impurities)
+// ------------------------------------------------------------------------------------------------
+template <int N, int TILE>
+static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a) {
+  const int tk = (N > 0) ? TILE : ctx->tkx;
+  const size_t smem = fft_smem(ctx->plz, tk, 3);
+  const int nthr = (N > 0) ? tile_threads(TILE) : 256;
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
+  CK(cudaFuncSetAttribute(k_zmix<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tname(ctx, a.nout == 0 ? "fft_z_fwd" : a.fwd_in ? "fft_z_mix_fwd" : "fft_z_mix");
+  k_zmix<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
+  LAUNCHED();
+  return HE_OK;
+}
+static int zmix(he_ctx_t* ctx, ZMixArgs a) {
+  a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
+  a.pl = ctx->plz;
+  const int tile = ctx->tile_z;
+  if (yz_fast(ctx->nz)) {
+    switch (ctx->nz) {
+#define HE_CASE(N) \
+  case N: return tile == 8 ? zmix_n<N, 8>(ctx, a) : zmix_n<N, 16>(ctx, a);
+      HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    }
+  }
+  return zmix_n<0, 16>(ctx, a);
+}
+
+// One synthesis output: sum over terms of (spectrum x kernel), inverse-transformed into `out`.
+struct QOut {
+  double* out;
+  int nterm;
+  const double2* src[kMaxTerms];
+  const double* ker[kMaxTerms];
+};
+
+// z synthesis of one or two outputs into wC (and wD), inverse y, and C2R in x.
+static int q_synth(he_ctx_t* ctx, const QOut* o, int nout, const double2* fwd_in) {
+  ZMixArgs z{};
+  z.fwd_in = fwd_in;
+  z.nout = nout;
+  double2* buf[2] = {ctx->wC, ctx->wD};
+  for (int k = 0; k < nout; ++k) {
+    z.out[k] = buf[k];
+    z.nterm[k] = o[k].nterm;
+    for (int t = 0; t < o[k].nterm; ++t) { z.src[k][t] = o[k].src[t]; z.ker[k][t] = o[k].ker[t]; }
+  }
+  TRY(zmix(ctx, z));
+  TRY(ypass(ctx, ctx->wC, nout > 1 ? ctx->wD : nullptr, true));
+  XArgs a = xargs(ctx);
+  a.specA = ctx->wC;
+  a.out1 = o[0].out;
+  if (nout > 1) {
+    a.specB = ctx->wD;
+    a.out2 = o[1].out;
+    return xpass<X_C2R2>(ctx, a);
+  }
+  return xpass<X_C2R1>(ctx, a);
+}
+
+// Forward spectra (x, y, z) of the impurity densities |psix_i|^2 into sx[i].
+static int q_denx_spectra(he_ctx_t* ctx) {
+  XArgs a = xargs(ctx);
+  for (int i = 0; i < ctx->nq; ++i) {
+    a.den = ctx->denx[i];
+    a.specA = ctx->sx[i];
+    TRY(xpass<X_R2C_DEN>(ctx, a));
+  }
+  for (int i = 0; i < ctx->nq; i += 2) TRY(ypass(ctx, ctx->sx[i], i + 1 < ctx->nq ? ctx->sx[i + 1] : nullptr, false));
+  for (int i = 0; i < ctx->nq; ++i) {
+    ZMixArgs z{};
+    z.fwd_in = ctx->sx[i];
+    z.fwd_store = ctx->sx[i];
+    TRY(zmix(ctx, z));
+  }
+  return HE_OK;
+}
+
+// potenimp (Dynamics_quantum_impurities/potenimp.f90:1-43): fden = R2C(den), potx4 and upotx_i.
+// The forward pass of den also leaves fden*wcgk and fden*fvlj4 (x,y domain) in wA/wB for poten.
+static int q_potenimp(he_ctx_t* ctx) {
+  const int n = ctx->nq;
+  XArgs a = xargs(ctx);
+  a.den = ctx->den;
+  a.specA = ctx->wA;
+  TRY(xpass<X_R2C_DEN>(ctx, a));
+  if (n == 1) {
+    a.den = ctx->denx[0];
+    a.specA = ctx->sx[0];
+    TRY(xpass<X_R2C_DEN>(ctx, a));
+    TRY(ypass(ctx, ctx->wA, ctx->sx[0], false));
+  } else {
+    TRY(ypass(ctx, ctx->wA, nullptr, false));
+  }
+  TRY(zconv(ctx, ctx->wA, ctx->wcgk, ctx->wB, ctx->fvlj4, ctx->fden));
+  ctx->cglj_pending = true;
+  if (n == 1) {
+    // potx4 = C2R(R2C(|psix|^2) uimp_k), upotx = C2R(fden uimp_k), fused behind psix's z pass.
+    QOut o[2] = {};
+    o[0].out = ctx->potx4; o[0].nterm = 1; o[0].src[0] = nullptr; o[0].ker[0] = ctx->uimpk[0];
+    o[1].out = ctx->upotx[0]; o[1].nterm = 1; o[1].src[0] = ctx->fden; o[1].ker[0] = ctx->uimpk[0];
+    return q_synth(ctx, o, 2, ctx->sx[0]);
+  }
+  TRY(q_denx_spectra(ctx));
+  // Outputs: potx4 = sum_i sx_i uimp_k_i; upotx_i = fden uimp_k_i + sum_{j != i} sx_j uimp_k_k(i,j).
+  // (The reference sums the C2R of each term in real space; the sums here are taken in k space.)
+  std::vector<QOut> outs(1 + n);
+  outs[0] = QOut{};
+  outs[0].out = ctx->potx4;
+  for (int i = 0; i < n; ++i) {
+    outs[0].src[outs[0].nterm] = ctx->sx[i];
+    outs[0].ker[outs[0].nterm++] = ctx->uimpk[i];
+  }
+  for (int i = 0; i < n; ++i) {
+    QOut& o = outs[1 + i];
+    o = QOut{};
+    o.out = ctx->upotx[i];
+    o.src[o.nterm] = ctx->fden;
+    o.ker[o.nterm++] = ctx->uimpk[i];
+    for (int j = 0; j < n; ++j) {
+      const double* kk = ctx->uimpkk[i + kMaxQImp * j];
+      if (j == i || !kk) continue;
+      o.src[o.nterm] = ctx->sx[j];
+      o.ker[o.nterm++] = kk;
+    }
+  }
+  for (size_t k = 0; k < outs.size(); k += 2) TRY(q_synth(ctx, &outs[k], k + 1 < outs.size() ? 2 : 1, nullptr));
+  return HE_OK;
+}
+
+// poten (Dynamics_quantum_impurities/poten.f90:5-155): dencg, delj4 from fden, then the
+// correlation term and pot4 = delj4 + dencg^2 (cp4/2 + cpp4/3 dencg) + sto1 + potx4 (+ penalty).
+static int q_poten(he_ctx_t* ctx) {
+  if (!ctx->cglj_pending) {
+    ZMixArgs z{};
+    z.nout = 2;
+    z.out[0] = ctx->wA; z.nterm[0] = 1; z.src[0][0] = ctx->fden; z.ker[0][0] = ctx->wcgk;
+    z.out[1] = ctx->wB; z.nterm[1] = 1; z.src[1][0] = ctx->fden; z.ker[1][0] = ctx->fvlj4;
+    TRY(zmix(ctx, z));
+  }
+  ctx->cglj_pending = false;
+  TRY(ypass(ctx, ctx->wA, ctx->wB, true));
+  XArgs a = xargs(ctx);
+  a.specA = ctx->wA; a.specB = ctx->wB;
+  a.den = ctx->den;
+  a.out1 = ctx->dencg; a.out2 = ctx->delj4;
+  TRY(xpass<X_C2R2_CORR>(ctx, a));
+  return correlation_tail(ctx, ctx->potx4);
+}
+
+static int q_field(he_ctx_t* ctx) {
+  TRY(q_potenimp(ctx));
+  return q_poten(ctx);
+}
+
+static int q_cnorm2(he_ctx_t* ctx, int i) {
+  tname(ctx, "impurity_density");
+  k_cnorm2<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double2*)ctx->psix[i], ctx->denx[i], ctx->N);
+  LAUNCHED();
+  return HE_OK;
+}
+
+// steprk (Dynamics_quantum_impurities/steprk.f90:1-124).  He and each impurity take the same
+// RK-Gill stage; the field is re-evaluated after stages 1-3.
+static int q_steprk(he_ctx_t* ctx, double deltat) {
+  const double r2 = 1.0 / std::sqrt(2.0);
+  const double arun[4] = {0.5, 1.0 - r2, 1.0 + r2, 1.0 / 6.0};
+  const double brun[4] = {2.0, 1.0, 1.0, 2.0};
+  const double crun[4] = {0.5, 1.0 - r2, 1.0 + r2, 0.5};
+  for (int jr = 0; jr < 4; ++jr) {
+    auto stage = [&](void*& f, void*& scratch, void* qq, void** po, void** ho, const double* pot,
+                     double mu, double h2o2m, double* dens) -> int {
+      OpRKQ op{};
+      op.s8[0] = pot;
+      op.s16[0] = (const double2*)qq;
+      op.q = (double2*)qq;
+      op.out = (double2*)(jr == 0 ? po[2] : scratch);
+      op.hsave = jr == 0 ? (double2*)ho[1] : nullptr;
+      op.den = dens;
+      op.tm = timec_view(ctx);
+      op.h2o2m = h2o2m;
+      op.mu = mu;
+      op.a = arun[jr]; op.b = brun[jr]; op.cc = crun[jr]; op.dt = deltat;
+      TRY(run_stencil(ctx, ctx->g2, (const double2*)f, op));
+      if (jr == 0) {
+        void* o3 = po[2];
+        po[2] = po[1];
+        po[1] = po[0];
+        po[0] = f;
+        f = o3;
+        std::swap(ho[0], ho[1]);
+      } else {
+        std::swap(f, scratch);
+      }
+      return HE_OK;
+    };
+    TRY(stage(ctx->psi, ctx->scratch, ctx->q, ctx->psiold, ctx->hpsiold, ctx->pot4, ctx->mu4,
+              ctx->fn.h2o2m4, ctx->den));
+    for (int i = 0; i < ctx->nq; ++i)
+      TRY(stage(ctx->psix[i], ctx->xscratch, ctx->qx[i], ctx->psixold[i], ctx->hpsixold[i],
+                ctx->upotx[i], 0.0, ctx->h2o2mx[i], ctx->denx[i]));
+    if (jr <= 2) TRY(q_field(ctx));
+  }
+  for (int i = 0; i < 3; ++i) ctx->ioldp[i] = i + 1;
+  ctx->ioldh[0] = 1; ctx->ioldh[1] = 2;
+  return HE_OK;
+}
+
+// steppc (Dynamics_quantum_impurities/steppc.f90:1-157): predictor + modifier for He and every
+// impurity, potenimp + poten, corrector for all.  The impurities' ring indices ioldpx/ioldhx
+// always equal ioldp/ioldh (both start at 1,2,3 / 1,2 and rotate together), so one set serves.
+static int q_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errpsix) {
+  const double c112 = 112.0 / 121.0, c9 = 9.0 / 121.0, c4o3 = 4.0 / 3.0;
+  auto predict = [&](void*& f, void* pcc, void** po, void** ho, const double* pot, double mu,
+                     double h2o2m, double* dens) -> int {
+    OpPredictQ op{};
+    op.s8[0] = pot;
+    op.po3 = (double2*)po[ctx->ioldp[2] - 1];
+    op.h2 = (double2*)ho[ctx->ioldh[1] - 1];
+    op.pc = (double2*)pcc;
+    op.s16[0] = op.po3;
+    op.s16[1] = (const double2*)ho[ctx->ioldh[0] - 1];
+    op.s16[2] = op.h2;
+    op.s16[3] = op.pc;
+    op.den = dens;
+    op.tm = timec_view(ctx);
+    op.h2o2m = h2o2m;
+    op.mu = mu;
+    op.s43 = c4o3 * deltat;
+    op.c112 = c112;
+    TRY(run_stencil(ctx, ctx->g2, (const double2*)f, op));
+    std::swap(f, po[ctx->ioldp[2] - 1]);
+    return HE_OK;
+  };
+  TRY(predict(ctx->psi, ctx->pc, ctx->psiold, ctx->hpsiold, ctx->pot4, ctx->mu4, ctx->fn.h2o2m4, ctx->den));
+  for (int i = 0; i < ctx->nq; ++i)
+    TRY(predict(ctx->psix[i], ctx->pcx[i], ctx->psixold[i], ctx->hpsixold[i], ctx->upotx[i], 0.0,
+                ctx->h2o2mx[i], ctx->denx[i]));
+  std::swap(ctx->ioldh[0], ctx->ioldh[1]);
+  TRY(q_field(ctx));
+  auto correct = [&](void*& f, void*& scratch, void* pcc, void** po, void** ho, const double* pot,
+                     double mu, double h2o2m, double* dens, int slot) -> int {
+    OpCorrectQ op{};
+    op.s8[0] = pot;
+    op.s16[0] = (const double2*)po[ctx->ioldp[2] - 1];
+    op.s16[1] = (const double2*)po[ctx->ioldp[1] - 1];
+    op.s16[2] = (const double2*)ho[ctx->ioldh[0] - 1];
+    op.s16[3] = (const double2*)ho[ctx->ioldh[1] - 1];
+    op.s16[4] = (const double2*)pcc;
+    op.pc = (double2*)pcc;
+    op.out = (double2*)scratch;
+    op.den = dens;
+    op.tm = timec_view(ctx);
+    op.h2o2m = h2o2m;
+    op.mu = mu;
+    op.s3 = 3.0 * deltat;
+    op.c9 = c9;
+    TRY(run_stencil_red(ctx, ctx->g2, (const double2*)f, op, slot));
+    std::swap(f, scratch);
+    return HE_OK;
+  };
+  TRY(correct(ctx->psi, ctx->scratch, ctx->pc, ctx->psiold, ctx->hpsiold, ctx->pot4, ctx->mu4,
+              ctx->fn.h2o2m4, ctx->den, S_ERRHE));
+  for (int i = 0; i < ctx->nq; ++i)
+    TRY(correct(ctx->psix[i], ctx->xscratch, ctx->pcx[i], ctx->psixold[i], ctx->hpsixold[i],
+                ctx->upotx[i], 0.0, ctx->h2o2mx[i], ctx->denx[i], S_ERRX + i));
+  const int a = ctx->ioldp[2];
+  ctx->ioldp[2] = ctx->ioldp[1];
+  ctx->ioldp[1] = ctx->ioldp[0];
+  ctx->ioldp[0] = a;
+  if (errHe || errpsix) {
+    TRY(read_sums(ctx));
+    if (errHe) *errHe = c9 * ctx->hsum[S_ERRHE] / (double)ctx->N;
+    if (errpsix) {
+      double e = 0.0;
+      for (int i = 0; i < ctx->nq; ++i) e = e + c9 * ctx->hsum[S_ERRX + i];
+      *errpsix = e / (double)ctx->N;
+    }
+  }
+  return HE_OK;
+}
+
+static int q_dot(he_ctx_t* ctx, const double* x, const double* y, int slot) {
+  tname(ctx, "dot_reduce");
+  k_dot<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(x, y, ctx->N, tail(ctx, slot));
+  LAUNCHED();
+  return HE_OK;
+}
+
+// energy (Dynamics_quantum_impurities/energy.f90:12-139).  sto2 of the reference lands in t4.
+static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
+  OpEnergy<double2> op{};
+  op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->den;
+  op.has_u = 0;
+  op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
+  op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
+  TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_EN));
+  const int n = ctx->nq;
+  for (int k = 0; k < n; ++k) {
+    OpGrad2 g{};
+    TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psix[k], g, S_QEK + k));
+  }
+  TRY(q_denx_spectra(ctx));
+  QOut o{};
+  o.out = ctx->t4;
+  for (int k = 0; k < n; ++k) { o.src[o.nterm] = ctx->sx[k]; o.ker[o.nterm++] = ctx->uimpk[k]; }
+  TRY(q_synth(ctx, &o, 1, nullptr));
+  TRY(q_dot(ctx, ctx->t4, ctx->den, S_QHEX));
+  int pair = 0;
+  for (int k = 0; k < n; ++k)
+    for (int m = k + 1; m < n; ++m, ++pair) {
+      const double* kk = ctx->uimpkk[k + kMaxQImp * m];
+      if (!kk) continue;
+      QOut p{};
+      p.out = ctx->t4;
+      p.nterm = 1; p.src[0] = ctx->sx[k]; p.ker[0] = kk;
+      TRY(q_synth(ctx, &p, 1, nullptr));
+      TRY(q_dot(ctx, ctx->t4, ctx->denx[m], S_QII + pair));
+    }
+  TRY(read_sums(ctx));
+  const double* s = ctx->hsum + S_EN;
+  const double dxyz = ctx->dxyz;
+  he_energies_t e{};
+  e.esolid = ctx->fn.lsolid ? ctx->fn.C * s[3] * dxyz : 0.0;
+  e.ekin4 = ctx->fn.h2o2m4 * s[0] * dxyz;
+  e.elj4 = 0.5 * s[1] * dxyz;
+  e.ecor4 = s[2] * dxyz;
+  e.etot4 = e.ekin4 + e.elj4 + e.ecor4 + e.esolid;
+  for (int k = 0; k < n; ++k) e.ekinx = e.ekinx + ctx->h2o2mx[k] * ctx->hsum[S_QEK + k];
+  e.ekinx = e.ekinx * dxyz;
+  e.eHeX = ctx->hsum[S_QHEX] * dxyz;
+  pair = 0;
+  for (int k = 0; k < n; ++k)
+    for (int m = k + 1; m < n; ++m, ++pair)
+      if (ctx->uimpkk[k + kMaxQImp * m]) e.eimpu_impu = e.eimpu_impu + ctx->hsum[S_QII + pair];
+  e.eimpu_impu = e.eimpu_impu * dxyz;
+  e.eimpu = e.ekinx + e.eHeX + e.eimpu_impu;
+  e.etot = e.etot4 + e.eimpu;
+  *out = e;
+  return HE_OK;
+}
+
+// ---- FT_V_spline (Dynamics_quantum_impurities/FT_V_spline.f90:14-276) --------------------------
+// Host half: the cubic splines (mates.f:36-110, Maron's tridiagonal algorithm with prescribed end
+// second derivatives; 1-based index helpers follow the reference's loops) and the small-q
+// redefinition; the transform of the pieces, which is the O(N_p * N_FT_V_spline) part, is k_ftv.
+namespace ftv {
+
+constexpr double kRmax = 5000.0, kEps = 1.0e-8, kSmallQ = 1.0e-2, kDr = 0.05;
+
+static double pair_value(const he_pairpot_t& v, double r) {
+  if (r < v.rcut) return v.umax;
+  if (v.kind == 0) return 0.0;
+  const double e = 1.0 - std::exp(-v.a * (r - v.re));
+  return v.D * (e * e - 1.0);
+}
+
+static void spline(const double* xv, const double* yv, double* av, double* bv, double* cv, double* dv,
+                   double s1, double sn, int n) {
+  auto X = [&](int i) { return xv[i - 1]; };
+  auto Y = [&](int i) { return yv[i - 1]; };
+  auto A = [&](int i) -> double& { return av[i - 1]; };
+  auto B = [&](int i) -> double& { return bv[i - 1]; };
+  auto C = [&](int i) -> double& { return cv[i - 1]; };
+  auto D = [&](int i) -> double& { return dv[i - 1]; };
+  const int n1 = n - 1, n2 = n - 2;
+  for (int i = 1; i <= n1; ++i) {
+    A(i) = X(i + 1) - X(i);
+    D(i) = (Y(i + 1) - Y(i)) / A(i);
+  }
+  for (int i = 1; i <= n2; ++i) {
+    B(i) = 2.0 * (A(i) + A(i + 1));
+    const int k = n1 - i + 1;
+    D(k) = 6.0 * (D(k) - D(k - 1));
+  }
+  D(2) = D(2) - A(1) * s1;
+  D(n1) = D(n1) - A(n1) * sn;
+  for (int i = 2; i <= n2; ++i) {
+    const double r = A(i) / B(i - 1);
+    B(i) = B(i) - r * A(i);
+    D(i + 1) = D(i + 1) - r * D(i);
+  }
+  D(n1) = D(n1) / B(n2);
+  for (int i = 2; i <= n2; ++i) {
+    const int k = n1 - i + 1;
+    D(k) = (D(k) - A(k) * D(k + 1)) / B(k - 1);
+  }
+  D(n) = sn;
+  double si1 = s1;
+  for (int i = 1; i <= n1; ++i) {
+    const double si = si1;
+    si1 = D(i + 1);
+    const double h = A(i), hi = 1.0 / h;
+    const double x0 = X(i), x1 = X(i + 1);
+    A(i) = (hi / 6.0) * (si * (x1 * x1 * x1) - si1 * (x0 * x0 * x0)) + hi * (Y(i) * x1 - Y(i + 1) * x0) +
+           (h / 6.0) * (si1 * x0 - si * x1);
+    B(i) = (hi / 2.0) * (si1 * (x0 * x0) - si * (x1 * x1)) + hi * (Y(i + 1) - Y(i)) + (h / 6.0) * (si - si1);
+    C(i) = (hi / 2.0) * (si * x1 - si1 * x0);
+    D(i) = (hi / 6.0) * (si1 - si);
+  }
+}
+
+// RAII device buffer for the set-up path.
+struct DBuf {
+  double* p = nullptr;
+  ~DBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t n) { return cudaMalloc(&p, n * sizeof(double)); }
+};
+
+// Builds the momentum table P_p, Vpp and its spline (A..D, np entries) on `stream`.
+static cudaError_t table(const he_pairpot_t& v, double pmax, double hp, int n, int parabolic,
+                         cudaStream_t st, std::vector<double>& P, std::vector<double>& V,
+                         std::vector<double>& A, std::vector<double>& B, std::vector<double>& C,
+                         std::vector<double>& D, std::string* why) {
+  if (n < 4) { *why = "n_spline must be at least 4"; return cudaErrorInvalidValue; }
+  const double X1 = v.rcut + kEps, XN = kRmax;
+  const double S1 = (pair_value(v, X1) - 2.0 * pair_value(v, X1 + kDr) + pair_value(v, X1 + kDr + kDr)) / (kDr * kDr);
+  const double Sn = (pair_value(v, XN - kDr) - 2.0 * pair_value(v, XN) + pair_value(v, XN + kDr)) / (kDr * kDr);
+  const double h = (XN - X1) / (n - 1);
+  std::vector<double> x(n), y(n), a(n), b(n), c(n), d(n);
+  for (int i = 1; i <= n; ++i) {
+    x[i - 1] = (i - 1) * h + X1;
+    y[i - 1] = pair_value(v, x[i - 1]);
+  }
+  spline(x.data(), y.data(), a.data(), b.data(), c.data(), d.data(), S1, Sn, n);
+  const int np = (int)(pmax / hp + 1.5);
+  if (np < 8) { *why = "momentum table too short"; return cudaErrorInvalidValue; }
+  FtvArgs F{};
+  F.n = n; F.hp = hp; F.r0 = v.rcut; F.f0 = v.umax; F.parabolic = parabolic;
+  if (parabolic) {
+    const double r0 = v.rcut, r1 = r0 + kDr, f0 = v.umax, f1 = pair_value(v, r1);
+    F.aa = (f0 - f1) / (r0 * r0 - r1 * r1);
+    F.cc = (r0 * r0 * f1 - r1 * r1 * f0) / (r0 * r0 - r1 * r1);
+    if (F.aa > 0.0) { *why = "parabolic core fit is not inverted (FT_V_spline.f90:142-145)"; return cudaErrorInvalidValue; }
+  }
+  DBuf dx, da, db, dc, dd, dv;
+  cudaError_t e;
+  if ((e = dx.alloc(n)) || (e = da.alloc(n)) || (e = db.alloc(n)) || (e = dc.alloc(n)) ||
+      (e = dd.alloc(n)) || (e = dv.alloc(np))) { *why = "device allocation"; return e; }
+  const std::vector<double>* hs[5] = {&x, &a, &b, &c, &d};
+  double* ds[5] = {dx.p, da.p, db.p, dc.p, dd.p};
+  for (int k = 0; k < 5; ++k)
+    if ((e = cudaMemcpyAsync(ds[k], hs[k]->data(), n * sizeof(double), cudaMemcpyHostToDevice, st))) {
+      *why = "upload"; return e;
+    }
+  F.x = dx.p; F.a = da.p; F.b = db.p; F.c = dc.p; F.d = dd.p; F.vpp = dv.p;
+  k_ftv<<<np, 256, 0, st>>>(F);
+  if ((e = cudaGetLastError())) { *why = "k_ftv launch"; return e; }
+  V.resize(np);
+  if ((e = cudaMemcpyAsync(V.data(), dv.p, np * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaStreamSynchronize(st))) { *why = "k_ftv"; return e; }
+  P.resize(np);
+  for (int i = 0; i < np; ++i) P[i] = i * hp;
+  // small-q redefinition (FT_V_spline.f90:229-258)
+  double qx[4] = {0.0, 0, 0, 0}, qy[4] = {V[0], 0, 0, 0};
+  int iaux = 1;
+  for (int i = 2; i <= np; ++i) {
+    if (P[i - 1] > kSmallQ) { ++iaux; qx[iaux - 1] = P[i - 1]; qy[iaux - 1] = V[i - 1]; }
+    if (iaux == 4) break;
+  }
+  double qa[4], qb[4], qc[4], qd[4];
+  spline(qx, qy, qa, qb, qc, qd, 0.0, 0.0, 4);
+  for (int i = 2; i <= np; ++i) {
+    const double p = P[i - 1];
+    if (p <= kSmallQ) V[i - 1] = qa[0] + p * (qb[0] + p * (qc[0] + p * qd[0]));
+    else break;
+  }
+  A.resize(np); B.resize(np); C.resize(np); D.resize(np);
+  spline(P.data(), V.data(), A.data(), B.data(), C.data(), D.data(), 0.0, 0.0, np);
+  return cudaSuccess;
+}
+
+}  // namespace ftv
+
+// potenimpini (Dynamics_quantum_impurities/potenimpini.f90:116-163): uimp_k of one pair potential
+// over this context's half spectrum; qmax = max(100, |pmax|), Hq = qmax/(max(10001,Nq)-1).
+static int q_kernel(he_ctx_t* ctx, const he_pairpot_t& v, int nspline, int nq, int parabolic, double* dst) {
+  const double pmx = 1.0 / (2.0 * ctx->hx), pmy = 1.0 / (2.0 * ctx->hy), pmz = 1.0 / (2.0 * ctx->hz);
+  const double qmax = std::max(100.0, std::sqrt(pmx * pmx + pmy * pmy + pmz * pmz));
+  const long Nq = std::max(10001L, (long)nq);
+  const double hq = qmax / (double)(Nq - 1);
+  std::vector<double> P, V, A, B, C, D;
+  std::string why;
+  cudaError_t e = ftv::table(v, qmax, hq, nspline, parabolic, ctx->stream, P, V, A, B, C, D, &why);
+  if (e != cudaSuccess)
+    return fail(ctx, e == cudaErrorInvalidValue ? HE_ERR_ARG : HE_ERR_CUDA, "FT_V_spline: %s (%s)",
+                why.c_str(), cudaGetErrorString(e));
+  const int np = (int)P.size();
+  ftv::DBuf dP, dA, dB, dC, dD;
+  CK(dP.alloc(np)); CK(dA.alloc(np)); CK(dB.alloc(np)); CK(dC.alloc(np)); CK(dD.alloc(np));
+  CK(cudaMemcpyAsync(dP.p, P.data(), np * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dA.p, A.data(), np * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dB.p, B.data(), np * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dC.p, C.data(), np * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dD.p, D.data(), np * 8, cudaMemcpyHostToDevice, ctx->stream));
+  UimpkArgs u{};
+  u.P = dP.p; u.a = dA.p; u.b = dB.p; u.c = dC.p; u.d = dD.p; u.np = np;
+  u.nx = ctx->nx; u.ny = ctx->ny; u.nz = ctx->nz; u.nxh = ctx->nxh;
+  u.hx = ctx->hx; u.hy = ctx->hy; u.hz = ctx->hz;
+  u.out = dst;
+  tname(ctx, "uimp_k_spline");
+  k_uimpk<<<kPwBlocks, 256, 0, ctx->stream>>>(u);
+  LAUNCHED();
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HE_OK;
+}
+
+static bool qfield(int f) { return f >= HE_F_PSIX && f <= HE_F_UIMPKK; }
+
+// Transfers of the per-impurity arrays (one device buffer per impurity and slot).
+static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
+  if (ctx->mode != HE_MODE_QUANTUM || ctx->nq == 0)
+    return fail(ctx, HE_ERR_STATE, "quantum-impurity fields need HE_MODE_QUANTUM and he_set_quantum_impurities");
+  const int n = ctx->nq;
+  const size_t N = ctx->N, Nk = ctx->Nk;
+  std::vector<std::pair<void*, size_t>> parts;
+  switch (field) {
+    case HE_F_PSIX: for (int i = 0; i < n; ++i) parts.push_back({ctx->psix[i], 16 * N}); break;
+    case HE_F_PCX: for (int i = 0; i < n; ++i) parts.push_back({ctx->pcx[i], 16 * N}); break;
+    case HE_F_QX: for (int i = 0; i < n; ++i) parts.push_back({ctx->qx[i], 16 * N}); break;
+    case HE_F_UPOTX: for (int i = 0; i < n; ++i) parts.push_back({ctx->upotx[i], 8 * N}); break;
+    case HE_F_POTX4: parts.push_back({ctx->potx4, 8 * N}); break;
+    case HE_F_PSIXOLD:
+      for (int i = 0; i < n; ++i) for (int s = 0; s < 3; ++s) parts.push_back({ctx->psixold[i][s], 16 * N});
+      break;
+    case HE_F_HPSIXOLD:
+      for (int i = 0; i < n; ++i) for (int s = 0; s < 2; ++s) parts.push_back({ctx->hpsixold[i][s], 16 * N});
+      break;
+    case HE_F_UIMPK: for (int i = 0; i < n; ++i) parts.push_back({ctx->uimpk[i], 8 * Nk}); break;
+    case HE_F_UIMPKK:  // pairs without a kernel ('null', i == j) read as zero and are not stored
+      for (int j = 0; j < n; ++j) for (int i = 0; i < n; ++i) parts.push_back({ctx->uimpkk[i + kMaxQImp * j], 8 * Nk});
+      break;
+    case HE_F_DENX: {
+      if (up) return fail(ctx, HE_ERR_ARG, "denx is derived from psix (download only)");
+      if (bytes != 8 * N) return fail(ctx, HE_ERR_ARG, "denx: expected %zu bytes", 8 * N);
+      std::vector<double> acc(N, 0.0), t(N);
+      for (int i = 0; i < n; ++i) {
+        CK(cudaMemcpyAsync(t.data(), ctx->denx[i], 8 * N, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (size_t k = 0; k < N; ++k) acc[k] = acc[k] + t[k];
+      }
+      std::memcpy(host, acc.data(), 8 * N);
+      return HE_OK;
+    }
+    default: return fail(ctx, HE_ERR_ARG, "unknown field %d", field);
+  }
+  size_t total = 0;
+  for (auto& p : parts) total += p.second;
+  if (bytes != total) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, total, bytes);
+  char* h = (char*)host;
+  for (auto& p : parts) {
+    if (up) {
+      if (p.first) CK(cudaMemcpyAsync(p.first, h, p.second, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+      if (p.first) CK(cudaMemcpyAsync(h, p.first, p.second, cudaMemcpyDeviceToHost, ctx->stream));
+      else std::memset(h, 0, p.second);
+    }
+    h += p.second;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (up && field == HE_F_PSIX)
+    for (int i = 0; i < n; ++i) TRY(q_cnorm2(ctx, i));
+  if (up && (field == HE_F_PSIX || field == HE_F_UIMPK || field == HE_F_UIMPKK)) ctx->cglj_pending = false;
+  return HE_OK;
+}
+
 extern "C" {
 
 int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, int precision,
@@ -825,7 +1411,8 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
     ctx->err = msg;
     st = code;
   };
-  if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS) bad(HE_ERR_ARG, "unknown mode");
+  if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS && mode != HE_MODE_QUANTUM)
+    bad(HE_ERR_ARG, "unknown mode");
   else if (precision != HE_PREC_F64) bad(HE_ERR_ARG, "unknown precision");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
   else if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18)
@@ -911,8 +1498,15 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   TRY(dalloc(ctx, &ctx->pc, wf));
   TRY(dalloc(ctx, &ctx->q, wf));
   TRY(dalloc(ctx, &ctx->scratch, wf));
-  if (mode == HE_MODE_DYNAMICS) {
-    TRY(dalloc_t(ctx, &ctx->uimp, N));
+  if (mode == HE_MODE_DYNAMICS) TRY(dalloc_t(ctx, &ctx->uimp, N));
+  if (mode == HE_MODE_QUANTUM) {
+    TRY(dalloc_t(ctx, &ctx->potx4, N));
+    TRY(dalloc_t(ctx, &ctx->t4, N));
+    TRY(dalloc_t(ctx, &ctx->wC, Nk));
+    TRY(dalloc_t(ctx, &ctx->wD, Nk));
+    TRY(dalloc(ctx, &ctx->xscratch, wf));
+  }
+  if (mode != HE_MODE_STATICS) {
     TRY(dalloc_t(ctx, &ctx->tabx, ctx->nx));
     TRY(dalloc_t(ctx, &ctx->taby, ctx->ny));
     TRY(dalloc_t(ctx, &ctx->tabz, ctx->nz));
@@ -992,7 +1586,7 @@ int he_compute_kernels(he_ctx_t* ctx) {
 
 int he_set_absorber(he_ctx_t* ctx, const he_absorber_t* ab) {
   if (!ctx || !ab) return fail(ctx, HE_ERR_ARG, "null absorber");
-  if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "absorber is a dynamics setting");
+  if (ctx->mode == HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "absorber is a dynamics setting");
   auto tab = [&](int n, double xm, double h, double mean, double surf, double* dst) -> int {
     std::vector<double> t(n);
     for (int i = 0; i < n; ++i) t[i] = std::tanh((std::fabs(-xm + h * i) - mean) / surf);
@@ -1046,6 +1640,7 @@ int he_set_impurities(he_ctx_t* ctx, const he_impurities_t* im) {
 
 int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   if (!ctx || !host) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (qfield(field)) return q_xfer(ctx, field, const_cast<void*>(host), bytes, true);
   if (field >= HE_F_RIMP && field <= HE_F_QV) {
     if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "no impurities in statics");
     ImpDev h;
@@ -1066,11 +1661,14 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   CK(cudaStreamSynchronize(ctx->stream));
   if (field == HE_F_FVLJ4 || field == HE_F_WCGK) ctx->kernels_ok = true;
   if (field == HE_F_DEN) ctx->force_fresh = false;
+  if (field == HE_F_DEN || field == HE_F_FDEN || field == HE_F_FVLJ4 || field == HE_F_WCGK)
+    ctx->cglj_pending = false;
   return HE_OK;
 }
 
 int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
   if (!ctx || !host) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (qfield(field)) return q_xfer(ctx, field, host, bytes, false);
   if (field == HE_F_RING) {
     if (bytes != 13 * 8) return fail(ctx, HE_ERR_ARG, "ring: expected 104 bytes");
     double* o = (double*)host;
@@ -1108,6 +1706,10 @@ int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
 int he_poten(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
   if (!ctx->kernels_ok) return fail(ctx, HE_ERR_STATE, "k-space kernels not set");
+  if (ctx->mode == HE_MODE_QUANTUM) {
+    if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
+    return q_poten(ctx);
+  }
   if (ctx->mode == HE_MODE_STATICS) {
     // He_statics/poten.f90:27-115: delj4 from the last refreshed fden (cached by
     // he_refresh_density), correlation with the current den and the stale dencg.
@@ -1129,6 +1731,11 @@ int he_poten(he_ctx_t* ctx) {
 
 int he_potenimp(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
+  if (ctx->mode == HE_MODE_QUANTUM) {
+    if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
+    if (!ctx->kernels_ok) return fail(ctx, HE_ERR_STATE, "k-space kernels not set");
+    return q_potenimp(ctx);
+  }
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "potenimp is a dynamics routine");
   if (ctx->n_imp == 0) {
     ctx->force_fresh = true;
@@ -1174,6 +1781,10 @@ int he_set_accel(he_ctx_t* ctx) {
 
 int he_steprk(he_ctx_t* ctx, double deltat) {
   if (!ctx) return HE_ERR_ARG;
+  if (ctx->mode == HE_MODE_QUANTUM) {
+    if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
+    return q_steprk(ctx, deltat);
+  }
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "steprk is a dynamics routine");
   const double r2 = 1.0 / std::sqrt(2.0);
   const double arun[4] = {0.5, 1.0 - r2, 1.0 + r2, 1.0 / 6.0};
@@ -1218,6 +1829,11 @@ int he_steprk(he_ctx_t* ctx, double deltat) {
 
 int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, double* errvimp) {
   if (!ctx) return HE_ERR_ARG;
+  if (ctx->mode == HE_MODE_QUANTUM) {
+    if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
+    if (errvimp) *errvimp = 0.0;
+    return q_steppc(ctx, deltat, errHe, errimp);
+  }
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "steppc is a dynamics routine");
   const double c112 = 112.0 / 121.0, c9 = 9.0 / 121.0, c4o3 = 4.0 / 3.0;
   {
@@ -1289,6 +1905,10 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
 
 int he_energy(he_ctx_t* ctx, he_energies_t* out) {
   if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (ctx->mode == HE_MODE_QUANTUM) {
+    if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
+    return q_energy(ctx, out);
+  }
   if (ctx->mode == HE_MODE_DYNAMICS) {
     OpEnergy<double2> op{};
     op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->uimp;
@@ -1406,8 +2026,7 @@ int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
     TRY(stat_hpsi(ctx, ctx->hpsi, S_STAT_H));
     if (jr == 0) {
       tname(ctx, "copy_slot");
-      tname(ctx, "copy_slot");
-  k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H);
+      k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H);
       LAUNCHED();
     }
     StatPW s = statpw(ctx, deltat, n4);
@@ -1553,6 +2172,117 @@ int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z) {
   *x = ctx->tile_x;
   *y = ctx->tile_y;
   *z = ctx->tile_z;
+  return HE_OK;
+}
+
+int he_set_quantum_impurities(he_ctx_t* ctx, const he_qimpurities_t* q) {
+  if (!ctx || !q) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (ctx->mode != HE_MODE_QUANTUM) return fail(ctx, HE_ERR_STATE, "quantum impurities need HE_MODE_QUANTUM");
+  const int n = q->n_imp;
+  if (n < 1 || n > kMaxQImp) return fail(ctx, HE_ERR_ARG, "n_imp must be in [1, %d]", kMaxQImp);
+  if (!q->m_imp_u) return fail(ctx, HE_ERR_ARG, "null m_imp_u");
+  if (ctx->nq != 0 && ctx->nq != n) return fail(ctx, HE_ERR_STATE, "n_imp cannot change once set");
+  for (int i = 0; i < n; ++i)
+    if (!(q->m_imp_u[i] > 0.0)) return fail(ctx, HE_ERR_ARG, "impurity masses must be positive");
+  const int nspline = q->n_spline > 0 ? q->n_spline : 100001;
+  const size_t N = ctx->N, Nk = ctx->Nk;
+  if (ctx->nq == 0) {
+    for (int i = 0; i < n; ++i) {
+      TRY(dalloc(ctx, &ctx->psix[i], 16 * N));
+      TRY(dalloc(ctx, &ctx->pcx[i], 16 * N));
+      TRY(dalloc(ctx, &ctx->qx[i], 16 * N));
+      for (int s = 0; s < 3; ++s) TRY(dalloc(ctx, &ctx->psixold[i][s], 16 * N));
+      for (int s = 0; s < 2; ++s) TRY(dalloc(ctx, &ctx->hpsixold[i][s], 16 * N));
+      TRY(dalloc_t(ctx, &ctx->denx[i], N));
+      TRY(dalloc_t(ctx, &ctx->upotx[i], N));
+      TRY(dalloc_t(ctx, &ctx->uimpk[i], Nk));
+      TRY(dalloc_t(ctx, &ctx->sx[i], Nk));
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      const bool want = i != j && (q->uimp_k_k || q->x_x[i + n * j].kind != 0);
+      double*& kk = ctx->uimpkk[i + kMaxQImp * j];
+      if (want && !kk) TRY(dalloc_t(ctx, &kk, Nk));
+      if (!want) kk = nullptr;  // a buffer left from an earlier call stays allocated, unused
+    }
+  ctx->nq = n;
+  ctx->mu4 = q->mu4;
+  for (int i = 0; i < n; ++i) ctx->h2o2mx[i] = ctx->fn.h2o2m4 * 4.002603 / q->m_imp_u[i];
+  // potenimpini: uimp_k_i and uimp_k_k(i,j), each distinct potential transformed once.
+  for (int i = 0; i < n; ++i) {
+    if (q->uimp_k) {
+      CK(cudaMemcpyAsync(ctx->uimpk[i], q->uimp_k + Nk * i, 8 * Nk, cudaMemcpyHostToDevice, ctx->stream));
+      continue;
+    }
+    const double* same = nullptr;
+    for (int k = 0; k < i && !same; ++k)
+      if (std::memcmp(&q->he_x[k], &q->he_x[i], sizeof(he_pairpot_t)) == 0) same = ctx->uimpk[k];
+    if (same) CK(cudaMemcpyAsync(ctx->uimpk[i], same, 8 * Nk, cudaMemcpyDeviceToDevice, ctx->stream));
+    else TRY(q_kernel(ctx, q->he_x[i], nspline, q->nq, q->parabolic, ctx->uimpk[i]));
+  }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      double* kk = ctx->uimpkk[i + kMaxQImp * j];
+      if (!kk) continue;
+      if (q->uimp_k_k) {
+        CK(cudaMemcpyAsync(kk, q->uimp_k_k + Nk * (i + (size_t)n * j), 8 * Nk, cudaMemcpyHostToDevice, ctx->stream));
+        continue;
+      }
+      TRY(q_kernel(ctx, q->x_x[i + n * j], nspline, q->nq, q->parabolic, kk));
+    }
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; ++i) TRY(q_cnorm2(ctx, i));
+  for (int i = 0; i < 3; ++i) ctx->ioldp[i] = i + 1;
+  ctx->ioldh[0] = 1; ctx->ioldh[1] = 2;
+  ctx->cglj_pending = false;
+  return HE_OK;
+}
+
+int he_qimp_moments(he_ctx_t* ctx, double* out) {
+  if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (ctx->mode != HE_MODE_QUANTUM || ctx->nq == 0)
+    return fail(ctx, HE_ERR_STATE, "no quantum impurities");
+  for (int i = 0; i < ctx->nq; ++i) {
+    tname(ctx, "impurity_moments");
+    k_moments<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
+        (const double2*)ctx->psix[i], ctx->nx, ctx->ny, ctx->N, -ctx->xmax, -ctx->ymax, -ctx->zmax,
+        ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i));
+    LAUNCHED();
+  }
+  TRY(read_sums(ctx));
+  for (int i = 0; i < ctx->nq; ++i) {
+    const double* m = ctx->hsum + S_QMOM + 4 * i;
+    const double a = m[0] * ctx->dxyz;
+    out[4 * i] = a;
+    out[4 * i + 1] = m[1] * ctx->dxyz / a;
+    out[4 * i + 2] = m[2] * ctx->dxyz / a;
+    out[4 * i + 3] = m[3] * ctx->dxyz / a;
+  }
+  return HE_OK;
+}
+
+int he_ft_v_spline_table(const he_pairpot_t* pot, double pmax, double hp, int n_spline,
+                         int parabolic, double* vpp, int n_p, char* err, size_t errlen) {
+  if (err && errlen) err[0] = '\0';
+  auto bad = [&](int code, const char* msg) {
+    if (err && errlen) snprintf(err, errlen, "%s", msg);
+    return code;
+  };
+  if (!pot || !vpp) return bad(HE_ERR_ARG, "null argument");
+  if (!(hp > 0.0) || !(pmax > 0.0)) return bad(HE_ERR_ARG, "pmax and hp must be positive");
+  if ((int)(pmax / hp + 1.5) != n_p) return bad(HE_ERR_ARG, "n_p must be int(pmax/hp + 1.5)");
+  std::vector<double> P, V, A, B, C, D;
+  std::string why;
+  cudaStream_t st = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = ftv::table(*pot, pmax, hp, n_spline > 0 ? n_spline : 100001, parabolic, st, P, V, A, B, C, D, &why);
+  if (st) cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    if (err && errlen) snprintf(err, errlen, "FT_V_spline: %s (%s)", why.c_str(), cudaGetErrorString(e));
+    return e == cudaErrorInvalidValue ? HE_ERR_ARG : HE_ERR_CUDA;
+  }
+  std::memcpy(vpp, V.data(), sizeof(double) * n_p);
   return HE_OK;
 }
 

@@ -29,23 +29,45 @@ HE_D double2 hpsi_rt(double2 dx, double2 dy, double2 dz, double2 c, double pot, 
   return make_double2(tr * ax - ay + u * c.y, tr * ay + ax - u * c.x);
 }
 
-// steppc predictor + modifier (steppc.f90:51-61).  po3 = psiold(ioldp(3)) is read and receives
-// the new psi (the host then swaps it with the psi buffer, so psiold(ioldp(3)) holds the old psi).
-struct OpPredict {
-  static const char* kname() { return "hpsi_pmc_predict"; }
+// H psi of the quantum-impurity path (Dynamics_quantum_impurities/steprk.f90:68,94,
+// steppc.f90:46,77): timec*((d2x+d2y+d2z)*h2o2m - v*psi), v = pot4 - mu4 for He and upotx_i
+// for impurity i (no -i*uimp term: the impurities enter through the potentials).
+HE_D double2 hpsi_q(double2 dx, double2 dy, double2 dz, double2 c, double v, double tr,
+                    double h2o2m) {
+  const double2 lap = cadd(cadd(dx, dy), dz);
+  const double ax = lap.x * h2o2m - v * c.x;
+  const double ay = lap.y * h2o2m - v * c.y;
+  return make_double2(tr * ax - ay, tr * ay + ax);
+}
+
+// H psi of either path from the staged operands: QU = false reads {pot4, uimp}, QU = true reads
+// {pot} and subtracts the constant mu.
+template <bool QU>
+HE_D double2 hpsi_any(double2 dx, double2 dy, double2 dz, double2 c, const double* v8, int vs,
+                      double mu, double tr, double h2o2m) {
+  if constexpr (QU) return hpsi_q(dx, dy, dz, c, v8[0] - mu, tr, h2o2m);
+  else return hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tr, h2o2m);
+}
+
+// steppc predictor + modifier (steppc.f90:51-61; quantum path steppc.f90:46-56, :77-87).  po3 =
+// psiold(ioldp(3)) is read and receives the new psi (the host then swaps it with the psi buffer,
+// so psiold(ioldp(3)) holds the old psi).
+template <bool QU>
+struct OpPredictT {
+  static const char* kname() { return QU ? "hpsi_pmc_predict_q" : "hpsi_pmc_predict"; }
   using T = double2;
-  static constexpr int NV = 0, N8 = 2, N16 = 4;
-  const double* s8[N8];      // pot4, uimp
+  static constexpr int NV = 0, N8 = QU ? 1 : 2, N16 = 4;
+  const double* s8[N8];      // pot4, uimp (QU: pot4 or upotx_i)
   const double2* s16[N16];   // psiold(ioldp(3)), hpsiold(ioldh(1)), hpsiold(ioldh(2)), pc
   double2* po3;
   double2* h2;
   double2* pc;
   double* den;
   Timec tm;
-  double h2o2m, s43, c112;
+  double h2o2m, s43, c112, mu;
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
                const double* v8, const double2* v16, int vs, double*) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tm.re(ix, iy, iz), h2o2m);
+    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
     const double2 p3 = v16[0], hh1 = v16[vs], hh2 = v16[2 * vs], pcv = v16[3 * vs];
     const double2 t = make_double2(2.0 * s4.x - hh1.x + 2.0 * hh2.x, 2.0 * s4.y - hh1.y + 2.0 * hh2.y);
     const double2 sto1 = make_double2(p3.x + s43 * t.x, p3.y + s43 * t.y);
@@ -57,21 +79,23 @@ struct OpPredict {
   }
 };
 
-// steppc corrector + final value (steppc.f90:118-127); accumulates sum |pc|.
-struct OpCorrect {
-  static const char* kname() { return "hpsi_pmc_correct"; }
+// steppc corrector + final value (steppc.f90:118-127; quantum path steppc.f90:105-137);
+// accumulates sum |pc|.
+template <bool QU>
+struct OpCorrectT {
+  static const char* kname() { return QU ? "hpsi_pmc_correct_q" : "hpsi_pmc_correct"; }
   using T = double2;
-  static constexpr int NV = 1, N8 = 2, N16 = 5;
-  const double* s8[N8];      // pot4, uimp
+  static constexpr int NV = 1, N8 = QU ? 1 : 2, N16 = 5;
+  const double* s8[N8];      // pot4, uimp (QU: pot4 or upotx_i)
   const double2* s16[N16];   // psiold(ioldp(3)), psiold(ioldp(2)), hpsiold(ioldh(1)), (ioldh(2)), pc
   double2* pc;
   double2* out;
   double* den;
   Timec tm;
-  double h2o2m, s3, c9;
+  double h2o2m, s3, c9, mu;
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
                const double* v8, const double2* v16, int vs, double* acc) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tm.re(ix, iy, iz), h2o2m);
+    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
     const double2 a3 = v16[0], a2 = v16[vs], b1 = v16[2 * vs], b2 = v16[3 * vs], p = v16[4 * vs];
     const double2 inner = make_double2(s4.x + 2.0 * b1.x - b2.x, s4.y + 2.0 * b1.y - b2.y);
     const double2 s5 = make_double2(0.125 * (9.0 * a3.x - a2.x + s3 * inner.x),
@@ -85,22 +109,24 @@ struct OpCorrect {
   }
 };
 
-// One RK-Gill stage (steprk.f90:67-79).  hsave (stage 1 only) receives H psi for hpsiold(1).
-struct OpRK {
-  static const char* kname() { return "hpsi_rkgill_stage"; }
+// One RK-Gill stage (steprk.f90:67-79; quantum path steprk.f90:68-80, :94-104).  hsave (stage 1
+// only) receives H psi for hpsiold(1).
+template <bool QU>
+struct OpRKT {
+  static const char* kname() { return QU ? "hpsi_rkgill_stage_q" : "hpsi_rkgill_stage"; }
   using T = double2;
-  static constexpr int NV = 0, N8 = 2, N16 = 1;
-  const double* s8[N8];      // pot4, uimp
+  static constexpr int NV = 0, N8 = QU ? 1 : 2, N16 = 1;
+  const double* s8[N8];      // pot4, uimp (QU: pot4 or upotx_i)
   const double2* s16[N16];   // q
   double2* q;
   double2* out;
   double2* hsave;
   double* den;
   Timec tm;
-  double h2o2m, a, b, cc, dt;
+  double h2o2m, a, b, cc, dt, mu;
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
                const double* v8, const double2* v16, int vs, double*) const {
-    const double2 s4 = hpsi_rt(dx, dy, dz, c, v8[0], v8[vs], tm.re(ix, iy, iz), h2o2m);
+    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
     const double2 qq = v16[0];
     const double2 s1 = make_double2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
     q[i] = make_double2(qq.x + 3.0 * s1.x - cc * s4.x, qq.y + 3.0 * s1.y - cc * s4.y);
@@ -110,6 +136,13 @@ struct OpRK {
     den[i] = cnorm2(pn);
   }
 };
+
+using OpPredict = OpPredictT<false>;
+using OpCorrect = OpCorrectT<false>;
+using OpRK = OpRKT<false>;
+using OpPredictQ = OpPredictT<true>;
+using OpCorrectQ = OpCorrectT<true>;
+using OpRKQ = OpRKT<true>;
 
 // energy(): Dynamics_TDDFT/energy.f90:107-165 sums (first derivatives of psi).
 //   acc = {sum |grad psi|^2, sum delj4*den, sum den*dencg^2*(cp4/2+cpp4/3*dencg),

@@ -1,0 +1,270 @@
+// quantum.cuh -- device side of the quantum-impurity path (Dynamics_quantum_impurities), binary64.
+//
+// The impurities are wave functions psix_i (nx,ny,nz) with their own Hamiltonians
+//   H_i psix_i = timec*(h2o2mx_i lap psix_i - upotx_i psix_i),  h2o2mx_i = h2o2m4*4.002603/m_i,
+// coupled to the helium through convolutions with radial kernels (potenimp.f90:1-43):
+//   potx4   = sum_i C2R(R2C(|psix_i|^2) uimp_k_i)                  (He sees the impurities)
+//   upotx_i = C2R(fden uimp_k_i) + sum_{j!=i} C2R(R2C(|psix_j|^2) uimp_k_k(i,j))
+// uimp_k_i is FT_V_spline of the He-X pair potential at |p| (FT_V_spline.f90:14-276,
+// potenimpini.f90:116-163).
+//
+// Kernels here:
+//   OpGrad2      stencil consumer: sum |d psi/dx|^2+|d psi/dy|^2+|d psi/dz|^2 (energy.f90:105-109)
+//   k_zmix       z pencils: optional forward z transform of one spectrum, then up to two outputs
+//                each a sum of up to kMaxTerms (spectrum x real kernel) products, inverse z.
+//   k_cnorm2     |psix|^2, k_dot sum a*b, k_moments sum |psix|^2 (1, x, y, z)
+//   k_ftv        FT_V_spline's closed-form transform of the cubic pieces, one CTA per momentum
+//   k_uimpk      the momentum spline evaluated at pmod over the half spectrum (findi + Horner)
+#pragma once
+#include "fft_kernels.cuh"
+#include "ops.cuh"
+#include "setup.cuh"
+
+namespace he {
+
+constexpr int kMaxQImp = 4;
+constexpr int kMaxTerms = 4;
+
+struct OpGrad2 {
+  static const char* kname() { return "grad2_reduce"; }
+  using T = double2;
+  static constexpr int NV = 1, N8 = 0, N16 = 0;
+  const double* s8[1];
+  const double2* s16[1];
+  HE_D void at(int, int, int, long, double2 dx, double2 dy, double2 dz, double2, const double*,
+               const double2*, int, double* acc) const {
+    acc[0] += cnorm2(dx) + cnorm2(dy) + cnorm2(dz);
+  }
+};
+
+struct ZMixArgs {
+  int nxh, ny, nz, tkx;
+  LinePlan pl;
+  const double2* fwd_in;   // x,y-transformed spectrum to transform along z (null: none)
+  double2* fwd_store;      // receives that z spectrum (null: not stored)
+  int nout;                // 0, 1 or 2
+  double2* out[2];
+  int nterm[2];
+  const double2* src[2][kMaxTerms];  // full spectra; null = the forward spectrum of fwd_in
+  const double* ker[2][kMaxTerms];   // real kernels over the half spectrum
+};
+
+template <int N, int TILE>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
+  extern __shared__ double2 smem[];
+  const int n = (N > 0) ? N : a.nz;
+  const int ls = line_stride(n);
+  const int TK = (N > 0) ? TILE : a.tkx;
+  const int nxh = a.nxh;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int kx0 = blockIdx.x * TK;
+  const int ky = blockIdx.y;
+  double2* tw = smem;
+  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  double2* P1 = P0 + TK * ls;
+  double2* P2 = P1 + TK * ls;
+  load_twiddles(tw, a.pl);
+  const long plane = (long)nxh * a.ny;
+  const long base = (long)nxh * ky;
+  double2* F = nullptr;
+  double2 *O0 = P0, *O1 = P1, *S = P2;
+  if (a.fwd_in) {
+    for (int e = tid; e < TK * n; e += nthr) {
+      const int j = e / TK, c = e - j * TK;
+      const int kx = kx0 + c;
+      P0[c * ls + sw<N>(j)] = (kx < nxh) ? a.fwd_in[base + kx + plane * j] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    F = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, false);
+    O0 = (F == P0) ? P1 : P0;
+    O1 = P2;
+    S = F;
+    if (a.fwd_store) {
+      for (int e = tid; e < TK * n; e += nthr) {
+        const int j = e / TK, c = e - j * TK;
+        const int kx = kx0 + c;
+        if (kx < nxh) a.fwd_store[base + kx + plane * j] = F[c * ls + sw<N>(j)];
+      }
+    }
+  }
+  if (a.nout == 0) return;
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
+    const int kx = kx0 + c;
+    const int s = c * ls + sw<N>(j);
+    const long g = base + kx + plane * j;
+    for (int o = 0; o < a.nout; ++o) {
+      double2 acc = make_double2(0.0, 0.0);
+      if (kx < nxh) {
+        for (int t = 0; t < a.nterm[o]; ++t) {
+          const double2 v = a.src[o][t] ? a.src[o][t][g] : F[s];
+          const double w = a.ker[o][t][g];
+          acc.x += v.x * w;
+          acc.y += v.y * w;
+        }
+      }
+      (o == 0 ? O0 : O1)[s] = acc;
+    }
+  }
+  __syncthreads();
+  double2* R0 = fft_lines<N>(O0, S, TK, ls, a.pl, tw, true);
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
+    const int kx = kx0 + c;
+    if (kx < nxh) a.out[0][base + kx + plane * j] = R0[c * ls + sw<N>(j)];
+  }
+  if (a.nout < 2) return;
+  __syncthreads();
+  double2* fr = (R0 == O0) ? S : O0;
+  double2* R1 = fft_lines<N>(O1, fr, TK, ls, a.pl, tw, true);
+  for (int e = tid; e < TK * n; e += nthr) {
+    const int j = e / TK, c = e - j * TK;
+    const int kx = kx0 + c;
+    if (kx < nxh) a.out[1][base + kx + plane * j] = R1[c * ls + sw<N>(j)];
+  }
+}
+
+// ---- pointwise passes (grid-stride, deterministic two-level reductions) -----------------------
+__global__ void __launch_bounds__(256) k_cnorm2(const double2* __restrict__ f, double* __restrict__ out,
+                                                long N) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    out[i] = cnorm2(f[i]);
+}
+
+__global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const double* __restrict__ b,
+                                             long N, const ReduceTail rt) {
+  double acc[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    acc[0] += a[i] * b[i];
+  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
+  reduce_tail<1>(rt, gridDim.x);
+}
+
+// {sum |f|^2, sum |f|^2 x, sum |f|^2 y, sum |f|^2 z} (DFT4He3d.f90:682-700 of the quantum driver).
+__global__ void __launch_bounds__(256) k_moments(const double2* __restrict__ f, int nx, int ny, long N,
+                                                 double x0, double y0, double z0, double hx,
+                                                 double hy, double hz, const ReduceTail rt) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const long r = i / nx;
+    const int ix = (int)(i - r * nx);
+    const int iy = (int)(r % ny), iz = (int)(r / ny);
+    const double s = cnorm2(f[i]);
+    acc[0] += s;
+    acc[1] += s * (x0 + hx * ix);
+    acc[2] += s * (y0 + hy * iy);
+    acc[3] += s * (z0 + hz * iz);
+  }
+  block_reduce_store<4>(acc, rt.partials + blockIdx.x * 4);
+  reduce_tail<4>(rt, gridDim.x);
+}
+
+// ---- FT_V_spline --------------------------------------------------------------------------------
+struct FtvArgs {
+  const double *x, *a, *b, *c, *d;  // cubic spline of V on n nodes: p_j(r) = a + r(b + r(c + r d))
+  int n;
+  double hp;                        // momentum step H_p; CTA i computes p = i*H_p
+  double r0, f0;                    // r_cutoff and f_cutoff (= umax)
+  int parabolic;
+  double aa, cc;                    // inverted-parabola core fit (FT_V_spline.f90:128-146)
+  double* vpp;
+};
+
+// Vpp(p) = [core + sum_j closed-form integral of r sin(qr) p_j(r) over [r_j, r_j+1]] * 4 pi / q,
+// q = 2 pi p (FT_V_spline.f90:151-225); p = 0 takes the moments r^2 p_j(r) (:164-188).  The
+// nodes' sin(q r_j), cos(q r_j) are computed once per node through shared memory.
+__global__ void __launch_bounds__(256) k_ftv(const FtvArgs A) {
+  __shared__ double s_s[257], s_c[257];
+  const int tid = threadIdx.x;
+  const double p = blockIdx.x * A.hp;
+  const double Qpi = 4.0 * kPi;
+  double acc[1] = {0.0};
+  double tot[1] = {0.0};
+  if (p == 0.0) {
+    for (int j = tid; j < A.n - 1; j += blockDim.x) {
+      const double u = A.x[j], w = A.x[j + 1];
+      const double u2 = u * u, w2 = w * w;
+      acc[0] += A.a[j] / 3.0 * (w2 * w - u2 * u) + A.b[j] / 4.0 * (w2 * w2 - u2 * u2) +
+                A.c[j] / 5.0 * (w2 * w2 * w - u2 * u2 * u) + A.d[j] / 6.0 * (w2 * w2 * w2 - u2 * u2 * u2);
+    }
+    block_reduce_store<1>(acc, tot);
+    if (tid == 0) {
+      const double r0 = A.r0;
+      const double Vp = A.parabolic ? A.aa * (r0 * r0 * r0 * r0 * r0) * 0.2 + A.cc * (r0 * r0 * r0) / 3.0
+                                    : (r0 * r0 * r0) * A.f0 / 3.0;
+      A.vpp[blockIdx.x] = (Vp + tot[0]) * Qpi;
+    }
+    return;
+  }
+  const double q = 2.0 * kPi * p;
+  const double c1oq = 1.0 / q, c1oq2 = c1oq * c1oq, c1oq3 = c1oq2 * c1oq, c1oq4 = c1oq2 * c1oq2,
+               c1oq5 = c1oq4 * c1oq;
+  for (int base = 0; base < A.n - 1; base += 256) {
+    const int j = base + tid;
+    if (j < A.n) sincos(q * A.x[j], &s_s[tid], &s_c[tid]);
+    if (tid == 0 && base + 256 < A.n) sincos(q * A.x[base + 256], &s_s[256], &s_c[256]);
+    __syncthreads();
+    if (j < A.n - 1) {
+      const double rj = A.x[j], rj1 = A.x[j + 1];
+      const double sqrj = s_s[tid], cqrj = s_c[tid], sqrj1 = s_s[tid + 1], cqrj1 = s_c[tid + 1];
+      const double a = A.a[j], b = A.b[j], c = A.c[j], d = A.d[j];
+      acc[0] += (a + (b + (c + d * rj) * rj) * rj) * rj * c1oq * cqrj -
+                (a + (b + (c + d * rj1) * rj1) * rj1) * rj1 * c1oq * cqrj1 +
+                (a + (2.0 * b + (3.0 * c + 4.0 * d * rj1) * rj1) * rj1) * c1oq2 * sqrj1 -
+                (a + (2.0 * b + (3.0 * c + 4.0 * d * rj) * rj) * rj) * c1oq2 * sqrj +
+                (2.0 * b + (6.0 * c + 12.0 * d * rj1) * rj1) * c1oq3 * cqrj1 -
+                (2.0 * b + (6.0 * c + 12.0 * d * rj) * rj) * c1oq3 * cqrj +
+                (6.0 * c + 24.0 * d * rj) * c1oq4 * sqrj - (6.0 * c + 24.0 * d * rj1) * c1oq4 * sqrj1 +
+                24.0 * d * c1oq5 * (cqrj - cqrj1);
+    }
+    __syncthreads();
+  }
+  block_reduce_store<1>(acc, tot);
+  if (tid == 0) {
+    const double r0 = A.r0;
+    double sq, cq;
+    sincos(q * r0, &sq, &cq);
+    const double Vp = A.parabolic
+                          ? c1oq * (cq * (6.0 * A.aa * r0 * c1oq2 - A.aa * (r0 * r0 * r0) - A.cc * r0) +
+                                    sq * ((3.0 * A.aa * (r0 * r0) + A.cc) * c1oq - 6.0 * A.aa * c1oq3))
+                          : A.f0 * c1oq * (sq * c1oq - r0 * cq);
+    A.vpp[blockIdx.x] = (Vp + tot[0]) * c1oq * Qpi;
+  }
+}
+
+struct UimpkArgs {
+  const double *P, *a, *b, *c, *d;  // momentum table (np) and its spline
+  int np;
+  int nx, ny, nz, nxh;
+  double hx, hy, hz;
+  double* out;                      // (nxh, ny, nz)
+};
+
+// uimp_k(ix,iy,iz) = FT_V_spline(pmod) (potenimpini.f90:136-144): findi's bisection
+// (mates.f:4-33) for the piece, then its cubic in p.
+__global__ void __launch_bounds__(256) k_uimpk(const UimpkArgs A) {
+  const long nk = (long)A.nxh * A.ny * A.nz;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nk; i += (long)gridDim.x * blockDim.x) {
+    const long r = i / A.nxh;
+    const int ix = (int)(i - r * A.nxh);
+    const int iy = (int)(r % A.ny), iz = (int)(r / A.ny);
+    const double px = freq_of(ix, A.nx, A.hx), py = freq_of(iy, A.ny, A.hy), pz = freq_of(iz, A.nz, A.hz);
+    const double p = sqrt(px * px + py * py + pz * pz);
+    int k;
+    if (p > A.P[A.np - 1]) k = A.np - 1;
+    else if (p < A.P[0]) k = 1;
+    else {
+      int lo = 1, hi = A.np;
+      do {
+        const int it = (lo + hi) / 2;
+        if (p > A.P[it - 1]) lo = it;
+        if (p <= A.P[it - 1]) hi = it;
+      } while (hi - lo > 1);
+      k = lo;
+    }
+    --k;
+    A.out[i] = A.a[k] + p * (A.b[k] + p * (A.c[k] + p * A.d[k]));
+  }
+}
+
+}  // namespace he

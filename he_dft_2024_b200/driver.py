@@ -70,3 +70,38 @@ def statics_iteration(s, iterrk, deltat, mu4, n4):
     s.refresh() if hasattr(s, "refresh") else s.refresh_density()
     s.poten()
     return mu4, err
+
+
+def quantum_setup(s, psi, psix):
+    """Quantum-impurity start (Dynamics_quantum_impurities/DFT4He3d.f90:538-541): psi and the
+    impurity wave functions psix (list, one (nx,ny,nz) array per impurity) in place,
+    den = conjg(psi)*psi, then potenimp and poten."""
+    den = (np.conj(psi) * psi).real
+    if hasattr(s, "set"):
+        s.set("psi", psi)
+        s.set("den", den)
+        for i, f in enumerate(psix):
+            s.set(f"psix:{i}", f)
+    else:
+        s.upload("psi", psi)
+        s.upload("den", den)
+        s.upload("psix", np.stack([np.asarray(f) for f in psix], axis=-1))
+    s.potenimp()
+    s.poten()
+
+
+def quantum_iteration(s, iteraux, deltat, lrk=False, errors=False):
+    """One pass of the quantum time loop (Dynamics_quantum_impurities/DFT4He3d.f90:666-677):
+    steprk for the first three iterations (or always when lrk), steppc(deltat,errHe,errpsix)
+    after; then potenimp and poten."""
+    err = None
+    if iteraux <= 3 or lrk:
+        s.steprk(deltat)
+    elif hasattr(s, "upload"):
+        err = s.steppc(deltat, errors=errors)
+        err = err[:2] if err else None
+    else:
+        err = s.steppc(deltat)
+    s.potenimp()
+    s.poten()
+    return err

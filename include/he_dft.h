@@ -35,7 +35,9 @@ extern "C" {
 
 typedef struct he_ctx he_ctx_t;
 
-enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1 };
+/* HE_MODE_QUANTUM: real-time dynamics with quantum impurities (Dynamics_quantum_impurities):
+ * complex psi plus impurity wave functions psix_i (he_set_quantum_impurities). */
+enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1, HE_MODE_QUANTUM = 2 };
 enum he_precision { HE_PREC_F64 = 0 };
 
 /* Grid: Dynamics_TDDFT/modules.f90:88-105 (grid), deriva npd/icon :31-37.  h = 2*xmax/n and
@@ -120,8 +122,45 @@ enum he_field {
   HE_F_PCV = 28,
   HE_F_QR = 29,
   HE_F_QV = 30,
-  HE_F_RING = 31     /* 13 ints as doubles: ioldp(3), ioldh(2), ioldr(3), ioldv(3), iolda(2) */
+  HE_F_RING = 31,    /* 13 ints as doubles: ioldp(3), ioldh(2), ioldr(3), ioldv(3), iolda(2);
+                        HE_MODE_QUANTUM: ioldp(3), ioldh(2) (ioldpx/ioldhx hold the same values) */
+  /* HE_MODE_QUANTUM (quantal_imp / rkpc modules, Dynamics_quantum_impurities/modules.f90:280-314) */
+  HE_F_PSIX = 32,     /* psix(nx,ny,nz,N_imp) complex */
+  HE_F_UPOTX = 33,    /* upotx(nx,ny,nz,N_imp) real */
+  HE_F_POTX4 = 34,    /* potx4(nx,ny,nz) real */
+  HE_F_DENX = 35,     /* denx = sum_i |psix_i|^2, real N (download only) */
+  HE_F_PCX = 36,      /* pcx(nx,ny,nz,N_imp) complex */
+  HE_F_QX = 37,       /* qx(nx,ny,nz,N_imp) complex */
+  HE_F_PSIXOLD = 38,  /* psixold(nx,ny,nz,3,N_imp) complex */
+  HE_F_HPSIXOLD = 39, /* hpsixold(nx,ny,nz,2,N_imp) complex */
+  HE_F_UIMPK = 40,    /* uimp_k(nx/2+1,ny,nz,N_imp) real */
+  HE_F_UIMPKK = 41    /* uimp_k_k(nx/2+1,ny,nz,N_imp,N_imp) real (zero for 'null' pairs) */
 };
+
+#define HE_MAX_QIMP 4
+
+/* A radial pair potential behind Select_Pot(selec,r,r_cutoff,umax)'s contract
+ * (V_impur.f90:90-2152; r < r_cutoff gives umax).  kind 0 = 'null' (zero beyond r_cutoff),
+ * 1 = Morse D[(1-exp(-a(r-re)))^2-1] (no counterpart in the reference's table). */
+typedef struct {
+  int kind;
+  double D, re, a, rcut, umax;
+} he_pairpot_t;
+
+/* Quantum impurities: the namelist /imp/ of Dynamics_quantum_impurities/DFT4He3d.f90:160-162 and
+ * potenimpini's kernels (potenimpini.f90:116-163). */
+typedef struct {
+  int n_imp;                                   /* 1..HE_MAX_QIMP */
+  const double* m_imp_u;                       /* masses in u (n_imp) */
+  double mu4;                                  /* H psi uses pot4 - mu4 (0 unless Lbulk) */
+  he_pairpot_t he_x[HE_MAX_QIMP];              /* Selec_gs_k / r_cutoff_gs_k / umax_gs_k */
+  he_pairpot_t x_x[HE_MAX_QIMP * HE_MAX_QIMP]; /* Selec_gs_k_k(i,j) at i + n_imp*j */
+  const double* uimp_k;   /* optional host uimp_k (nx/2+1,ny,nz,n_imp); NULL: FT_V_spline here */
+  const double* uimp_k_k; /* optional host uimp_k_k (...,n_imp,n_imp); NULL: FT_V_spline here */
+  int n_spline;           /* N_FT_V_spline (FT_V_spline.f90:2); 0 = 100001 */
+  int nq;                 /* Nq (modules.f90:165); the transform uses max(10001, nq) momenta */
+  int parabolic;          /* Lparabolic_fit_FT_V_spline */
+} he_qimpurities_t;
 
 /* Context life cycle.  Replaces the allocations of dimen.f90 and the plans of fftini
  * (Dynamics_TDDFT/fft.f90:5-91).  mode: HE_MODE_DYNAMICS (complex psi, Dynamics_TDDFT) or
@@ -174,6 +213,24 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
 int he_energy(he_ctx_t* ctx, he_energies_t* out);
 /* derden(): derden.f90:26-28, materialises dxden/dyden/dzden. */
 int he_derden(he_ctx_t* ctx);
+
+/* ---- Dynamics_quantum_impurities call surface (HE_MODE_QUANTUM) ----
+ * he_potenimp: potenimp.f90:1-43 (fden, potx4, upotx from den and psix).  he_poten:
+ * poten.f90:5-155 (pot4 with potx4; uses the fden of the last he_potenimp).  he_steprk:
+ * steprk.f90:1-124; he_steppc(ctx, dt, errHe, errpsix, NULL): steppc.f90:1-157.  he_energy:
+ * energy.f90:12-139 (ekinx, eHeX, eimpu_impu from the impurity wave functions). */
+/* Sets the impurities and builds uimp_k / uimp_k_k: FT_V_spline's radial transform runs on the
+ * device (one CTA per momentum) unless host tables are given. */
+int he_set_quantum_impurities(he_ctx_t* ctx, const he_qimpurities_t* q);
+/* Norm and centre of each impurity density, out[4i..4i+3] = {sum |psix_i|^2 dxyz, <x>, <y>, <z>}
+ * (the per-step trajectory of Dynamics_quantum_impurities/DFT4He3d.f90:682-700).  Synchronises. */
+int he_qimp_moments(he_ctx_t* ctx, double* out);
+/* FT_V_spline's momentum table for one pair potential: vpp[i] = V(p = i*hp), i < n_p,
+ * n_p = int(pmax/hp + 1.5), after the small-q redefinition (FT_V_spline.f90:229-258); n_spline
+ * nodes for the radial spline (0 = 100001).  Context-free (allocates and frees its own device
+ * memory on the current device); err[errlen] receives a message on failure. */
+int he_ft_v_spline_table(const he_pairpot_t* pot, double pmax, double hp, int n_spline,
+                         int parabolic, double* vpp, int n_p, char* err, size_t errlen);
 
 /* ---- He_statics call surface ---- */
 /* The driver's per-iteration refresh (BCN4HeDFT.f90:1131-1155): derden, fftfw(den,fden),

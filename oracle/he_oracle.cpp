@@ -489,7 +489,9 @@ struct Common {
     fft.c2r(wk1.data(), delj4.data(), renor);
   }
   // Correlation convolution, penalty and pot4 assembly (poten.f90:160-198, :214-218).
-  void correlation_and_assembly() {
+  // extra (optional): potx4 of the quantum-impurity path, added after the correlation term
+  // (Dynamics_quantum_impurities/poten.f90:116-121).
+  void correlation_and_assembly(const double* extra = nullptr) {
     const long N = g.nxyz;
     const double cp4 = p.cp4, cpp4 = p.cpp4;
     const double a0 = cp4 / 2.0, a1 = cpp4 / 3.0;
@@ -509,6 +511,7 @@ struct Common {
     for (long i = 0; i < N; ++i) {
       double dc = dencg[i];
       pot4[i] = delj4[i] + dc * dc * (a0 + a1 * dc) + sto1[i];
+      if (extra) pot4[i] = pot4[i] + extra[i];
     }
     if (p.lsolid) {
 #pragma omp parallel for schedule(static)
@@ -888,6 +891,522 @@ struct Dyn : Common {
 };
 
 // ------------------------------------------------------------------------------------------------
+// Cubic splines and interval search of the quantum-impurity path.
+// findi: Dynamics_quantum_impurities/mates.f:4-33 -- bisection for the 1-based interval i with
+//   x(i) < xc <= x(i+1); i = n-1 above the table, 1 below it.
+// spline: mates.f:36-110 -- cubic spline with prescribed end second derivatives s1, sn
+//   (Maron, Numerical Analysis, 1982), coefficients of p_i(x) = a + x(b + x(c + x d)) in the
+//   absolute abscissa.  1-based helpers keep the restatement next to the reference's indexing.
+// ------------------------------------------------------------------------------------------------
+static int findi(const double* x, double xc, int n) {
+  if (xc > x[n - 1]) return n - 1;
+  if (xc < x[0]) return 1;
+  int i = 1, i1 = n;
+  do {
+    const int it = (i + i1) / 2;
+    if (xc > x[it - 1]) i = it;
+    if (xc <= x[it - 1]) i1 = it;
+  } while (i1 - i > 1);
+  return i;
+}
+
+static void spline_maron(const double* xv, const double* yv, double* av, double* bv, double* cv,
+                         double* dv, double s1, double sn, int n) {
+  auto X = [&](int i) { return xv[i - 1]; };
+  auto Y = [&](int i) { return yv[i - 1]; };
+  auto A = [&](int i) -> double& { return av[i - 1]; };
+  auto B = [&](int i) -> double& { return bv[i - 1]; };
+  auto C = [&](int i) -> double& { return cv[i - 1]; };
+  auto D = [&](int i) -> double& { return dv[i - 1]; };
+  const int n1 = n - 1, n2 = n - 2;
+  for (int i = 1; i <= n1; ++i) {
+    A(i) = X(i + 1) - X(i);
+    D(i) = (Y(i + 1) - Y(i)) / A(i);
+  }
+  for (int i = 1; i <= n2; ++i) {
+    B(i) = 2.0 * (A(i) + A(i + 1));
+    const int k = n1 - i + 1;
+    D(k) = 6.0 * (D(k) - D(k - 1));
+  }
+  D(2) = D(2) - A(1) * s1;
+  D(n1) = D(n1) - A(n1) * sn;
+  for (int i = 2; i <= n2; ++i) {
+    const double r = A(i) / B(i - 1);
+    B(i) = B(i) - r * A(i);
+    D(i + 1) = D(i + 1) - r * D(i);
+  }
+  D(n1) = D(n1) / B(n2);
+  for (int i = 2; i <= n2; ++i) {
+    const int k = n1 - i + 1;
+    D(k) = (D(k) - A(k) * D(k + 1)) / B(k - 1);
+  }
+  D(n) = sn;
+  double si1 = s1;
+  for (int i = 1; i <= n1; ++i) {
+    const double si = si1;
+    si1 = D(i + 1);
+    const double h = A(i), hi = 1.0 / h;
+    const double x0 = X(i), x1 = X(i + 1);
+    A(i) = (hi / 6.0) * (si * (x1 * x1 * x1) - si1 * (x0 * x0 * x0)) + hi * (Y(i) * x1 - Y(i + 1) * x0) +
+           (h / 6.0) * (si1 * x0 - si * x1);
+    B(i) = (hi / 2.0) * (si1 * (x0 * x0) - si * (x1 * x1)) + hi * (Y(i + 1) - Y(i)) + (h / 6.0) * (si - si1);
+    C(i) = (hi / 2.0) * (si * x1 - si1 * x0);
+    D(i) = (hi / 6.0) * (si1 - si);
+  }
+}
+
+// A pair potential of the quantum path: {kind, D, re, a, r_cutoff, umax} (Select_Pot contract).
+struct PairPot {
+  int kind = 0;
+  double D = 0, re = 0, a = 0, rcut = 0, umax = 0;
+  double operator()(double r) const { return select_pot(kind, D, re, a, rcut, umax, r); }
+  bool same(const PairPot& o) const {
+    return kind == o.kind && D == o.D && re == o.re && a == o.a && rcut == o.rcut && umax == o.umax;
+  }
+};
+
+// FT_V_spline (Dynamics_quantum_impurities/FT_V_spline.f90:14-276): the 3-D Fourier transform
+// V(p) = 4 pi/q int r sin(q r) V(r) dr, q = 2 pi p, of a radial potential.  V is held at
+// f_cutoff = umax below r_cutoff (integrated analytically, optionally by the inverted-parabola
+// fit of :128-146), splined on [r_cutoff + 1e-8, 5000] with N_FT_V_spline nodes and second
+// derivatives from 3-point differences at the ends (:92-120), and each cubic piece is
+// integrated in closed form (:151-225).  The momentum table P_p = (i-1) H_p, i = 1..N_p with
+// N_p = int(Pmax/H_p + 1.5), is redefined below small_q = 0.01 by a natural 4-point spline through
+// p = 0 and the first three p > small_q (:229-258) and splined for evaluation (:262).
+struct FTVSpline {
+  std::vector<double> P, A, B, C, D, Vpp;
+  int np = 0;
+  static constexpr double kRmax = 5000.0, kEps = 1.0e-8, kSmallQ = 1.0e-2, kDr = 0.05;
+
+  // Vpp(p) of one momentum, given the spline of V (x, a, b, c, d; n nodes).
+  static double transform(double p, const PairPot& v, bool parabolic, const std::vector<double>& x,
+                          const std::vector<double>& a, const std::vector<double>& b,
+                          const std::vector<double>& c, const std::vector<double>& d, int n) {
+    const double Qpi = 4.0 * kPi;
+    const double r0 = v.rcut, f0 = v.umax;
+    double aa = 0, cc = 0;
+    if (parabolic) {
+      const double r1 = r0 + kDr, f1 = v(r1);
+      aa = (f0 - f1) / (r0 * r0 - r1 * r1);
+      cc = (r0 * r0 * f1 - r1 * r1 * f0) / (r0 * r0 - r1 * r1);
+    }
+    if (p == 0.0) {
+      double Vp = parabolic ? aa * (r0 * r0 * r0 * r0 * r0) * 0.2 + cc * (r0 * r0 * r0) / 3.0
+                            : (r0 * r0 * r0) * f0 / 3.0;
+      double Fi = 0.0;
+      for (int j = 0; j < n - 1; ++j) {
+        const double u = x[j], w = x[j + 1];
+        const double u2 = u * u, w2 = w * w;
+        Fi = Fi + a[j] / 3.0 * (w2 * w - u2 * u) + b[j] / 4.0 * (w2 * w2 - u2 * u2) +
+             c[j] / 5.0 * (w2 * w2 * w - u2 * u2 * u) + d[j] / 6.0 * (w2 * w2 * w2 - u2 * u2 * u2);
+      }
+      return (Vp + Fi) * Qpi;
+    }
+    const double q = 2.0 * kPi * p;
+    const double c1oq = 1.0 / q, c1oq2 = c1oq * c1oq, c1oq3 = c1oq2 * c1oq, c1oq4 = c1oq2 * c1oq2,
+                 c1oq5 = c1oq4 * c1oq;
+    double Vp;
+    if (parabolic)
+      Vp = c1oq * (std::cos(q * r0) * (6.0 * aa * r0 * c1oq2 - aa * (r0 * r0 * r0) - cc * r0) +
+                   std::sin(q * r0) * ((3.0 * aa * (r0 * r0) + cc) * c1oq - 6.0 * aa * c1oq3));
+    else
+      Vp = f0 * c1oq * (std::sin(q * r0) * c1oq - r0 * std::cos(q * r0));
+    double Fi = 0.0;
+    for (int j = 0; j < n - 1; ++j) {
+      const double rj = x[j], rj1 = x[j + 1];
+      const double sqrj = std::sin(q * rj), cqrj = std::cos(q * rj);
+      const double sqrj1 = std::sin(q * rj1), cqrj1 = std::cos(q * rj1);
+      const double A_ = a[j], B_ = b[j], C_ = c[j], D_ = d[j];
+      Fi = Fi + (A_ + (B_ + (C_ + D_ * rj) * rj) * rj) * rj * c1oq * cqrj -
+           (A_ + (B_ + (C_ + D_ * rj1) * rj1) * rj1) * rj1 * c1oq * cqrj1 +
+           (A_ + (2.0 * B_ + (3.0 * C_ + 4.0 * D_ * rj1) * rj1) * rj1) * c1oq2 * sqrj1 -
+           (A_ + (2.0 * B_ + (3.0 * C_ + 4.0 * D_ * rj) * rj) * rj) * c1oq2 * sqrj +
+           (2.0 * B_ + (6.0 * C_ + 12.0 * D_ * rj1) * rj1) * c1oq3 * cqrj1 -
+           (2.0 * B_ + (6.0 * C_ + 12.0 * D_ * rj) * rj) * c1oq3 * cqrj +
+           (6.0 * C_ + 24.0 * D_ * rj) * c1oq4 * sqrj - (6.0 * C_ + 24.0 * D_ * rj1) * c1oq4 * sqrj1 +
+           24.0 * D_ * c1oq5 * (cqrj - cqrj1);
+    }
+    return (Vp + Fi) * c1oq * Qpi;
+  }
+
+  // The spline of V on [r_cutoff + eps, r_max] (FT_V_spline.f90:83-120).
+  static void radial_spline(const PairPot& v, int n, std::vector<double>& x, std::vector<double>& a,
+                            std::vector<double>& b, std::vector<double>& c, std::vector<double>& d) {
+    const double X1 = v.rcut + kEps, XN = kRmax;
+    double r0 = X1, r1 = r0 + kDr, r2 = r1 + kDr;
+    const double S1 = (v(r0) - 2.0 * v(r1) + v(r2)) / (kDr * kDr);
+    r0 = XN;
+    const double Sn = (v(r0 - kDr) - 2.0 * v(r0) + v(r0 + kDr)) / (kDr * kDr);
+    const double h = (XN - X1) / (n - 1);
+    x.resize(n); a.resize(n); b.resize(n); c.resize(n); d.resize(n);
+    std::vector<double> y(n);
+    for (int i = 1; i <= n; ++i) {
+      const double r = (i - 1) * h + X1;
+      x[i - 1] = r;
+      y[i - 1] = v(r);
+    }
+    spline_maron(x.data(), y.data(), a.data(), b.data(), c.data(), d.data(), S1, Sn, n);
+  }
+
+  // Table of Vpp at P_p (i-1)*hp after the small-q redefinition, and its spline.
+  void build(const PairPot& v, double pmax, double hp, int n, bool parabolic) {
+    std::vector<double> x, a, b, c, d;
+    radial_spline(v, n, x, a, b, c, d);
+    np = (int)(pmax / hp + 1.5);
+    P.resize(np); Vpp.resize(np);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < np; ++i) {
+      const double p = i * hp;
+      P[i] = p;
+      Vpp[i] = transform(p, v, parabolic, x, a, b, c, d, n);
+    }
+    redefine_small_q(P, Vpp);
+    A.resize(np); B.resize(np); C.resize(np); D.resize(np);
+    spline_maron(P.data(), Vpp.data(), A.data(), B.data(), C.data(), D.data(), 0.0, 0.0, np);
+  }
+  static void redefine_small_q(const std::vector<double>& P, std::vector<double>& V) {
+    const int np = (int)P.size();
+    double x[4] = {0.0, 0, 0, 0}, y[4] = {V[0], 0, 0, 0};
+    int iaux = 1;
+    for (int i = 2; i <= np; ++i) {
+      const double p = P[i - 1];
+      if (p > kSmallQ) {
+        ++iaux;
+        x[iaux - 1] = p;
+        y[iaux - 1] = V[i - 1];
+      }
+      if (iaux == 4) break;
+    }
+    double a[4], b[4], c[4], d[4];
+    spline_maron(x, y, a, b, c, d, 0.0, 0.0, 4);
+    for (int i = 2; i <= np; ++i) {
+      const double p = P[i - 1];
+      if (p <= kSmallQ) V[i - 1] = a[0] + p * (b[0] + p * (c[0] + p * d[0]));
+      else break;
+    }
+  }
+  double eval(double p) const {
+    const int k = findi(P.data(), p, np) - 1;
+    return A[k] + p * (B[k] + p * (C[k] + p * D[k]));
+  }
+};
+
+// ------------------------------------------------------------------------------------------------
+// Real-time TDDFT with quantum impurities (Dynamics_quantum_impurities): the impurities are wave
+// functions psix_i with masses m_imp_u(i) and He-X kernels uimp_k (FT_V_spline of the pair
+// potential) and X-X kernels uimp_k_k.
+// ------------------------------------------------------------------------------------------------
+struct QDyn : Common {
+  int ni = 0;
+  double mu4 = 0.0;
+  std::vector<double> h2o2mx;
+  std::vector<cplx> psi, pc, q, timec, s1, s2, s3, s4, s5, wk2;
+  std::vector<cplx> psiold[3], hpsiold[2];
+  std::vector<std::vector<cplx>> psix, pcx, qx, psixold, hpsixold;  // [i], [3i+s], [2i+s]
+  std::vector<std::vector<double>> upotx, uimpk, uimpkk;             // uimpkk[i + ni j]
+  std::vector<double> potx4, sto2, sto1x;
+  int ioldp[3] = {1, 2, 3}, ioldh[2] = {1, 2};
+  std::vector<int> ioldpx, ioldhx;  // (3, N_imp), (2, N_imp) as in the rkpc module
+
+  // potenimpini (Dynamics_quantum_impurities/potenimpini.f90:116-163): qmax = max(100,
+  // |pmax|), Nq = max(10001, nq), Hq = qmax/(Nq-1), uimp_k = FT_V_spline(pmod), and uimp_k_k
+  // for the non-'null' pairs i != j.
+  void init(const ho_params& pp, int n, const double* m_imp_u, double mu, const double* hex,
+            const double* xx, int nspline, int nq, int parabolic) {
+    init_common(pp);
+    ni = n;
+    mu4 = mu;
+    const long N = g.nxyz;
+    for (auto* v : {&psi, &pc, &q, &timec, &s1, &s2, &s3, &s4, &s5}) v->assign(N, 0);
+    for (auto& v : psiold) v.assign(N, 0);
+    for (auto& v : hpsiold) v.assign(N, 0);
+    wk2.assign(g.nk, 0);
+    potx4.assign(N, 0); sto2.assign(N, 0); sto1x.assign(N, 0);
+    psix.assign(ni, std::vector<cplx>(N)); pcx = psix; qx = psix;
+    psixold.assign(3 * ni, std::vector<cplx>(N)); hpsixold.assign(2 * ni, std::vector<cplx>(N));
+    upotx.assign(ni, std::vector<double>(N));
+    h2o2mx.resize(ni);
+    for (int i = 0; i < ni; ++i) h2o2mx[i] = p.h2o2m4 * 4.002603 / m_imp_u[i];
+    ioldpx.resize(3 * ni); ioldhx.resize(2 * ni);
+    for (int i = 0; i < ni; ++i) {
+      for (int s = 0; s < 3; ++s) ioldpx[3 * i + s] = s + 1;
+      for (int s = 0; s < 2; ++s) ioldhx[2 * i + s] = s + 1;
+    }
+    for (int k = 0; k < g.nz; ++k)  // timec: Dynamics_quantum_impurities/DFT4He3d.f90:581-591
+      for (int j = 0; j < g.ny; ++j)
+        for (int i = 0; i < g.nx; ++i) {
+          double s = 1.0 + std::tanh((std::fabs(g.x[i]) - p.txmean) / p.txsurf);
+          s = s + 1.0 + std::tanh((std::fabs(g.y[j]) - p.tymean) / p.tysurf);
+          s = s + 1.0 + std::tanh((std::fabs(g.z[k]) - p.tzmean) / p.tzsurf);
+          timec[i + (long)g.nx * (j + (long)g.ny * k)] = cplx(p.lambdah * s, 1.0);
+        }
+    const double pmx = 1.0 / (2.0 * g.hx), pmy = 1.0 / (2.0 * g.hy), pmz = 1.0 / (2.0 * g.hz);
+    const double qmax = std::max(100.0, std::sqrt(pmx * pmx + pmy * pmy + pmz * pmz));
+    const long Nq = std::max(10001L, (long)nq);
+    const double Hq = qmax / (double)(Nq - 1);
+    auto pot = [](const double* v) {
+      PairPot pp_;
+      pp_.kind = (int)v[0]; pp_.D = v[1]; pp_.re = v[2]; pp_.a = v[3]; pp_.rcut = v[4]; pp_.umax = v[5];
+      return pp_;
+    };
+    std::vector<std::pair<PairPot, FTVSpline>> cache;
+    auto table = [&](const PairPot& v) -> const FTVSpline& {
+      for (auto& e : cache)
+        if (e.first.same(v)) return e.second;
+      cache.emplace_back(v, FTVSpline());
+      cache.back().second.build(v, qmax, Hq, nspline, parabolic != 0);
+      return cache.back().second;
+    };
+    uimpk.assign(ni, std::vector<double>());
+    uimpkk.assign((size_t)ni * ni, std::vector<double>());
+    for (int i = 0; i < ni; ++i) {
+      const FTVSpline& t = table(pot(hex + 6 * i));
+      uimpk[i].resize(g.nk);
+#pragma omp parallel for schedule(static)
+      for (long k = 0; k < g.nk; ++k) uimpk[i][k] = t.eval(g.pmod[k]);
+      for (int j = 0; j < ni; ++j) {
+        const double* v = xx + 6 * (i + (size_t)ni * j);
+        if (i == j || (int)v[0] == 0) continue;
+        const FTVSpline& tj = table(pot(v));
+        auto& dst = uimpkk[i + (size_t)ni * j];
+        dst.resize(g.nk);
+#pragma omp parallel for schedule(static)
+        for (long k = 0; k < g.nk; ++k) dst[k] = tj.eval(g.pmod[k]);
+      }
+    }
+  }
+
+  void density() {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < g.nxyz; ++i) den[i] = std::norm(psi[i]);
+  }
+  // Sto1 = psix*conjg(psix) (real part), R2C into wk1.
+  void fft_denx(int i) {
+    const cplx* f = psix[i].data();
+#pragma omp parallel for schedule(static)
+    for (long k = 0; k < g.nxyz; ++k) sto1x[k] = f[k].real() * f[k].real() + f[k].imag() * f[k].imag();
+    fft.r2c(sto1x.data(), wk1.data());
+  }
+  // potenimp: Dynamics_quantum_impurities/potenimp.f90:1-43.
+  void potenimp() {
+    fftfw_den();
+    const long N = g.nxyz;
+    std::fill(potx4.begin(), potx4.end(), 0.0);
+    for (int i = 0; i < ni; ++i) {
+      fft_denx(i);
+      for (long k = 0; k < g.nk; ++k) wk2[k] = wk1[k] * uimpk[i][k];
+      fft.c2r(wk2.data(), sto2.data(), renor);
+      for (long k = 0; k < N; ++k) potx4[k] = potx4[k] + sto2[k];
+      for (long k = 0; k < g.nk; ++k) wk2[k] = fden[k] * uimpk[i][k];
+      fft.c2r(wk2.data(), upotx[i].data(), renor);
+      for (int j = 0; j < ni; ++j) {
+        const auto& kk = uimpkk[i + (size_t)ni * j];
+        if (j == i || kk.empty()) continue;
+        fft_denx(j);
+        for (long k = 0; k < g.nk; ++k) wk2[k] = wk1[k] * kk[k];
+        fft.c2r(wk2.data(), sto2.data(), renor);
+        for (long k = 0; k < N; ++k) upotx[i][k] = upotx[i][k] + sto2[k];
+      }
+    }
+  }
+  // poten: Dynamics_quantum_impurities/poten.f90:5-155 (fden comes from potenimp).
+  void poten() {
+    coarse_grain();
+    lennard_jones();
+    correlation_and_assembly(potx4.data());
+  }
+  // s4 = timec*((d2x+d2y+d2z)*h2o2m - (pot - shift)*f)  (steprk.f90:68,94; steppc.f90:46,77).
+  void hpsi_q(const std::vector<cplx>& f, const std::vector<double>& pot, double shift, double h2) {
+    deriv3d<cplx>(2, g, 0, p.icon, w1, w2, f.data(), s1.data());
+    deriv3d<cplx>(2, g, 1, p.icon, w1, w2, f.data(), s2.data());
+    deriv3d<cplx>(2, g, 2, p.icon, w1, w2, f.data(), s3.data());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < g.nxyz; ++i) {
+      const cplx lap = s1[i] + s2[i] + s3[i];
+      s4[i] = timec[i] * (lap * h2 - (pot[i] - shift) * f[i]);
+    }
+  }
+
+  // steprk: Dynamics_quantum_impurities/steprk.f90:1-124.
+  void steprk(double deltat) {
+    const double arun[4] = {0.5, 1.0 - 1.0 / std::sqrt(2.0), 1.0 + 1.0 / std::sqrt(2.0), 1.0 / 6.0};
+    const double brun[4] = {2.0, 1.0, 1.0, 2.0};
+    const double crun[4] = {0.5, 1.0 - 1.0 / std::sqrt(2.0), 1.0 + 1.0 / std::sqrt(2.0), 0.5};
+    const long N = g.nxyz;
+    auto stage = [&](int jr, std::vector<cplx>& f, std::vector<cplx>& qq, std::vector<cplx>* po,
+                     std::vector<cplx>* ho) {
+      if (jr == 0) {
+        ho[1] = ho[0];
+        ho[0] = s4;
+        po[2] = po[1];
+        po[1] = po[0];
+        po[0] = f;
+      }
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < N; ++i) {
+        const cplx sto1c = arun[jr] * (s4[i] - brun[jr] * qq[i]);
+        qq[i] = qq[i] + 3.0 * sto1c - crun[jr] * s4[i];
+        f[i] = f[i] + deltat * sto1c;
+      }
+    };
+    for (int jr = 0; jr < 4; ++jr) {
+      hpsi_q(psi, pot4, mu4, p.h2o2m4);
+      stage(jr, psi, q, psiold, hpsiold);
+      density();
+      for (int i = 0; i < ni; ++i) {
+        hpsi_q(psix[i], upotx[i], 0.0, h2o2mx[i]);
+        stage(jr, psix[i], qx[i], &psixold[3 * i], &hpsixold[2 * i]);
+      }
+      if (jr <= 2) { potenimp(); poten(); }
+    }
+    for (int s = 0; s < 3; ++s) {
+      ioldp[s] = s + 1;
+      for (int i = 0; i < ni; ++i) ioldpx[3 * i + s] = s + 1;
+    }
+    for (int s = 0; s < 2; ++s) {
+      ioldh[s] = s + 1;
+      for (int i = 0; i < ni; ++i) ioldhx[2 * i + s] = s + 1;
+    }
+  }
+
+  // steppc: Dynamics_quantum_impurities/steppc.f90:1-157.
+  void steppc(double deltat, double* errHe, double* errpsix) {
+    const double c112 = 112.0 / 121.0, c9 = 9.0 / 121.0, c4o3 = 4.0 / 3.0;
+    const long N = g.nxyz;
+    auto predict = [&](std::vector<cplx>& f, std::vector<cplx>& pcc, std::vector<cplx>* po,
+                       std::vector<cplx>* ho, int* ip, int* ih) {
+      std::vector<cplx>& po3 = po[ip[2] - 1];
+      const std::vector<cplx>& h1 = ho[ih[0] - 1];
+      std::vector<cplx>& h2 = ho[ih[1] - 1];
+      const double s = c4o3 * deltat;
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < N; ++i) {
+        const cplx sto1c = po3[i] + s * (2.0 * s4[i] - h1[i] + 2.0 * h2[i]);
+        po3[i] = f[i];
+        f[i] = sto1c - c112 * pcc[i];
+        pcc[i] = sto1c;
+        h2[i] = s4[i];
+      }
+      std::swap(ih[0], ih[1]);
+    };
+    auto correct = [&](std::vector<cplx>& f, std::vector<cplx>& pcc, std::vector<cplx>* po,
+                       std::vector<cplx>* ho, const int* ip, const int* ih) {
+      const std::vector<cplx>& po3 = po[ip[2] - 1];
+      const std::vector<cplx>& po2 = po[ip[1] - 1];
+      const std::vector<cplx>& h1 = ho[ih[0] - 1];
+      const std::vector<cplx>& h2 = ho[ih[1] - 1];
+      const double s3 = 3.0 * deltat;
+      double sabs = 0.0;
+#pragma omp parallel for reduction(+ : sabs) schedule(static)
+      for (long i = 0; i < N; ++i) {
+        const cplx sto5c = 0.125 * (9.0 * po3[i] - po2[i] + s3 * (s4[i] + 2.0 * h1[i] - h2[i]));
+        pcc[i] = pcc[i] - sto5c;
+        f[i] = sto5c + c9 * pcc[i];
+        sabs += std::abs(pcc[i]);
+      }
+      return c9 * sabs;
+    };
+    auto rotate = [](int* ip) {
+      const int a = ip[2];
+      ip[2] = ip[1]; ip[1] = ip[0]; ip[0] = a;
+    };
+    hpsi_q(psi, pot4, mu4, p.h2o2m4);
+    predict(psi, pc, psiold, hpsiold, ioldp, ioldh);
+    density();
+    for (int i = 0; i < ni; ++i) {
+      hpsi_q(psix[i], upotx[i], 0.0, h2o2mx[i]);
+      predict(psix[i], pcx[i], &psixold[3 * i], &hpsixold[2 * i], &ioldpx[3 * i], &ioldhx[2 * i]);
+    }
+    potenimp();
+    poten();
+    hpsi_q(psi, pot4, mu4, p.h2o2m4);
+    double eh = correct(psi, pc, psiold, hpsiold, ioldp, ioldh);
+    density();
+    double ex = 0.0;
+    for (int i = 0; i < ni; ++i) {
+      hpsi_q(psix[i], upotx[i], 0.0, h2o2mx[i]);
+      ex = ex + correct(psix[i], pcx[i], &psixold[3 * i], &hpsixold[2 * i], &ioldpx[3 * i], &ioldhx[2 * i]);
+    }
+    if (errpsix) *errpsix = ex / (double)N;
+    if (errHe) *errHe = eh / (double)N;
+    rotate(ioldp);
+    for (int i = 0; i < ni; ++i) rotate(&ioldpx[3 * i]);
+  }
+
+  // energy: Dynamics_quantum_impurities/energy.f90:12-139.  out = {etot4, ekin4, elj4, ecor4,
+  // esolid, ealphas, ekinx, eHeX, eimpu_impu, eimpu, etot}.
+  void energy(double* out) {
+    const long N = g.nxyz;
+    auto grad2 = [&](const std::vector<cplx>& f) {
+      deriv3d<cplx>(1, g, 0, p.icon, w1, w2, f.data(), s1.data());
+      deriv3d<cplx>(1, g, 1, p.icon, w1, w2, f.data(), s2.data());
+      deriv3d<cplx>(1, g, 2, p.icon, w1, w2, f.data(), s3.data());
+      double ek = 0;
+#pragma omp parallel for reduction(+ : ek) schedule(static)
+      for (long i = 0; i < N; ++i) ek += std::norm(s1[i]) + std::norm(s2[i]) + std::norm(s3[i]);
+      return ek;
+    };
+    const double ek = grad2(psi);
+    double ekin4, elj4, ecor4, esolid;
+    he_energy_sums(ek, &ekin4, &elj4, &ecor4, &esolid);
+    const double etot4 = ekin4 + elj4 + ecor4 + esolid;
+    double ekinx = 0.0;
+    std::fill(wk2.begin(), wk2.end(), cplx(0.0));
+    for (int k = 0; k < ni; ++k) {
+      ekinx = ekinx + h2o2mx[k] * grad2(psix[k]);
+      fft_denx(k);
+      for (long i = 0; i < g.nk; ++i) wk2[i] = wk2[i] + wk1[i] * uimpk[k][i];
+    }
+    ekinx = ekinx * g.dxyz;
+    fft.c2r(wk2.data(), sto2.data(), renor);
+    double sh = 0;
+#pragma omp parallel for reduction(+ : sh) schedule(static)
+    for (long i = 0; i < N; ++i) sh += sto2[i] * den[i];
+    const double eHeX = sh * g.dxyz;
+    double eii = 0.0;
+    for (int k = 0; k < ni; ++k) {
+      fft_denx(k);
+      for (int m = k + 1; m < ni; ++m) {
+        const auto& kk = uimpkk[k + (size_t)ni * m];
+        for (long i = 0; i < g.nk; ++i) wk2[i] = kk.empty() ? cplx(0.0) : wk1[i] * kk[i];
+        fft.c2r(wk2.data(), sto2.data(), renor);
+        double s = 0;
+        const cplx* f = psix[m].data();
+#pragma omp parallel for reduction(+ : s) schedule(static)
+        for (long i = 0; i < N; ++i) s += sto2[i] * (f[i].real() * f[i].real() + f[i].imag() * f[i].imag());
+        eii = eii + s;
+      }
+    }
+    eii = eii * g.dxyz;
+    const double eimpu = ekinx + eHeX + eii;
+    const double v[11] = {etot4, ekin4, elj4, ecor4, esolid, 0.0, ekinx, eHeX, eii, eimpu, etot4 + eimpu};
+    std::memcpy(out, v, sizeof(v));
+  }
+
+  // Norm and centre of |psix_k|^2 (Dynamics_quantum_impurities/DFT4He3d.f90:682-700):
+  // out[4k..4k+3] = {sum |psix|^2 dxyz, <x>, <y>, <z>}.
+  void moments(double* out) const {
+    for (int k = 0; k < ni; ++k) {
+      double a = 0, ax = 0, ay = 0, az = 0;
+      const cplx* f = psix[k].data();
+#pragma omp parallel for collapse(2) reduction(+ : a, ax, ay, az) schedule(static)
+      for (int iz = 0; iz < g.nz; ++iz)
+        for (int iy = 0; iy < g.ny; ++iy)
+          for (int ix = 0; ix < g.nx; ++ix) {
+            const cplx v = f[ix + (long)g.nx * (iy + (long)g.ny * iz)];
+            const double s = v.real() * v.real() + v.imag() * v.imag();
+            a += s; ax += s * g.x[ix]; ay += s * g.y[iy]; az += s * g.z[iz];
+          }
+      a = a * g.dxyz;
+      out[4 * k] = a;
+      out[4 * k + 1] = ax * g.dxyz / a;
+      out[4 * k + 2] = ay * g.dxyz / a;
+      out[4 * k + 3] = az * g.dxyz / a;
+    }
+  }
+};
+
+// ------------------------------------------------------------------------------------------------
 // Imaginary-time statics (He_statics), pure droplet, real psi.
 // ------------------------------------------------------------------------------------------------
 struct Stat : Common {
@@ -1135,6 +1654,53 @@ static double* stat_field(Stat* d, const char* name, long* n) {
   return nullptr;
 }
 
+static double* qdyn_field(QDyn* d, const char* name, long* n) {
+  std::string s(name);
+  const long N = d->g.nxyz, K = d->g.nk;
+  int idx = 0;
+  const size_t colon = s.find(':');
+  if (colon != std::string::npos) {
+    idx = std::atoi(s.c_str() + colon + 1);
+    s = s.substr(0, colon);
+  }
+  auto R = [&](std::vector<double>& v, long nn) { *n = nn; return v.data(); };
+  auto C = [&](std::vector<cplx>& v, long nn) { *n = 2 * nn; return (double*)v.data(); };
+  const bool ok = idx >= 0 && idx < d->ni;
+  if (s == "den") return R(d->den, N);
+  if (s == "dencg") return R(d->dencg, N);
+  if (s == "delj4") return R(d->delj4, N);
+  if (s == "pot4") return R(d->pot4, N);
+  if (s == "potx4") return R(d->potx4, N);
+  if (s == "fvlj4") return R(d->fvlj4, K);
+  if (s == "wcgk") return R(d->wcgk, K);
+  if (s == "psi") return C(d->psi, N);
+  if (s == "pc") return C(d->pc, N);
+  if (s == "q") return C(d->q, N);
+  if (s == "fden") return C(d->fden, K);
+  if (s == "psiold1") return C(d->psiold[0], N);
+  if (s == "psiold2") return C(d->psiold[1], N);
+  if (s == "psiold3") return C(d->psiold[2], N);
+  if (s == "hpsiold1") return C(d->hpsiold[0], N);
+  if (s == "hpsiold2") return C(d->hpsiold[1], N);
+  if (!ok) return nullptr;
+  if (s == "psix") return C(d->psix[idx], N);
+  if (s == "pcx") return C(d->pcx[idx], N);
+  if (s == "qx") return C(d->qx[idx], N);
+  if (s == "upotx") return R(d->upotx[idx], N);
+  if (s == "uimpk") return R(d->uimpk[idx], K);
+  if (s == "psixold1" || s == "psixold2" || s == "psixold3")
+    return C(d->psixold[3 * idx + (s[7] - '1')], N);
+  if (s == "hpsixold1" || s == "hpsixold2") return C(d->hpsixold[2 * idx + (s[8] - '1')], N);
+  if (s.rfind("uimpkk", 0) == 0) {  // "uimpkk:i" with j in name "uimpkk<j>:i"
+    const int j = (s.size() > 6) ? std::atoi(s.c_str() + 6) : 0;
+    if (j < 0 || j >= d->ni) return nullptr;
+    auto& v = d->uimpkk[idx + (size_t)d->ni * j];
+    if (v.empty()) return nullptr;
+    return R(v, K);
+  }
+  return nullptr;
+}
+
 extern "C" {
 // Generic helpers (tests).
 double ho_sine_integral(double x) { return sine_integral(x); }
@@ -1222,4 +1788,63 @@ void ho_stat_steppcr(void* h, double dt, double* mu, double* muerr, int n4) {
 double ho_stat_errpc(void* h) { return ((Stat*)h)->errpc; }
 void ho_stat_energy(void* h, double* out) { ((Stat*)h)->energy(out); }
 double ho_stat_varmu(void* h, int npart, double mu) { return ((Stat*)h)->varmu(npart, mu); }
+
+// Quantum impurities.  he_x: n_imp rows of {kind, D, re, a, r_cutoff, umax}; x_x: n_imp^2 rows
+// (i + n_imp*j), kind 0 = 'null'.
+void* ho_qdyn_create(const ho_params* p, int n_imp, const double* m_imp_u, double mu4,
+                     const double* he_x, const double* x_x, int nspline, int nq, int parabolic) {
+  QDyn* d = new QDyn();
+  d->init(*p, n_imp, m_imp_u, mu4, he_x, x_x, nspline, nq, parabolic);
+  return d;
+}
+void ho_qdyn_destroy(void* h) { delete (QDyn*)h; }
+double* ho_qdyn_field(void* h, const char* name, long* n) { return qdyn_field((QDyn*)h, name, n); }
+void ho_qdyn_potenimp(void* h) { ((QDyn*)h)->potenimp(); }
+void ho_qdyn_poten(void* h) { ((QDyn*)h)->poten(); }
+void ho_qdyn_steprk(void* h, double dt) { ((QDyn*)h)->steprk(dt); }
+void ho_qdyn_steppc(void* h, double dt, double* err2) { ((QDyn*)h)->steppc(dt, &err2[0], &err2[1]); }
+void ho_qdyn_energy(void* h, double* out) { ((QDyn*)h)->energy(out); }
+void ho_qdyn_moments(void* h, double* out) { ((QDyn*)h)->moments(out); }
+void ho_qdyn_ring(void* h, int* r, int set) {
+  QDyn* d = (QDyn*)h;
+  int* dst[5] = {&d->ioldp[0], &d->ioldp[1], &d->ioldp[2], &d->ioldh[0], &d->ioldh[1]};
+  for (int i = 0; i < 5; ++i) {
+    if (set) *dst[i] = r[i];
+    else r[i] = *dst[i];
+  }
+  for (int k = 0; k < d->ni; ++k) {
+    for (int s = 0; s < 3; ++s) {
+      if (set) d->ioldpx[3 * k + s] = r[s];
+    }
+    for (int s = 0; s < 2; ++s) {
+      if (set) d->ioldhx[2 * k + s] = r[3 + s];
+    }
+  }
+}
+// Vpp(P_p(i)), i < n_p, of FT_V_spline for one pair potential (after the small-q redefinition),
+// and the spline evaluation at arbitrary momenta.
+int ho_ft_vpp_table(const double* pot, double pmax, double hp, int nspline, int parabolic,
+                    double* vpp, int n_p) {
+  PairPot v;
+  v.kind = (int)pot[0]; v.D = pot[1]; v.re = pot[2]; v.a = pot[3]; v.rcut = pot[4]; v.umax = pot[5];
+  FTVSpline t;
+  t.build(v, pmax, hp, nspline, parabolic != 0);
+  if (n_p != t.np) return t.np;
+  std::memcpy(vpp, t.Vpp.data(), sizeof(double) * n_p);
+  return n_p;
+}
+// One raw transform value (no small-q redefinition) at momentum p.
+double ho_ft_vpp_point(const double* pot, double p, int nspline, int parabolic) {
+  PairPot v;
+  v.kind = (int)pot[0]; v.D = pot[1]; v.re = pot[2]; v.a = pot[3]; v.rcut = pot[4]; v.umax = pot[5];
+  std::vector<double> x, a, b, c, d;
+  FTVSpline::radial_spline(v, nspline, x, a, b, c, d);
+  return FTVSpline::transform(p, v, parabolic != 0, x, a, b, c, d, nspline);
+}
+// The spline of mates.f (for tests against an independent spline).
+void ho_spline(const double* x, const double* y, double s1, double sn, int n, double* a, double* b,
+               double* c, double* d) {
+  spline_maron(x, y, a, b, c, d, s1, sn, n);
+}
+int ho_findi(const double* x, double xc, int n) { return findi(x, xc, n); }
 }

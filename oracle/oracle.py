@@ -108,6 +108,26 @@ def lib():
         L.ho_stat_energy.argtypes = [vp, dp]
         L.ho_stat_varmu.restype = ctypes.c_double
         L.ho_stat_varmu.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        ci, cd = ctypes.c_int, ctypes.c_double
+        L.ho_qdyn_create.restype = vp
+        L.ho_qdyn_create.argtypes = [P, ci, dp, cd, dp, dp, ci, ci, ci]
+        L.ho_qdyn_destroy.argtypes = [vp]
+        L.ho_qdyn_field.restype = dp
+        L.ho_qdyn_field.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long)]
+        for f in ("potenimp", "poten"):
+            getattr(L, "ho_qdyn_" + f).argtypes = [vp]
+        L.ho_qdyn_steprk.argtypes = [vp, cd]
+        L.ho_qdyn_steppc.argtypes = [vp, cd, dp]
+        L.ho_qdyn_energy.argtypes = [vp, dp]
+        L.ho_qdyn_moments.argtypes = [vp, dp]
+        L.ho_qdyn_ring.argtypes = [vp, ctypes.POINTER(ci), ci]
+        L.ho_ft_vpp_table.restype = ci
+        L.ho_ft_vpp_table.argtypes = [dp, cd, cd, ci, ci, dp, ci]
+        L.ho_ft_vpp_point.restype = cd
+        L.ho_ft_vpp_point.argtypes = [dp, cd, ci, ci]
+        L.ho_spline.argtypes = [dp, dp, cd, cd, ci, dp, dp, dp, dp]
+        L.ho_findi.restype = ci
+        L.ho_findi.argtypes = [dp, cd, ci]
         _lib = L
     return _lib
 
@@ -273,3 +293,96 @@ def bickley13():
     w1, w2 = np.zeros(13), np.zeros(13)
     lib().ho_bickley13(_dp(w1), _dp(w2))
     return w1, w2
+
+
+class QDynamics(_Fields):
+    """Dynamics_quantum_impurities module state + potenimp/poten/steprk/steppc/energy.
+    Per-impurity fields are named "psix:0", "upotx:1", "uimpk:0", ...; "uimpkk<j>:<i>" is
+    uimp_k_k(:,:,:,i,j)."""
+    COMPLEX_BASE = {"psi", "pc", "q", "fden", "psiold1", "psiold2", "psiold3", "hpsiold1",
+                    "hpsiold2", "psix", "pcx", "qx", "psixold1", "psixold2", "psixold3",
+                    "hpsixold1", "hpsixold2"}
+
+    class _C:
+        def __contains__(self, name):
+            return name.split(":")[0] in QDynamics.COMPLEX_BASE
+
+    COMPLEX = _C()
+
+    def __init__(self, cfg, nthreads=0):
+        from he_dft_2024_b200 import config as C  # pair rows share the product's workload layout
+        self.L = lib()
+        self.p = make_params(cfg, nthreads)
+        w = C.Workload(**{k: v for k, v in cfg.items() if k in C.Workload.__dataclass_fields__})
+        hex_, xx = C.pair_rows(w)
+        self.ni = w.nq_imp
+        m = np.asarray(list(w.mq_imp_u) + [0.0], dtype=np.float64)
+        hex_ = np.ascontiguousarray(hex_.ravel())
+        xx = np.ascontiguousarray(xx.ravel()) if xx.size else np.zeros(6)
+        self.h = self.L.ho_qdyn_create(ctypes.byref(self.p), self.ni, _dp(m), w.mu4, _dp(hex_),
+                                       _dp(xx), w.n_spline, w.nq, w.parabolic)
+        self._field_fn = self.L.ho_qdyn_field
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ho_qdyn_destroy(self.h)
+            self.h = None
+
+    def potenimp(self): self.L.ho_qdyn_potenimp(self.h)
+    def poten(self): self.L.ho_qdyn_poten(self.h)
+    def steprk(self, dt): self.L.ho_qdyn_steprk(self.h, dt)
+
+    def steppc(self, dt):
+        e = np.zeros(2)
+        self.L.ho_qdyn_steppc(self.h, dt, _dp(e))
+        return tuple(e)
+
+    def energy(self):
+        e = np.zeros(11)
+        self.L.ho_qdyn_energy(self.h, _dp(e))
+        return dict(zip(ENERGY_KEYS, e))
+
+    def moments(self):
+        out = np.zeros(4 * self.ni)
+        self.L.ho_qdyn_moments(self.h, _dp(out))
+        return out.reshape(self.ni, 4)
+
+    def ring(self, values=None):
+        r = (ctypes.c_int * 5)()
+        if values is not None:
+            for i, v in enumerate(values[:5]):
+                r[i] = int(v)
+            self.L.ho_qdyn_ring(self.h, r, 1)
+            return list(values[:5])
+        self.L.ho_qdyn_ring(self.h, r, 0)
+        return list(r)
+
+
+def ft_vpp_table(pot, pmax, hp, nspline=100001, parabolic=0):
+    """FT_V_spline's Vpp table (after the small-q redefinition) for pot = {kind,D,re,a,rcut,umax}."""
+    pot = np.ascontiguousarray(pot, dtype=np.float64)
+    n_p = int(pmax / hp + 1.5)
+    out = np.zeros(n_p)
+    got = lib().ho_ft_vpp_table(_dp(pot), pmax, hp, nspline, parabolic, _dp(out), n_p)
+    assert got == n_p, (got, n_p)
+    return out
+
+
+def ft_vpp_point(pot, p, nspline=100001, parabolic=0):
+    pot = np.ascontiguousarray(pot, dtype=np.float64)
+    return lib().ho_ft_vpp_point(_dp(pot), p, nspline, parabolic)
+
+
+def spline(x, y, s1, sn):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    n = len(x)
+    a, b, c, d = (np.zeros(n) for _ in range(4))
+    lib().ho_spline(_dp(x), _dp(y), s1, sn, n, _dp(a), _dp(b), _dp(c), _dp(d))
+    return a, b, c, d
+
+
+def findi(x, xc):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().ho_findi(_dp(x), float(xc), len(x))
+
