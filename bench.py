@@ -36,6 +36,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "TDDFT grid-pt-steps/s (FP64, 128^3 classical-impurity steppc loop)"
+METRIC_Q = "TDDFT grid-pt-steps/s (FP64, 192^3 quantum impurity, batch of trajectories)"
+REF_MAX_STEPS = 40
 UNIT = "grid-pt-steps/s"
 
 # Algorithmic bytes per grid point of each kernel (binary64; N-sized field = 8 B real / 16 B
@@ -335,6 +337,123 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def quantum_bytes_per_point(nx):
+    """Algorithmic bytes per grid point of the quantum kernels (binary64, see kernel_bytes_per_point)."""
+    hk = (nx // 2 + 1) / nx
+    c, r = 16.0, 8.0
+    return {
+        # psi, pot, psiold(ioldp3), hpsiold x2, pc -> psi_new, pc, hpsiold, den
+        "hpsi_pmc_predict_q": (c + r + c + 2 * c + c) + (c + c + c + r),
+        "hpsi_pmc_correct_q": (c + r + 2 * c + 2 * c + c) + (c + c + r),
+        "hpsi_rkgill_stage_q": (c + r + c) + (c + c + r),
+        "fft_x_r2c_den": r + c * hk,
+        "fft_x_c2r_cg_lj_r2c_corr": 2 * c * hk + r + 2 * r + c * hk,
+        "fft_x_c2r_cg_lj": 2 * c * hk + 2 * r,
+        "fft_x_c2r_pot4": c * hk + 4 * r + r,
+        "fft_y": 2 * c * hk,
+        "fft_z_conv1": 2 * c * hk + r * hk,
+        "fft_z_conv2": c * hk + 3 * c * hk + 2 * r * hk,
+        "fft_z_mix_fwd": c * hk + 2 * c * hk + c * hk + r * hk,
+    }
+
+
+def run_quantum(args):
+    """The batched quantum-impurity workload: args.batch trajectories of 4He_2000 on 192^3 with
+    one 23 u quantum impurity each (seeded kicks), one context per trajectory on one stream; a
+    step advances every trajectory by one loop iteration (steppc + potenimp + poten)."""
+    import torch
+    from he_dft_2024_b200 import config as C, driver as D
+    from he_dft_2024_b200.context import Context
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    ws_ = ws
+    batch = C.quantum_batch(count=args.batch, n=args.n if args.n != 128 else 192, seed=1234 + rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctxs = []
+    t0 = time.perf_counter()
+    for w in batch:
+        c = Context(w, mode="quantum")
+        c.set_stream(stream.cuda_stream)
+        den = C.woods_saxon(w)
+        D.quantum_setup(c, D.initial_wavefunction(w, den), [C.psix_initial(w, 0)])
+        ctxs.append(c)
+    setup_s = time.perf_counter() - t0
+    w = batch[0]
+    for c in ctxs:
+        for it in range(1, 4):
+            D.quantum_iteration(c, it, w.deltat)
+    it = 4
+    for _ in range(args.warmup):
+        for c in ctxs:
+            D.quantum_iteration(c, it, w.deltat)
+        it += 1
+    torch.cuda.synchronize()
+    l0 = sum(c.launches for c in ctxs)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            for c in ctxs:
+                D.quantum_iteration(c, it, w.deltat)
+            it += 1
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    secs = ev0.elapsed_time(ev1) / 1e3
+    launches = sum(c.launches for c in ctxs) - l0
+    N = w.n
+    value = N * args.steps * len(ctxs) * ws_ / secs
+    # e2e: every step the host reads errHe/errpsix and the impurity trajectory (moments) of
+    # every trajectory, as the driver writes them per step.
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        for c in ctxs:
+            D.quantum_iteration(c, it, w.deltat, errors=True)
+            c.qimp_moments()
+        it += 1
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t1
+    ctxs[0].timing(True)
+    for _ in range(3):
+        D.quantum_iteration(ctxs[0], it, w.deltat)
+        it += 1
+    rep = ctxs[0].timing_report()
+    ctxs[0].timing(False)
+    tot = sum(v[1] for v in rep.values())
+    bpp = quantum_bytes_per_point(w.nx)
+    peak, peak_kind = measured_peak()
+    breakdown = {k: {"launches": v[0], "ms_per_launch": v[1] / v[0], "share": v[1] / tot,
+                     "GB/s": (bpp[k] * N / (v[1] / v[0] / 1e3) / 1e9) if k in bpp else None}
+                 for k, v in sorted(rep.items(), key=lambda kv: -kv[1][1])}
+    name, (nl, kms) = max(rep.items(), key=lambda kv: kv[1][1])
+    achieved = bpp.get(name, 0.0) * N / (kms / nl / 1e3) / 1e9
+    line = {
+        "metric": METRIC_Q, "value": value, "unit": UNIT, "n_gpus": ws_, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "trajectories": len(ctxs), "grid": [w.nx, w.ny, w.nz],
+                   "n4": w.n4, "impurity": "23 u quantum, Morse He-X via FT_V_spline",
+                   "deltat_ps": w.deltatps, "parallelism": f"replicas{ws_}",
+                   "device_gb": sum(c.device_bytes for c in ctxs) / 1e9},
+        "e2e": {"value": N * args.steps * len(ctxs) / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": len(ctxs) * (16 + 32)},
+        "gpu_launches": launches,
+        "setup_s": setup_s,
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "alg_bytes_per_launch": bpp.get(name, 0.0) * N,
+                     "ms_per_launch": kms / nl},
+        "step_alg_bytes_per_point": 1032.0,
+        "step_roofline_frac": 1032.0 * N * args.steps * len(ctxs) / secs / 1e9 / peak,
+        "kernels": breakdown,
+        "clocks": clk.summary(),
+    }
+    for c in ctxs:
+        c.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -350,27 +469,32 @@ def run_reference(args):
     for it in range(1, 4):
         D.dynamics_iteration(o, it, w.deltat, w.n_imp)
     it = 4
-    for _ in range(args.warmup):
+    # Each timed step is one CPU iteration (~0.2 s on 16 cores at 128^3); the sample is capped
+    # so that the whole run stays within a few minutes whatever --steps asks for.
+    warm = min(args.warmup, 3)
+    steps = min(args.steps, REF_MAX_STEPS)
+    for _ in range(warm):
         D.dynamics_iteration(o, it, w.deltat, w.n_imp)
         it += 1
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         D.dynamics_iteration(o, it, w.deltat, w.n_imp)
         it += 1
     secs = time.perf_counter() - t0
-    v = w.n * args.steps / secs
+    v = w.n * steps / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "n4": w.n4, "n_imp": w.n_imp,
                    "deltat_ps": w.deltatps, "parallelism": "cpu"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} driver iterations of the {w.nx}^3 workload "
-                                   f"after the 3-iteration RK start and {args.warmup} warm-up "
-                                   "iterations (C++ restatement of the reference; the Fortran "
-                                   "reference cannot be built in this image)"},
+                         "sample": f"{steps} timed driver iterations of the {w.nx}^3 workload "
+                                   f"(of the {args.steps} requested) after the 3-iteration RK "
+                                   f"start and {warm} warm-up iterations (C++ restatement of the "
+                                   "reference; the Fortran reference cannot be built in this "
+                                   "image)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -385,8 +509,12 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="classical", choices=["classical", "quantum"])
+    ap.add_argument("--batch", type=int, default=16)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "quantum" and args.impl == "ours":
+        run_quantum(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
