@@ -24,7 +24,8 @@ FIELDS = dict(
     psiold3=11, hpsiold1=12, hpsiold2=13, dxden=14, dyden=15, dzden=16, hpsi=17, fvlj4=18,
     wcgk=19, rimp=20, vimp=21, aimp=22, F=23, rimpold=24, vimpold=25, aimpold=26, pcr=27, pcv=28,
     qr=29, qv=30, ring=31, psix=32, upotx=33, potx4=34, denx=35, pcx=36, qx=37, psixold=38,
-    hpsixold=39, uimpk=40, uimpkk=41)
+    hpsixold=39, uimpk=40, uimpkk=41, denalf=42, falfs=43, intxalf=44, intyalf=45, intzalf=46,
+    ualphas=47, kalfs=48)
 
 
 class HeGrid(ctypes.Structure):

@@ -103,7 +103,7 @@ class Context:
 
     def _shape(self, name):
         w = self.w
-        if name in ("fden", "fvlj4", "wcgk"):
+        if name in ("fden", "fvlj4", "wcgk", "kalfs"):
             return (w.nx // 2 + 1, w.ny, w.nz)
         if name in ("rimp", "vimp", "aimp", "F", "pcr", "pcv", "qr", "qv"):
             return (w.n_imp, 3)
@@ -146,10 +146,11 @@ class Context:
         return buf.reshape(shape, order="F")
 
     # ---- set-up ---------------------------------------------------------------------------------
-    def set_kernels(self, fvlj4, wcgk):
+    def set_kernels(self, fvlj4, wcgk, kalfs=None):
         a = np.ascontiguousarray(np.asarray(fvlj4, np.float64).ravel(order="F"))
         b = np.ascontiguousarray(np.asarray(wcgk, np.float64).ravel(order="F"))
-        self._ck(self.L.he_set_kernels(self.h, dptr(a), dptr(b), None))
+        k = None if kalfs is None else np.ascontiguousarray(np.asarray(kalfs, np.float64).ravel(order="F"))
+        self._ck(self.L.he_set_kernels(self.h, dptr(a), dptr(b), None if k is None else dptr(k)))
 
     def set_impurities(self, w: Workload):
         potion, npot, delinter, rmax = potion_table(w)

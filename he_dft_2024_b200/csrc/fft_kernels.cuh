@@ -12,7 +12,7 @@
 //     X_C2R2       dencg = C2R(A)*renor, delj4 = C2R(B)*renor                      (:142,:154)
 //     X_C2R2_CORR  the same, then the R2C of the correlation source into A         (:166-171)
 //     X_C2R_POT    sto1 = C2R(A)*renor, penalty, pot4 assembly (+ potx4 of the quantum
-//                  impurities when extra is set)                                   (:178-218)
+//                  impurities when extra is set, + ualphas when extra2 is set)     (:178-218)
 //     X_C2R1       out1 = C2R(A)*renor (rows 2p, 2p+1 packed in one line)
 // y/z pass (k_ypass, k_zconv): CTA = TKX consecutive kx of one pencil family, staged transposed
 //   in shared memory (odd line stride to spread banks).  The z pass does forward z, the k-space
@@ -49,6 +49,7 @@ struct XArgs {
   double* out1;              // dencg  (C2R2*) or pot4 (C2R_POT)
   double* out2;              // delj4  (C2R2*)
   const double* extra;       // C2R_POT: potx4 added after the correlation term (null: none)
+  const double* extra2;      // C2R_POT: ualphas (alpha_s term) added next (null: none)
   double renor, cp4, cpp4, a0, a1;
   int lsolid;
   double C, beta, den_m;
@@ -164,6 +165,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
       const double dc = a.dencg_in[g];
       double pot = a.delj4_in[g] + dc * dc * (a.a0 + a.a1 * dc) + sto1;
       if (a.extra) pot = pot + a.extra[g];
+      if (a.extra2) pot = pot + a.extra2[g];
       if (a.lsolid) {
         const double d = a.den[g];
         const double t = tanh(a.beta * (d - a.den_m));

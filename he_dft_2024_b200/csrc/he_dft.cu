@@ -20,6 +20,7 @@
 #include "ops.cuh"
 #include "setup.cuh"
 #include "quantum.cuh"
+#include "alphas.cuh"
 
 using namespace he;
 
@@ -45,6 +46,7 @@ enum Slot {
   S_QHEX = 56,      // quantum: sum sto2*den (eHeX)
   S_QII = 57,       // quantum: impurity-pair sums (eimpu_impu), 6 slots
   S_QMOM = 64,      // quantum: moments, 4 per impurity
+  S_ALF = 80,       // alpha_s energy sum
   S_COUNT = 96
 };
 
@@ -93,6 +95,10 @@ struct he_ctx {
   size_t pot_tab_cap = 0;
   double delinter = 0.0, rmaxinterpol = 0.0;
   bool force_fresh = false;
+  // alpha_s term (core4 = 'OTC'): alphasterm module arrays and work arrays
+  double *denalf = nullptr, *falfs = nullptr, *intxalf = nullptr, *intyalf = nullptr,
+         *intzalf = nullptr, *ualphas = nullptr, *ua_raw = nullptr;
+  double *as1 = nullptr, *as2 = nullptr, *as3 = nullptr, *as4 = nullptr, *as5 = nullptr;
   // quantum impurities (HE_MODE_QUANTUM); psixold[i][s-1] is Fortran slot s of impurity i
   int nq = 0;
   double mu4 = 0.0, h2o2mx[kMaxQImp] = {};
@@ -492,7 +498,8 @@ static int spectrum_cg_lj(he_ctx_t* ctx) {
 }
 // Correlation convolution of the spectrum in wA (already x-transformed) and pot4 assembly
 // (extra: potx4 of the quantum impurities, or null).
-static int correlation_tail(he_ctx_t* ctx, const double* extra = nullptr) {
+static int correlation_tail(he_ctx_t* ctx, const double* extra = nullptr,
+                            const double* extra2 = nullptr) {
   TRY(ypass(ctx, ctx->wA, nullptr, false));
   TRY(zconv(ctx, ctx->wA, ctx->wcgk, nullptr, nullptr, nullptr));
   TRY(ypass(ctx, ctx->wA, nullptr, true));
@@ -501,6 +508,7 @@ static int correlation_tail(he_ctx_t* ctx, const double* extra = nullptr) {
   a.den = ctx->den; a.dencg_in = ctx->dencg; a.delj4_in = ctx->delj4;
   a.out1 = ctx->pot4;
   a.extra = extra;
+  a.extra2 = extra2;
   return xpass<X_C2R_POT>(ctx, a);
 }
 
@@ -558,6 +566,18 @@ static int field_ref(he_ctx_t* ctx, int field, FieldRef* r) {
     case HE_F_HPSI:
       if (!ctx->hpsi) break;
       *r = {ctx->hpsi, 8 * N, false};
+      return HE_OK;
+    case HE_F_DENALF: case HE_F_FALFS: case HE_F_INTXALF: case HE_F_INTYALF: case HE_F_INTZALF:
+    case HE_F_UALPHAS: {
+      if (!ctx->otc) break;
+      double* const arr[6] = {ctx->denalf, ctx->falfs, ctx->intxalf, ctx->intyalf, ctx->intzalf,
+                              ctx->ualphas};
+      *r = {arr[field - HE_F_DENALF], 8 * N, false};
+      return HE_OK;
+    }
+    case HE_F_KALFS:
+      if (!ctx->otc) break;
+      *r = {ctx->kalfs, 8 * Nk, true};
       return HE_OK;
     case HE_F_FVLJ4: *r = {ctx->fvlj4, 8 * Nk, true}; return HE_OK;
     case HE_F_WCGK: *r = {ctx->wcgk, 8 * Nk, true}; return HE_OK;
@@ -831,6 +851,110 @@ static int autotune_tiles(he_ctx_t* ctx) {
 // C-ABI
 // ------------------------------------------------------------------------------------------------
 // ------------------------------------------------------------------------------------------------
+// alpha_s term (core4 = 'OTC'): term_alfa.f90:5-117
+// ------------------------------------------------------------------------------------------------
+template <int N, int TILE>
+static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a);
+static int zmix(he_ctx_t* ctx, ZMixArgs a);
+
+// out[k] = C2R(R2C(in[k]) * ker) for n <= 3 real fields, through wB, wC, wD.
+static int conv_fields(he_ctx_t* ctx, const double* const* in, double* const* out, int n,
+                       const double* ker) {
+  double2* buf[3] = {ctx->wB, ctx->wC, ctx->wD};
+  XArgs a = xargs(ctx);
+  for (int k = 0; k < n; ++k) {
+    a.den = in[k];
+    a.specA = buf[k];
+    TRY(xpass<X_R2C_DEN>(ctx, a));
+  }
+  TRY(ypass(ctx, buf[0], n > 1 ? buf[1] : nullptr, false));
+  if (n > 2) TRY(ypass(ctx, buf[2], nullptr, false));
+  for (int k = 0; k < n; ++k) TRY(zconv(ctx, buf[k], ker, nullptr, nullptr, nullptr));
+  TRY(ypass(ctx, buf[0], n > 1 ? buf[1] : nullptr, true));
+  if (n > 2) TRY(ypass(ctx, buf[2], nullptr, true));
+  XArgs c = xargs(ctx);
+  int k = 0;
+  if (n >= 2) {
+    c.specA = buf[0]; c.specB = buf[1];
+    c.out1 = out[0]; c.out2 = out[1];
+    TRY(xpass<X_C2R2>(ctx, c));
+    k = 2;
+  }
+  if (k < n) {
+    XArgs d = xargs(ctx);
+    d.specA = buf[k];
+    d.out1 = out[k];
+    TRY(xpass<X_C2R1>(ctx, d));
+  }
+  return HE_OK;
+}
+
+// denalf = C2R(fden * kalfs) (Dynamics_TDDFT/poten.f90:200-205; BCN4HeDFT.f90:1142-1148).
+static int alfa_density(he_ctx_t* ctx) {
+  ZMixArgs z{};
+  z.nout = 1;
+  z.out[0] = ctx->wC; z.nterm[0] = 1; z.src[0][0] = ctx->fden; z.ker[0][0] = ctx->kalfs;
+  TRY(zmix(ctx, z));
+  TRY(ypass(ctx, ctx->wC, nullptr, true));
+  XArgs a = xargs(ctx);
+  a.specA = ctx->wC;
+  a.out1 = ctx->denalf;
+  return xpass<X_C2R1>(ctx, a);
+}
+
+// term_alfa (needs denalf and materialised dxden/dyden/dzden); leaves ualphas, falfs, int*alf.
+static int term_alfa(he_ctx_t* ctx) {
+  const long N = ctx->N;
+  const int nb = pw_blocks(ctx);
+  tname(ctx, "alphas_pointwise");
+  k_alf_src<<<nb, 256, 0, ctx->stream>>>(ctx->denalf, ctx->dxden, ctx->dyden, ctx->dzden,
+                                         ctx->fn.den0s, N, ctx->falfs, ctx->as1, ctx->as2, ctx->as3);
+  LAUNCHED();
+  {
+    const double* in[3] = {ctx->as1, ctx->as2, ctx->as3};
+    double* out[3] = {ctx->intxalf, ctx->intyalf, ctx->intzalf};
+    TRY(conv_fields(ctx, in, out, 3, ctx->kalfs));
+  }
+  tname(ctx, "alphas_pointwise");
+  k_alf_dot<<<nb, 256, 0, ctx->stream>>>(ctx->dxden, ctx->dyden, ctx->dzden, ctx->intxalf,
+                                         ctx->intyalf, ctx->intzalf, N, ctx->as1);
+  LAUNCHED();
+  {
+    const double* in[1] = {ctx->as1};
+    double* out[1] = {ctx->ua_raw};
+    TRY(conv_fields(ctx, in, out, 1, ctx->kalfs));
+  }
+  tname(ctx, "alphas_pointwise");
+  k_alf_fi<<<nb, 256, 0, ctx->stream>>>(ctx->falfs, ctx->intxalf, ctx->intyalf, ctx->intzalf, N,
+                                        ctx->as1, ctx->as2, ctx->as3);
+  LAUNCHED();
+  OpAxisDeriv<0> dx{};
+  dx.out = ctx->as4;
+  TRY(run_stencil(ctx, ctx->g1, ctx->as1, dx));
+  OpAxisDeriv<1> dy{};
+  dy.out = ctx->as5;
+  TRY(run_stencil(ctx, ctx->g1, ctx->as2, dy));
+  OpAlfFinal fin{};
+  fin.s8[0] = ctx->ua_raw; fin.s8[1] = ctx->as4; fin.s8[2] = ctx->as5;
+  fin.out = ctx->ualphas;
+  fin.den0s = ctx->fn.den0s; fin.h2o2m4 = ctx->fn.h2o2m4; fin.alphas = ctx->fn.alphas;
+  return run_stencil(ctx, ctx->g1, ctx->as3, fin);
+}
+
+// The ealphas sum, queued into slot S_ALF (read with the other energy sums).
+static int alfa_energy_sum(he_ctx_t* ctx) {
+  tname(ctx, "alphas_energy");
+  k_alf_energy<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(ctx->falfs, ctx->dxden, ctx->dyden, ctx->dzden,
+                                                        ctx->intxalf, ctx->intyalf, ctx->intzalf,
+                                                        ctx->N, tail(ctx, S_ALF));
+  LAUNCHED();
+  return HE_OK;
+}
+static double alfa_energy(const he_ctx_t* ctx) {
+  return -ctx->fn.h2o2m4 * 0.5 * ctx->fn.alphas * ctx->hsum[S_ALF] * ctx->dxyz;
+}
+
+// ------------------------------------------------------------------------------------------------
 // quantum impurities (HE_MODE_QUANTUM, Dynamics_quantum_impurities)
 // ------------------------------------------------------------------------------------------------
 template <int N, int TILE>
@@ -979,7 +1103,12 @@ static int q_poten(he_ctx_t* ctx) {
   a.den = ctx->den;
   a.out1 = ctx->dencg; a.out2 = ctx->delj4;
   TRY(xpass<X_C2R2_CORR>(ctx, a));
-  return correlation_tail(ctx, ctx->potx4);
+  if (ctx->otc) {  // Dynamics_quantum_impurities/poten.f90:48 (derden), :126-139
+    TRY(he_derden(ctx));
+    TRY(alfa_density(ctx));
+    TRY(term_alfa(ctx));
+  }
+  return correlation_tail(ctx, ctx->potx4, ctx->otc ? ctx->ualphas : nullptr);
 }
 
 static int q_field(he_ctx_t* ctx) {
@@ -1151,6 +1280,7 @@ static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
       TRY(q_synth(ctx, &p, 1, nullptr));
       TRY(q_dot(ctx, ctx->t4, ctx->denx[m], S_QII + pair));
     }
+  if (ctx->otc) TRY(alfa_energy_sum(ctx));
   TRY(read_sums(ctx));
   const double* s = ctx->hsum + S_EN;
   const double dxyz = ctx->dxyz;
@@ -1160,6 +1290,10 @@ static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
   e.elj4 = 0.5 * s[1] * dxyz;
   e.ecor4 = s[2] * dxyz;
   e.etot4 = e.ekin4 + e.elj4 + e.ecor4 + e.esolid;
+  if (ctx->otc) {
+    e.ealphas = alfa_energy(ctx);
+    e.etot4 = e.etot4 + e.ealphas;
+  }
   for (int k = 0; k < n; ++k) e.ekinx = e.ekinx + ctx->h2o2mx[k] * ctx->hsum[S_QEK + k];
   e.ekinx = e.ekinx * dxyz;
   e.eHeX = ctx->hsum[S_QHEX] * dxyz;
@@ -1426,9 +1560,11 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   else if (grid->xmax == 0.0 || grid->ymax == 0.0 || grid->zmax == 0.0)
     bad(HE_ERR_ARG, "xmax, ymax, zmax must be non-zero");
   if (st == HE_OK) {
-    if (std::strncmp(fun->core4, "OTC", 3) == 0) bad(HE_ERR_ARG, "core4='OTC' (alpha_s term) is not built yet");
-    else if (std::strncmp(fun->core4, "OP", 2) != 0 && std::strncmp(fun->core4, "OT", 2) != 0)
+    if (std::strncmp(fun->core4, "OP", 2) != 0 && std::strncmp(fun->core4, "OT ", 3) != 0 &&
+        std::strncmp(fun->core4, "OTC", 3) != 0)
       bad(HE_ERR_ARG, "core4 must be 'OT ', 'OP ' or 'OTC'");
+    else if (std::strncmp(fun->core4, "OTC", 3) == 0 && !(fun->den0s != 0.0))
+      bad(HE_ERR_ARG, "core4='OTC' needs den0s != 0");
   }
   if (st != HE_OK) {
     *out = ctx;
@@ -1449,6 +1585,7 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   ctx->icon = grid->icon;
   ctx->fn = *fun;
   ctx->op_core = std::strncmp(fun->core4, "OP", 2) == 0;
+  ctx->otc = std::strncmp(fun->core4, "OTC", 3) == 0;
   bickley13(ctx->w1, ctx->w2);
   make_geom(ctx, 1, &ctx->g1);
   make_geom(ctx, 2, &ctx->g2);
@@ -1502,9 +1639,18 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (mode == HE_MODE_QUANTUM) {
     TRY(dalloc_t(ctx, &ctx->potx4, N));
     TRY(dalloc_t(ctx, &ctx->t4, N));
+    TRY(dalloc(ctx, &ctx->xscratch, wf));
+  }
+  if (mode == HE_MODE_QUANTUM || ctx->otc) {
     TRY(dalloc_t(ctx, &ctx->wC, Nk));
     TRY(dalloc_t(ctx, &ctx->wD, Nk));
-    TRY(dalloc(ctx, &ctx->xscratch, wf));
+  }
+  if (ctx->otc) {
+    TRY(dalloc_t(ctx, &ctx->kalfs, Nk));
+    for (double** a : {&ctx->denalf, &ctx->falfs, &ctx->intxalf, &ctx->intyalf, &ctx->intzalf,
+                       &ctx->ualphas, &ctx->ua_raw, &ctx->as1, &ctx->as2, &ctx->as3, &ctx->as4,
+                       &ctx->as5, &ctx->dxden, &ctx->dyden, &ctx->dzden})
+      TRY(dalloc_t(ctx, a, N));
   }
   if (mode != HE_MODE_STATICS) {
     TRY(dalloc_t(ctx, &ctx->tabx, ctx->nx));
@@ -1560,7 +1706,8 @@ int he_synchronize(he_ctx_t* ctx) {
 
 int he_set_kernels(he_ctx_t* ctx, const double* fvlj4, const double* wcgk, const double* kalfs) {
   if (!ctx || !fvlj4 || !wcgk) return fail(ctx, HE_ERR_ARG, "null kernel array");
-  (void)kalfs;
+  if (ctx->otc && !kalfs) return fail(ctx, HE_ERR_ARG, "core4='OTC' needs kalfs");
+  if (ctx->otc) CK(cudaMemcpyAsync(ctx->kalfs, kalfs, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->fvlj4, fvlj4, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->wcgk, wcgk, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1573,7 +1720,7 @@ int he_compute_kernels(he_ctx_t* ctx) {
   KernArgs a{};
   a.nx = ctx->nx; a.ny = ctx->ny; a.nz = ctx->nz; a.nxh = ctx->nxh;
   a.hx = ctx->hx; a.hy = ctx->hy; a.hz = ctx->hz;
-  a.op_core = ctx->op_core; a.otc = 0;
+  a.op_core = ctx->op_core; a.otc = ctx->otc;
   a.eps = ctx->fn.eps4; a.sigma = ctx->fn.sigma4; a.hc = ctx->fn.h4; a.l = ctx->fn.l;
   a.fvlj4 = ctx->fvlj4; a.wcgk = ctx->wcgk; a.kalfs = ctx->kalfs;
   tname(ctx, "kspace_kernels");
@@ -1717,7 +1864,8 @@ int he_poten(he_ctx_t* ctx) {
     a.den = ctx->den; a.dencg_in = ctx->dencg;
     a.specA = ctx->wA;
     TRY(xpass<X_R2C_CORR>(ctx, a));
-    return correlation_tail(ctx);
+    if (ctx->otc) TRY(term_alfa(ctx));  // He_statics/poten.f90:86-91 (denalf from the refresh)
+    return correlation_tail(ctx, nullptr, ctx->otc ? ctx->ualphas : nullptr);
   }
   TRY(spectrum_cg_lj(ctx));
   XArgs a = xargs(ctx);
@@ -1725,7 +1873,12 @@ int he_poten(he_ctx_t* ctx) {
   a.den = ctx->den;
   a.out1 = ctx->dencg; a.out2 = ctx->delj4;
   TRY(xpass<X_C2R2_CORR>(ctx, a));
-  return correlation_tail(ctx);
+  if (ctx->otc) {  // Dynamics_TDDFT/poten.f90:144 (derden), :200-210 (denalf, term_alfa)
+    TRY(he_derden(ctx));
+    TRY(alfa_density(ctx));
+    TRY(term_alfa(ctx));
+  }
+  return correlation_tail(ctx, nullptr, ctx->otc ? ctx->ualphas : nullptr);
 }
 
 
@@ -1924,6 +2077,7 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
     op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
     TRY(run_stencil_red(ctx, ctx->g1, (const double*)ctx->psi, op, S_EN));
   }
+  if (ctx->otc) TRY(alfa_energy_sum(ctx));
   CK(cudaMemcpyAsync(ctx->hsum, ctx->sums, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   const double* s = ctx->hsum + S_EN;
@@ -1935,6 +2089,10 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
   e.ecor4 = s[2] * dxyz;
   e.etot4 = e.ekin4 + e.elj4 + e.ecor4 + e.esolid;
   e.ealphas = 0.0;
+  if (ctx->otc) {
+    e.ealphas = alfa_energy(ctx);
+    e.etot4 = e.etot4 + e.ealphas;
+  }
   if (ctx->mode == HE_MODE_DYNAMICS) {
     ImpDev h;
     TRY(imp_pull(ctx, &h));
@@ -1993,7 +2151,9 @@ int he_refresh_density(he_ctx_t* ctx) {
   XArgs a = xargs(ctx);
   a.specA = ctx->wA; a.specB = ctx->wB;
   a.out1 = ctx->dencg; a.out2 = ctx->delj4;
-  return xpass<X_C2R2>(ctx, a);
+  TRY(xpass<X_C2R2>(ctx, a));
+  if (ctx->otc) TRY(alfa_density(ctx));  // BCN4HeDFT.f90:1142-1148
+  return HE_OK;
 }
 
 

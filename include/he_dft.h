@@ -134,7 +134,15 @@ enum he_field {
   HE_F_PSIXOLD = 38,  /* psixold(nx,ny,nz,3,N_imp) complex */
   HE_F_HPSIXOLD = 39, /* hpsixold(nx,ny,nz,2,N_imp) complex */
   HE_F_UIMPK = 40,    /* uimp_k(nx/2+1,ny,nz,N_imp) real */
-  HE_F_UIMPKK = 41    /* uimp_k_k(nx/2+1,ny,nz,N_imp,N_imp) real (zero for 'null' pairs) */
+  HE_F_UIMPKK = 41,   /* uimp_k_k(nx/2+1,ny,nz,N_imp,N_imp) real (zero for 'null' pairs) */
+  /* core4 = 'OTC' (alphasterm module, Dynamics_TDDFT/modules.f90; term_alfa.f90) */
+  HE_F_DENALF = 42,   /* real N */
+  HE_F_FALFS = 43,    /* real N */
+  HE_F_INTXALF = 44,  /* real N */
+  HE_F_INTYALF = 45,
+  HE_F_INTZALF = 46,
+  HE_F_UALPHAS = 47,  /* real N */
+  HE_F_KALFS = 48     /* real Nk */
 };
 
 #define HE_MAX_QIMP 4

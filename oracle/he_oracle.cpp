@@ -447,6 +447,8 @@ struct Common {
   std::vector<double> fvlj4, wcgk, kalfs;
   std::vector<double> den, dencg, delj4, pot4, sto1, penalty, dxden, dyden, dzden;
   std::vector<cplx> fden, wk1;
+  // alpha_s term (core4 = 'OTC'; alphasterm module)
+  std::vector<double> denalf, falfs, intxalf, intyalf, intzalf, ualphas, a1, a2, a3, a4, a5, a6;
 
   void init_common(const ho_params& pp) {
     p = pp;
@@ -469,6 +471,62 @@ struct Common {
     sto1.assign(N, 0); penalty.assign(N, 0);
     dxden.assign(N, 0); dyden.assign(N, 0); dzden.assign(N, 0);
     fden.assign(g.nk, 0); wk1.assign(g.nk, 0);
+    if (p.core == 2)
+      for (auto* v : {&denalf, &falfs, &intxalf, &intyalf, &intzalf, &ualphas, &a1, &a2, &a3, &a4,
+                      &a5, &a6})
+        v->assign(N, 0);
+  }
+  bool otc() const { return p.core == 2; }
+  // g = C2R(R2C(f) * kalfs) * renor
+  void conv_kalfs(const std::vector<double>& f, std::vector<double>& out) {
+    fft.r2c(f.data(), wk1.data());
+    for (long i = 0; i < g.nk; ++i) wk1[i] = kalfs[i] * wk1[i];
+    fft.c2r(wk1.data(), out.data(), renor);
+  }
+  // denalf = C2R(fden*kalfs) (Dynamics_TDDFT/poten.f90:200-205; BCN4HeDFT.f90:1142-1148).
+  void alfa_density() {
+    for (long i = 0; i < g.nk; ++i) wk1[i] = fden[i] * kalfs[i];
+    fft.c2r(wk1.data(), denalf.data(), renor);
+  }
+  // term_alfa: Dynamics_TDDFT/term_alfa.f90:5-117 (He_statics/term_alfa.f90 is the same
+  // arithmetic).  Needs denalf and dxden/dyden/dzden.
+  void term_alfa() {
+    const long N = g.nxyz;
+    const double d0 = p.den0s;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < N; ++i) {
+      falfs[i] = 1.0 - denalf[i] / d0;
+      a1[i] = falfs[i] * dxden[i];
+      a2[i] = falfs[i] * dyden[i];
+      a3[i] = falfs[i] * dzden[i];
+    }
+    conv_kalfs(a1, intxalf);
+    conv_kalfs(a2, intyalf);
+    conv_kalfs(a3, intzalf);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < N; ++i) a1[i] = dxden[i] * intxalf[i] + dyden[i] * intyalf[i] + dzden[i] * intzalf[i];
+    conv_kalfs(a1, ualphas);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < N; ++i) {
+      ualphas[i] = ualphas[i] / d0;
+      a1[i] = falfs[i] * intxalf[i];
+      a2[i] = falfs[i] * intyalf[i];
+      a3[i] = falfs[i] * intzalf[i];
+    }
+    deriv3d<double>(1, g, 0, p.icon, w1, w2, a1.data(), a4.data());
+    deriv3d<double>(1, g, 1, p.icon, w1, w2, a2.data(), a5.data());
+    deriv3d<double>(1, g, 2, p.icon, w1, w2, a3.data(), a6.data());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < N; ++i) ualphas[i] = (ualphas[i] + a4[i] + a5[i] + a6[i]) * p.h2o2m4 * p.alphas;
+  }
+  // ealphas of energy() (Dynamics_TDDFT/energy.f90:131-135, He_statics/energy.f90:110-114).
+  double ealphas() const {
+    if (!otc()) return 0.0;
+    double s = 0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (long i = 0; i < g.nxyz; ++i)
+      s += falfs[i] * (dxden[i] * intxalf[i] + dyden[i] * intyalf[i] + dzden[i] * intzalf[i]);
+    return -p.h2o2m4 * 0.5 * p.alphas * s * g.dxyz;
   }
   // derden: Dynamics_TDDFT/derden.f90:26-28.
   void derden() {
@@ -491,7 +549,9 @@ struct Common {
   // Correlation convolution, penalty and pot4 assembly (poten.f90:160-198, :214-218).
   // extra (optional): potx4 of the quantum-impurity path, added after the correlation term
   // (Dynamics_quantum_impurities/poten.f90:116-121).
-  void correlation_and_assembly(const double* extra = nullptr) {
+  // extra2 (optional): ualphas of the alpha_s term, added before the solid penalty
+  // (poten.f90:200-210).
+  void correlation_and_assembly(const double* extra = nullptr, const double* extra2 = nullptr) {
     const long N = g.nxyz;
     const double cp4 = p.cp4, cpp4 = p.cpp4;
     const double a0 = cp4 / 2.0, a1 = cpp4 / 3.0;
@@ -512,6 +572,7 @@ struct Common {
       double dc = dencg[i];
       pot4[i] = delj4[i] + dc * dc * (a0 + a1 * dc) + sto1[i];
       if (extra) pot4[i] = pot4[i] + extra[i];
+      if (extra2) pot4[i] = pot4[i] + extra2[i];
     }
     if (p.lsolid) {
 #pragma omp parallel for schedule(static)
@@ -641,7 +702,11 @@ struct Dyn : Common {
     coarse_grain();
     derden();
     lennard_jones();
-    correlation_and_assembly();
+    if (otc()) {
+      alfa_density();
+      term_alfa();
+    }
+    correlation_and_assembly(nullptr, otc() ? ualphas.data() : nullptr);
   }
   // forceimp: potenimp.f90:23-67.
   void forceimp() {
@@ -863,7 +928,9 @@ struct Dyn : Common {
     for (long i = 0; i < g.nxyz; ++i) ek += std::norm(s1[i]) + std::norm(s2[i]) + std::norm(s3[i]);
     double ekin4, elj4, ecor4, esolid;
     he_energy_sums(ek, &ekin4, &elj4, &ecor4, &esolid);
+    const double ea = ealphas();
     double etot4 = ekin4 + elj4 + ecor4 + esolid;
+    if (otc()) etot4 = etot4 + ea;
     double ekinx = 0;
     for (int k = 0; k < ni; ++k) {
       double v2 = 0;
@@ -885,7 +952,7 @@ struct Dyn : Common {
         eii += select_pot(p.ii_kind, p.ii_D, p.ii_re, p.ii_a, p.ii_rcut, p.ii_umax, std::sqrt(s));
       }
     double eimpu = ekinx + eHeX + eii;
-    double v[11] = {etot4, ekin4, elj4, ecor4, esolid, 0.0, ekinx, eHeX, eii, eimpu, etot4 + eimpu};
+    double v[11] = {etot4, ekin4, elj4, ecor4, esolid, ea, ekinx, eHeX, eii, eimpu, etot4 + eimpu};
     std::memcpy(out, v, sizeof(v));
   }
 };
@@ -1212,8 +1279,13 @@ struct QDyn : Common {
   // poten: Dynamics_quantum_impurities/poten.f90:5-155 (fden comes from potenimp).
   void poten() {
     coarse_grain();
+    if (otc()) derden();
     lennard_jones();
-    correlation_and_assembly(potx4.data());
+    if (otc()) {
+      alfa_density();
+      term_alfa();
+    }
+    correlation_and_assembly(potx4.data(), otc() ? ualphas.data() : nullptr);
   }
   // s4 = timec*((d2x+d2y+d2z)*h2o2m - (pot - shift)*f)  (steprk.f90:68,94; steppc.f90:46,77).
   void hpsi_q(const std::vector<cplx>& f, const std::vector<double>& pot, double shift, double h2) {
@@ -1349,7 +1421,8 @@ struct QDyn : Common {
     const double ek = grad2(psi);
     double ekin4, elj4, ecor4, esolid;
     he_energy_sums(ek, &ekin4, &elj4, &ecor4, &esolid);
-    const double etot4 = ekin4 + elj4 + ecor4 + esolid;
+    const double ea = ealphas();
+    const double etot4 = ekin4 + elj4 + ecor4 + esolid + (otc() ? ea : 0.0);
     double ekinx = 0.0;
     std::fill(wk2.begin(), wk2.end(), cplx(0.0));
     for (int k = 0; k < ni; ++k) {
@@ -1379,7 +1452,7 @@ struct QDyn : Common {
     }
     eii = eii * g.dxyz;
     const double eimpu = ekinx + eHeX + eii;
-    const double v[11] = {etot4, ekin4, elj4, ecor4, esolid, 0.0, ekinx, eHeX, eii, eimpu, etot4 + eimpu};
+    const double v[11] = {etot4, ekin4, elj4, ecor4, esolid, ea, ekinx, eHeX, eii, eimpu, etot4 + eimpu};
     std::memcpy(out, v, sizeof(v));
   }
 
@@ -1427,13 +1500,15 @@ struct Stat : Common {
   // driver refreshes them once per iteration (BCN4HeDFT.f90:1131-1155).
   void poten() {
     lennard_jones();
-    correlation_and_assembly();
+    if (otc()) term_alfa();
+    correlation_and_assembly(nullptr, otc() ? ualphas.data() : nullptr);
   }
   // The driver's per-iteration refresh: derden, fftfw(den,fden), dencg (BCN4HeDFT.f90:1131-1155).
   void refresh() {
     derden();
     fftfw_den();
     coarse_grain();
+    if (otc()) alfa_density();
   }
   void lap(const std::vector<double>& f) {
     deriv3d<double>(2, g, 0, p.icon, w1, w2, f.data(), t1.data());
@@ -1585,8 +1660,10 @@ struct Stat : Common {
     for (long i = 0; i < g.nxyz; ++i) ek += t1[i] * t1[i] + t2[i] * t2[i] + t3[i] * t3[i];
     double ekin4, elj4, ecor4, esolid;
     he_energy_sums(ek, &ekin4, &elj4, &ecor4, &esolid);
+    const double ea = ealphas();
     double etot4 = ekin4 + elj4 + ecor4 + esolid;
-    double v[11] = {etot4, ekin4, elj4, ecor4, esolid, 0.0, 0.0, 0.0, 0.0, 0.0, etot4};
+    if (otc()) etot4 = etot4 + ea;
+    double v[11] = {etot4, ekin4, elj4, ecor4, esolid, ea, 0.0, 0.0, 0.0, 0.0, etot4};
     std::memcpy(out, v, sizeof(v));
   }
   // varmu: He_statics/varmu.f90:31 (hpsi holds H psi of the last predictor).
@@ -1605,6 +1682,16 @@ static double* dyn_field(Dyn* d, const char* name, long* n) {
   long N = d->g.nxyz, K = d->g.nk;
   auto R = [&](std::vector<double>& v, long nn) { *n = nn; return v.data(); };
   auto C = [&](std::vector<cplx>& v, long nn) { *n = 2 * nn; return (double*)v.data(); };
+  if (d->otc()) {
+    if (s == "denalf") { *n = d->g.nxyz; return d->denalf.data(); }
+    if (s == "falfs") { *n = d->g.nxyz; return d->falfs.data(); }
+    if (s == "intxalf") { *n = d->g.nxyz; return d->intxalf.data(); }
+    if (s == "intyalf") { *n = d->g.nxyz; return d->intyalf.data(); }
+    if (s == "intzalf") { *n = d->g.nxyz; return d->intzalf.data(); }
+    if (s == "ualphas") { *n = d->g.nxyz; return d->ualphas.data(); }
+    if (s == "kalfs") { *n = d->g.nk; return d->kalfs.data(); }
+  }
+  if (s == "dxden") { *n = d->g.nxyz; return d->dxden.data(); }
   if (s == "den") return R(d->den, N);
   if (s == "dencg") return R(d->dencg, N);
   if (s == "delj4") return R(d->delj4, N);
@@ -1642,6 +1729,16 @@ static double* stat_field(Stat* d, const char* name, long* n) {
   std::string s(name);
   long N = d->g.nxyz, K = d->g.nk;
   auto R = [&](std::vector<double>& v, long nn) { *n = nn; return v.data(); };
+  if (d->otc()) {
+    if (s == "denalf") { *n = d->g.nxyz; return d->denalf.data(); }
+    if (s == "falfs") { *n = d->g.nxyz; return d->falfs.data(); }
+    if (s == "intxalf") { *n = d->g.nxyz; return d->intxalf.data(); }
+    if (s == "intyalf") { *n = d->g.nxyz; return d->intyalf.data(); }
+    if (s == "intzalf") { *n = d->g.nxyz; return d->intzalf.data(); }
+    if (s == "ualphas") { *n = d->g.nxyz; return d->ualphas.data(); }
+    if (s == "kalfs") { *n = d->g.nk; return d->kalfs.data(); }
+  }
+  if (s == "dxden") { *n = d->g.nxyz; return d->dxden.data(); }
   if (s == "den") return R(d->den, N);
   if (s == "psi") return R(d->psi, N);
   if (s == "dencg") return R(d->dencg, N);
@@ -1666,6 +1763,16 @@ static double* qdyn_field(QDyn* d, const char* name, long* n) {
   auto R = [&](std::vector<double>& v, long nn) { *n = nn; return v.data(); };
   auto C = [&](std::vector<cplx>& v, long nn) { *n = 2 * nn; return (double*)v.data(); };
   const bool ok = idx >= 0 && idx < d->ni;
+  if (d->otc()) {
+    if (s == "denalf") { *n = d->g.nxyz; return d->denalf.data(); }
+    if (s == "falfs") { *n = d->g.nxyz; return d->falfs.data(); }
+    if (s == "intxalf") { *n = d->g.nxyz; return d->intxalf.data(); }
+    if (s == "intyalf") { *n = d->g.nxyz; return d->intyalf.data(); }
+    if (s == "intzalf") { *n = d->g.nxyz; return d->intzalf.data(); }
+    if (s == "ualphas") { *n = d->g.nxyz; return d->ualphas.data(); }
+    if (s == "kalfs") { *n = d->g.nk; return d->kalfs.data(); }
+  }
+  if (s == "dxden") { *n = d->g.nxyz; return d->dxden.data(); }
   if (s == "den") return R(d->den, N);
   if (s == "dencg") return R(d->dencg, N);
   if (s == "delj4") return R(d->delj4, N);

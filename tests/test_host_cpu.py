@@ -21,11 +21,11 @@ def test_library_exports_every_header_symbol():
     assert not missing, missing
 
 
-def _create(nx=32, ny=32, nz=32, npd=13, icon=13, core=b"OT ", mode=0):
+def _create(nx=32, ny=32, nz=32, npd=13, icon=13, core=b"OT ", mode=0, den0s=0.04):
     L = _lib.load()
     g = _lib.HeGrid(nx, ny, nz, 10.0, 10.0, 10.0, npd, icon)
     f = _lib.HeFunctional(core, 2.190323, 10.22, 2.556, -2.41186e4, 1.8585e6, 0.062, 54.31, 1.0,
-                          0.04, 6.05969638298, 1, 3.1577504e4, 40.0, 0.37)
+                          den0s, 6.05969638298, 1, 3.1577504e4, 40.0, 0.37)
     h = ctypes.c_void_p()
     st = L.he_ctx_create(ctypes.byref(g), ctypes.byref(f), mode, 0, ctypes.byref(h))
     msg = L.he_last_error(h.value).decode() if h.value else ""
@@ -46,7 +46,8 @@ def test_tstgrid_sizes_enforced():
     (dict(npd=11), "npd"),
     (dict(icon=24), "icon"),
     (dict(core=b"XX "), "core4"),
-    (dict(core=b"OTC"), "OTC"),
+    (dict(core=b"OTC", den0s=0.0), "den0s"),
+    (dict(core=b"OTE"), "core4"),
     (dict(mode=7), "mode"),
     (dict(nx=45), "nx must be even"),
 ])
