@@ -1549,8 +1549,9 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
     bad(HE_ERR_ARG, "unknown mode");
   else if (precision != HE_PREC_F64) bad(HE_ERR_ARG, "unknown precision");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
-  else if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18)
-    bad(HE_ERR_ARG, "icon must be 13, 8 or 18");
+  else if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18 &&
+           grid->icon != 24)
+    bad(HE_ERR_ARG, "icon must be 13, 8, 18 or 24");
   else if (!tstgrid_ok(grid->nx) || !tstgrid_ok(grid->ny) || !tstgrid_ok(grid->nz))
     bad(HE_ERR_ARG, "grid size is not an admissible tstgrid value");
   else if (grid->nx % 2 || grid->ny < 2 || (grid->ny * (long)grid->nz) % 2)

@@ -111,7 +111,8 @@ extern "C" int he_energy_noalloc(const he_grid_t* grid, const he_functional_t* f
   if (!grid || !fun || !out) return bad("null grid, functional or output");
   if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS) return bad("unknown mode");
   if (grid->npd != 13) return bad("npd must be 13");
-  if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18) return bad("icon must be 13, 8 or 18");
+  if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18 &&
+           grid->icon != 24) return bad("icon must be 13, 8, 18 or 24");
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return bad("grid sizes must be positive");
   if (grid->xmax == 0.0 || grid->ymax == 0.0 || grid->zmax == 0.0)
     return bad("xmax, ymax, zmax must be non-zero");

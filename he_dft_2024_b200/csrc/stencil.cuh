@@ -3,7 +3,8 @@
 // Restates Deriv3D_p / Deriv3D_pc (Dynamics_TDDFT/init_deriv_parallel.f90:373-648, :933-1209)
 // with the boundary rows of Redef (redef.f:133-170): for icon=13 every boundary row is the centred
 // row shifted with zero fill, i.e. a centred 13-point stencil over a zero-padded field; icon=8 and
-// icon=18 wrap periodically / antiperiodically (init_deriv_parallel.f90:1094-1206).  An axis
+// icon=18 wrap periodically / antiperiodically (init_deriv_parallel.f90:1094-1206); icon=24
+// reflects evenly about the end points (redef.f:245-279).  An axis
 // shorter than npd gives a zero derivative (init_deriv_parallel.f90:949-953).  The weights are
 // the Bickley rows times Sto = 1/h**id.
 //
@@ -25,10 +26,19 @@ namespace he {
 struct StencilGeom {
   int nx, ny, nz;
   int zc;            // z-chunk per CTA
-  int icon;          // 13, 8 or 18
+  int icon;          // 13, 8, 18 or 24
   int axis_on[3];    // 0 when n(axis) < npd
   double w[3][13];   // scaled weights per axis
 };
+
+// icon=24 (redef.f:245-279, then ICON=4 at :18-56): the boundary rows fold the centred row
+// onto the grid as an even reflection about the first and last points, f(1-m) = f(1+m) and
+// f(n+m) = f(n-m).
+HE_HD int mirror_index(int i, int n) {
+  if (i < 0) i = -i;
+  else if (i >= n) i = 2 * (n - 1) - i;
+  return min(max(i, 0), n - 1);
+}
 
 // Resolve (ix,iy,iz) under the boundary condition: returns false for a zero-padded point
 // (icon=13), otherwise the in-range index and whether the value is negated (icon=18).
@@ -36,6 +46,12 @@ HE_D bool resolve_bc(const StencilGeom& g, int& ix, int& iy, int& iz, bool& neg)
   neg = false;
   if (g.icon == 13)
     return !(ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny || iz < 0 || iz >= g.nz);
+  if (g.icon == 24) {
+    ix = mirror_index(ix, g.nx);
+    iy = mirror_index(iy, g.ny);
+    iz = mirror_index(iz, g.nz);
+    return true;
+  }
   const bool anti = (g.icon == 18);
   if (ix < 0) { ix += g.nx; neg ^= anti; } else if (ix >= g.nx) { ix -= g.nx; neg ^= anti; }
   if (iy < 0) { iy += g.ny; neg ^= anti; } else if (iy >= g.ny) { iy -= g.ny; neg ^= anti; }
@@ -182,6 +198,10 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<typename Op::T>())
     zneg = false;
     zz = iz;
     if (!wrap) return iz >= 0 && iz < g.nz;
+    if (g.icon == 24) {
+      zz = mirror_index(iz, g.nz);
+      return true;
+    }
     if (zz < 0) { zz += g.nz; zneg = anti; } else if (zz >= g.nz) { zz -= g.nz; zneg = anti; }
     zz = min(max(zz, 0), g.nz - 1);
     return true;

@@ -42,7 +42,8 @@ enum he_precision { HE_PREC_F64 = 0 };
 
 /* Grid: Dynamics_TDDFT/modules.f90:88-105 (grid), deriva npd/icon :31-37.  h = 2*xmax/n and
  * x_i = -xmax + h*(i-1) (DFT4He3d.f90:265-329).  npd must be 13; icon 13 (zero padding), 8
- * (periodic) or 18 (antiperiodic).  n must be a tstgrid size (tstgrid.f90:9-13). */
+ * (periodic), 18 (antiperiodic) or 24 (even reflection about the end points, redef.f:245-279).
+ * n must be a tstgrid size (tstgrid.f90:9-13). */
 typedef struct {
   int nx, ny, nz;
   double xmax, ymax, zmax;

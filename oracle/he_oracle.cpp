@@ -393,7 +393,8 @@ static double select_dpot(int kind, double D, double re, double a, double rcut, 
 // Finite differences: Deriv3D_p / Deriv3D_pc (init_deriv_parallel.f90:373-648, :933-1209) with
 // the Redef boundary rows.  icon=13 (redef.f:151-170 then :133-150) makes every boundary row the
 // centred row shifted with zero fill, i.e. a centred stencil with zero padding; icon=8/18 wrap
-// periodically / antiperiodically (init_deriv_parallel.f90:1094-1206).  Axes shorter than npd
+// periodically / antiperiodically (init_deriv_parallel.f90:1094-1206); icon=24 (redef.f:245-279,
+// then ICON=4 at :18-56) folds the centred row into an even reflection about the end points.  Axes shorter than npd
 // return zero (init_deriv_parallel.f90:949-953).  Weights are scaled by Sto = 1/h**id.
 // ------------------------------------------------------------------------------------------------
 template <typename T>
@@ -414,6 +415,7 @@ static void deriv3d(int id, const Grid& g, int axis, int icon, const double w1[1
   const int n = nn[axis];
   const double sgn = (icon == 18) ? -1.0 : 1.0;
   const bool wrap = (icon == 8 || icon == 18);
+  const bool mirror = (icon == 24);  // redef.f:245-279 + ICON=4: even reflection about the ends
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < n3; ++k)
     for (int j = 0; j < n2; ++j)
@@ -429,6 +431,9 @@ static void deriv3d(int id, const Grid& g, int axis, int icon, const double w1[1
           } else if (wrap) {
             int qq = (q < 0) ? q + n : q - n;
             acc += (sgn * cd[m]) * f[base + qq * stride];
+          } else if (mirror) {
+            int qq = (q < 0) ? -q : 2 * (n - 1) - q;
+            acc += cd[m] * f[base + qq * stride];
           }
         }
         df[p] = acc;

@@ -61,7 +61,7 @@ def oracle_kernels(ctx, o):
 
 
 @pytest.mark.parametrize("n", [(32, 32, 32), (48, 40, 36), (64, 64, 64), (40, 30, 24)])
-@pytest.mark.parametrize("icon", [13, 8])
+@pytest.mark.parametrize("icon", [13, 8, 24])
 def test_poten_matches_oracle(n, icon):
     w = C.replace(small_dyn(n_imp=0), nx=n[0], ny=n[1], nz=n[2], icon=icon, noise=0.05)
     den = C.woods_saxon(w)
@@ -185,8 +185,11 @@ def test_steppc_errors_and_ring_match_oracle():
                                        rtol=1e-10, atol=1e-14)
 
 
-def test_short_axis_and_periodic_dynamics():
-    w = C.replace(small_dyn(n=32, n_imp=1), nz=12, zmax=6.0, icon=8,
+@pytest.mark.parametrize("icon", [8, 24])
+def test_short_axis_and_boundary_dynamics(icon):
+    """A 12-point z axis (derivative off, init_deriv_parallel.f90:949-953) with periodic (8) or
+    mirror (24, redef.f:245-279) boundaries on the other axes."""
+    w = C.replace(small_dyn(n=32, n_imp=1), nz=12, zmax=6.0, icon=icon,
                   rimp0=((0.5, -0.3, 1.0),), vimp0_aps=((0.0, 0.0, 0.0),))
     o = O.Dynamics(w.as_dict(), m_imp_u=w.m_imp_u)
     ref = run_dynamics(w, 5, o)

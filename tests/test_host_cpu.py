@@ -44,7 +44,7 @@ def test_tstgrid_sizes_enforced():
 
 @pytest.mark.parametrize("kw,text", [
     (dict(npd=11), "npd"),
-    (dict(icon=24), "icon"),
+    (dict(icon=25), "icon"),
     (dict(core=b"XX "), "core4"),
     (dict(core=b"OTC", den0s=0.0), "den0s"),
     (dict(core=b"OTE"), "core4"),

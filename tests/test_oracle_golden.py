@@ -81,6 +81,60 @@ def test_icon13_boundary_rows_are_zero_padding(k):
     np.testing.assert_allclose(ref, padded, rtol=0, atol=1e-13)
 
 
+def redef_icon24(cd):
+    """redef.f:245-279 (ICON=24: rows K..KO2+2 from the centred row, folded at the last point)
+    then, with TORNA, :18-56 (ICON=4, IP=+1: rows 1..KO2 folded at the first point), written out
+    loop by loop on the row-major K x K block (CD(j + (i-1)K) = c[i-1, j-1])."""
+    c = cd.copy()
+    k, ko2, ko2p1 = 13, 6, 7
+    i0 = ko2p1
+    C = lambda i, j: c[i - 1, j - 1]
+    for i in range(k, ko2 + 1, -1):            # I = K..KO2+2
+        j0 = ko2p1 - i + k
+        j1 = j0
+        c[i - 1, k - 1] = C(i0, j0)
+        for j in range(k - 1, 0, -1):
+            j0 -= 1
+            j1 += 1
+            if j0 >= 1:
+                c[i - 1, j - 1] = C(i0, j0) + C(i0, j1) if j1 <= k else C(i0, j0)
+            else:
+                c[i - 1, j - 1] = 0.0
+    for i in range(1, ko2 + 1):                # ICON=4, I = 1..KO2
+        j0 = ko2p1 - i + 1
+        j1 = j0
+        c[i - 1, 0] = C(i0, j0)
+        for j in range(2, k + 1):
+            j0 += 1
+            j1 -= 1
+            if j0 <= k:
+                c[i - 1, j - 1] = C(i0, j0) + C(i0, j1) if j1 >= 1 else C(i0, j0)
+            else:
+                c[i - 1, j - 1] = 0.0
+    return c
+
+
+@pytest.mark.parametrize("k", [1, 2])
+def test_icon24_boundary_rows_are_even_reflection(k):
+    """icon=24's Redef rows equal the centred stencil on a field reflected evenly about its first
+    and last points (numpy's 'reflect' padding), which the oracle and device stencils use."""
+    c = redef_icon24(golden_matrix(k))
+    centred = golden_matrix(k)[6]
+    n = 20
+    f = np.random.default_rng(2).normal(size=n)
+    fp = np.pad(f, 6, mode="reflect")
+    mirrored = np.array([centred @ fp[i:i + 13] for i in range(n)])
+    ref = np.empty(n)
+    for i in range(n):
+        if i < 6:
+            ref[i] = c[i] @ f[:13]
+        elif i >= n - 6:
+            ref[i] = c[i - n + 13] @ f[n - 13:]
+        else:
+            ref[i] = centred @ f[i - 6:i + 7]
+    np.testing.assert_allclose(ref, mirrored, rtol=0, atol=1e-12)
+
+
 def test_bforce_matches_b4():
     b_ot = O.lib().ho_bforce(0, CONST["eps4"], CONST["sigma4"], CONST["h4ot"])
     b_op = O.lib().ho_bforce(1, CONST["eps4"], CONST["sigma4"], CONST["h4op"])
@@ -128,7 +182,7 @@ def np_deriv(f, w, h, axis, icon=13):
         return np.zeros_like(f)
     pad = [(0, 0)] * 3
     pad[axis] = (6, 6)
-    fp = np.pad(f, pad, mode="wrap" if icon == 8 else "constant")
+    fp = np.pad(f, pad, mode={8: "wrap", 24: "reflect"}.get(icon, "constant"))
     out = np.zeros_like(f)
     for m in range(13):
         sl = [slice(None)] * 3
@@ -137,7 +191,7 @@ def np_deriv(f, w, h, axis, icon=13):
     return out / h
 
 
-@pytest.mark.parametrize("icon", [13, 8])
+@pytest.mark.parametrize("icon", [13, 8, 24])
 @pytest.mark.parametrize("id_", [1, 2])
 def test_derivatives(icon, id_):
     n = (20, 16, 14)
