@@ -454,6 +454,44 @@ def run_quantum(args):
         print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """The serving workload: a seeded Poisson stream of trajectory requests (N log-uniform in
+    [300, 10000], classical Morse impurity at U(100,500) m/s), each args.req_steps driver
+    iterations on the smallest grid that holds its droplet, scheduled with continuous batching
+    under an HBM budget (he_dft_2024_b200/serving.py)."""
+    import torch
+    from he_dft_2024_b200 import serving as S
+    from he_dft_2024_b200.context import Context
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    reqs = S.make_requests(count=args.requests, rate_hz=args.rate, steps=args.req_steps,
+                           seed=1234 + rank)
+    srv = S.Server(lambda w: Context(w), hbm_budget_gb=args.hbm_gb,
+                   max_active=args.max_active if args.max_active > 0 else None)
+    with ClockSampler(local) as clk:
+        rep = srv.run(reqs)
+    launches = None
+    line = {
+        "metric": "TDDFT serving: aggregate grid-pt-steps/s (FP64, continuous batching)",
+        "value": rep["grid_pt_steps_per_s"], "unit": UNIT, "n_gpus": ws, "steps": rep["ticks"],
+        "warmup": 0, "ms_per_step": rep["step_ms_p50"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"serve-{args.requests}req-poisson{args.rate:g}hz-{args.req_steps}steps",
+                   "requests": args.requests, "rate_hz": args.rate, "steps_per_request": args.req_steps,
+                   "hbm_budget_gb": args.hbm_gb, "max_active": args.max_active,
+                   "grids": rep["grids"], "parallelism": f"replicas{ws}"},
+        "latency": {k: rep[k] for k in ("step_ms_p50", "step_ms_p99", "trajectory_s_p50",
+                                         "trajectory_s_p99")},
+        "peak_active": rep["peak_active"], "peak_device_gb": rep["peak_device_gb"],
+        "wall_s": rep["wall_s"], "gpu_launches": launches, "clocks": clk.summary(),
+        "e2e": {"value": rep["grid_pt_steps_per_s"], "unit": UNIT, "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None,
+                "note": "wall clock from the first arrival to the last completion, set-up included"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -509,11 +547,18 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="classical", choices=["classical", "quantum"])
+    ap.add_argument("--workload", default="classical", choices=["classical", "quantum", "serving"])
     ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--requests", type=int, default=128)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--req-steps", type=int, default=1000)
+    ap.add_argument("--hbm-gb", type=float, default=120.0)
+    ap.add_argument("--max-active", type=int, default=0, help="0: no cap (HBM budget only)")
     args = ap.parse_args()
     if args.workload == "quantum" and args.impl == "ours":
         run_quantum(args)
+    elif args.workload == "serving" and args.impl == "ours":
+        run_serving(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -147,6 +147,7 @@ def load():
         "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
         "he_set_quantum_impurities": (ip, [vp, ctypes.POINTER(HeQImpurities)]),
         "he_qimp_moments": (ip, [vp, dp]),
+        "he_observables": (ip, [vp, ip, dp]),
         "he_ft_v_spline_table": (ip, [ctypes.POINTER(HePairPot), d, d, ip, ip, dp, ip,
                                       ctypes.c_char_p, ctypes.c_size_t]),
         "he_energy_noalloc": (ip, [ctypes.POINTER(HeGrid), ctypes.POINTER(HeFunctional), ip, vp,

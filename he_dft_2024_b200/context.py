@@ -191,6 +191,15 @@ class Context:
         q.n_spline, q.nq, q.parabolic = w.n_spline, w.nq, w.parabolic
         self._ck(self.L.he_set_quantum_impurities(self.h, ctypes.byref(q)))
 
+    OBSERVABLES = ("n", "xcm", "ycm", "zcm", "lx", "ly", "lz", "vcomx", "vcomy", "vcomz",
+                   "r2x", "r2y", "r2z")
+
+    def observables(self, npart):
+        """Droplet observables of the dynamics drivers (N, r_cm, <L>, <Vcom>, <r^2>)."""
+        out = np.zeros(13)
+        self._ck(self.L.he_observables(self.h, int(npart), dptr(out)))
+        return dict(zip(self.OBSERVABLES, out))
+
     def qimp_moments(self):
         """(N_imp, 4): norm, <x>, <y>, <z> of each impurity density."""
         n = self.w.nq_imp

@@ -47,7 +47,8 @@ enum Slot {
   S_QII = 57,       // quantum: impurity-pair sums (eimpu_impu), 6 slots
   S_QMOM = 64,      // quantum: moments, 4 per impurity
   S_ALF = 80,       // alpha_s energy sum
-  S_COUNT = 96
+  S_OBS = 96,       // observables, 16 sums
+  S_COUNT = 112
 };
 
 }  // namespace
@@ -2444,6 +2445,32 @@ int he_ft_v_spline_table(const he_pairpot_t* pot, double pmax, double hp, int n_
     return e == cudaErrorInvalidValue ? HE_ERR_ARG : HE_ERR_CUDA;
   }
   std::memcpy(vpp, V.data(), sizeof(double) * n_p);
+  return HE_OK;
+}
+
+int he_observables(he_ctx_t* ctx, int npart, double* out) {
+  if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (ctx->mode == HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "observables need a complex psi");
+  if (npart <= 0) return fail(ctx, HE_ERR_ARG, "npart must be positive");
+  OpObservables op{};
+  op.s8[0] = ctx->den;
+  op.x0 = -ctx->xmax; op.y0 = -ctx->ymax; op.z0 = -ctx->zmax;
+  op.hx = ctx->hx; op.hy = ctx->hy; op.hz = ctx->hz;
+  TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_OBS));
+  TRY(read_sums(ctx));
+  const double* s = ctx->hsum + S_OBS;
+  const double dxyz = ctx->dxyz;
+  const double mhe = 4.002572164 * kMpU;  // DFT4He3d.f90:103, :315
+  const double auxn4 = s[9] * dxyz;
+  const double xcm = s[10] * dxyz / npart, ycm = s[11] * dxyz / npart, zcm = s[12] * dxyz / npart;
+  // <L> = Re sum i conj(psi) (r - r_cm) x grad psi dxyz, Re(i w) = -Im w
+  const double lz = -(s[3] - s[4] - ycm * s[0] + xcm * s[1]) * dxyz;
+  const double ly = -(s[5] - s[6] - xcm * s[2] + zcm * s[0]) * dxyz;
+  const double lx = -(s[7] - s[8] - zcm * s[1] + ycm * s[2]) * dxyz;
+  const double v[13] = {auxn4, xcm, ycm, zcm, lx, ly, lz,
+                        s[0] * dxyz / (auxn4 * mhe), s[1] * dxyz / (auxn4 * mhe), s[2] * dxyz / (auxn4 * mhe),
+                        s[13] * dxyz, s[14] * dxyz, s[15] * dxyz};
+  std::memcpy(out, v, sizeof(v));
   return HE_OK;
 }
 

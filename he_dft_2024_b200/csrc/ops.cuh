@@ -169,6 +169,45 @@ struct OpEnergy {
   }
 };
 
+// Droplet observables of the dynamics driver (Dynamics_TDDFT/DFT4He3d.f90:720-838, r_cm.f90) in
+// one pass over psi: with c_a = conj(psi) d_a psi, acc holds
+//   [0..2]  Im sum c_x, c_y, c_z                   (<Vcom> = Im sum c_a dxyz / (N mhe))
+//   [3..8]  Im sum y c_x, x c_y, x c_z, z c_x, z c_y, y c_z   (<L> about the origin; the
+//           shift to the centre of mass uses [0..2] on the host)
+//   [9..15] sum den, den x, den y, den z, den x^2, den y^2, den z^2     (N, r_cm, <r^2>)
+struct OpObservables {
+  static const char* kname() { return "observables_reduce"; }
+  using T = double2;
+  static constexpr int NV = 16, N8 = 1, N16 = 0;
+  const double* s8[N8];      // den
+  const double2* s16[1];
+  double x0, y0, z0, hx, hy, hz;
+  HE_D void at(int ix, int iy, int iz, long, double2 dx, double2 dy, double2 dz, double2 c,
+               const double* v8, const double2*, int, double* acc) const {
+    const double x = x0 + hx * ix, y = y0 + hy * iy, z = z0 + hz * iz;
+    const double cx = c.x * dx.y - c.y * dx.x;  // Im conj(psi) d_x psi
+    const double cy = c.x * dy.y - c.y * dy.x;
+    const double cz = c.x * dz.y - c.y * dz.x;
+    acc[0] += cx;
+    acc[1] += cy;
+    acc[2] += cz;
+    acc[3] += y * cx;
+    acc[4] += x * cy;
+    acc[5] += x * cz;
+    acc[6] += z * cx;
+    acc[7] += z * cy;
+    acc[8] += y * cz;
+    const double d = v8[0];
+    acc[9] += d;
+    acc[10] += d * x;
+    acc[11] += d * y;
+    acc[12] += d * z;
+    acc[13] += d * (x * x);
+    acc[14] += d * (y * y);
+    acc[15] += d * (z * z);
+  }
+};
+
 // derden(): dxden, dyden, dzden (derden.f90:26-28).
 struct OpDerden {
   static const char* kname() { return "derden"; }

@@ -241,6 +241,15 @@ int he_qimp_moments(he_ctx_t* ctx, double* out);
 int he_ft_v_spline_table(const he_pairpot_t* pot, double pmax, double hp, int n_spline,
                          int parabolic, double* vpp, int n_p, char* err, size_t errlen);
 
+/* Droplet observables the dynamics drivers print every pener steps
+ * (Dynamics_TDDFT/DFT4He3d.f90:720-838 with r_cm.f90; Dynamics_quantum_impurities/DFT4He3d.f90
+ * has the same): out[13] = {N = sum den dxyz, r_cm (x, y, z) = sum den r dxyz / npart,
+ * <L> (x, y, z) = Re sum i conj(psi) (r - r_cm) x grad psi dxyz,
+ * <Vcom> (x, y, z) = Re sum -i conj(psi) grad psi dxyz / (N mhe), mhe = 4.002572164 mp_u,
+ * <r^2> (x, y, z) = sum den x^2 dxyz, ...}.  One fused pass over psi and den; synchronises.
+ * Not in statics mode (real psi). */
+int he_observables(he_ctx_t* ctx, int npart, double* out);
+
 /* ---- He_statics call surface ---- */
 /* The driver's per-iteration refresh (BCN4HeDFT.f90:1131-1155): derden, fftfw(den,fden),
  * dencg = fftbk(fden*wcgk), and delj4 = fftbk(fden*fvlj4) which the statics poten() recomputes

@@ -606,6 +606,61 @@ struct Common {
 };
 
 // ------------------------------------------------------------------------------------------------
+// Droplet observables printed every pener steps (Dynamics_TDDFT/DFT4He3d.f90:720-838, r_cm.f90),
+// with the reference's loops: out = {N, xcm, ycm, zcm, Lx, Ly, Lz, Vcomx, Vcomy, Vcomz, <x^2>,
+// <y^2>, <z^2>}.
+// ------------------------------------------------------------------------------------------------
+static void observables(const Grid& g, const ho_params& p, const double w1[13], const double w2[13],
+                        const std::vector<cplx>& psi, const std::vector<double>& den, int npart,
+                        double* out) {
+  const long N = g.nxyz;
+  std::vector<cplx> s1(N), s2(N), s3(N);
+  double auxn4 = 0;
+  for (long i = 0; i < N; ++i) auxn4 += den[i];
+  auxn4 = auxn4 * g.dxyz;
+  double xcm = 0, ycm = 0, zcm = 0;  // r_cm.f90:38-52
+  for (int iz = 0; iz < g.nz; ++iz)
+    for (int iy = 0; iy < g.ny; ++iy)
+      for (int ix = 0; ix < g.nx; ++ix) {
+        const double a = den[ix + (long)g.nx * (iy + (long)g.ny * iz)];
+        xcm = xcm + a * g.x[ix];
+        ycm = ycm + a * g.y[iy];
+        zcm = zcm + a * g.z[iz];
+      }
+  xcm = xcm * g.dxyz / npart;
+  ycm = ycm * g.dxyz / npart;
+  zcm = zcm * g.dxyz / npart;
+  deriv3d<cplx>(1, g, 0, p.icon, w1, w2, psi.data(), s1.data());
+  deriv3d<cplx>(1, g, 1, p.icon, w1, w2, psi.data(), s2.data());
+  deriv3d<cplx>(1, g, 2, p.icon, w1, w2, psi.data(), s3.data());
+  const cplx ci(0.0, 1.0);
+  cplx lx = 0, ly = 0, lz = 0, vx = 0, vy = 0, vz = 0;
+  double r2x = 0, r2y = 0, r2z = 0;
+  for (int iz = 0; iz < g.nz; ++iz)
+    for (int iy = 0; iy < g.ny; ++iy)
+      for (int ix = 0; ix < g.nx; ++ix) {
+        const long i = ix + (long)g.nx * (iy + (long)g.ny * iz);
+        const cplx c = std::conj(psi[i]);
+        const double X = g.x[ix] - xcm, Y = g.y[iy] - ycm, Z = g.z[iz] - zcm;
+        lz = lz + ci * c * (Y * s1[i] - X * s2[i]);
+        ly = ly + ci * c * (X * s3[i] - Z * s1[i]);
+        lx = lx + ci * c * (Z * s2[i] - Y * s3[i]);
+        vx = vx - ci * c * s1[i];
+        vy = vy - ci * c * s2[i];
+        vz = vz - ci * c * s3[i];
+        r2x = r2x + den[i] * (g.x[ix] * g.x[ix]);
+        r2y = r2y + den[i] * (g.y[iy] * g.y[iy]);
+        r2z = r2z + den[i] * (g.z[iz] * g.z[iz]);
+      }
+  const double mhe = 4.002572164 * 0.02061484;  // DFT4He3d.f90:103, :315
+  const double v[13] = {auxn4, xcm, ycm, zcm, (lx * g.dxyz).real(), (ly * g.dxyz).real(),
+                        (lz * g.dxyz).real(), (vx * g.dxyz).real() / (auxn4 * mhe),
+                        (vy * g.dxyz).real() / (auxn4 * mhe), (vz * g.dxyz).real() / (auxn4 * mhe),
+                        r2x * g.dxyz, r2y * g.dxyz, r2z * g.dxyz};
+  std::memcpy(out, v, sizeof(v));
+}
+
+// ------------------------------------------------------------------------------------------------
 // Real-time TDDFT with classical impurities (Dynamics_TDDFT).
 // ------------------------------------------------------------------------------------------------
 struct Dyn : Common {
@@ -1959,4 +2014,12 @@ void ho_spline(const double* x, const double* y, double s1, double sn, int n, do
   spline_maron(x, y, a, b, c, d, s1, sn, n);
 }
 int ho_findi(const double* x, double xc, int n) { return findi(x, xc, n); }
+void ho_dyn_observables(void* h, int npart, double* out) {
+  Dyn* d = (Dyn*)h;
+  observables(d->g, d->p, d->w1, d->w2, d->psi, d->den, npart, out);
+}
+void ho_qdyn_observables(void* h, int npart, double* out) {
+  QDyn* d = (QDyn*)h;
+  observables(d->g, d->p, d->w1, d->w2, d->psi, d->den, npart, out);
+}
 }

@@ -126,6 +126,8 @@ def lib():
         L.ho_ft_vpp_point.restype = cd
         L.ho_ft_vpp_point.argtypes = [dp, cd, ci, ci]
         L.ho_spline.argtypes = [dp, dp, cd, cd, ci, dp, dp, dp, dp]
+        L.ho_dyn_observables.argtypes = [vp, ci, dp]
+        L.ho_qdyn_observables.argtypes = [vp, ci, dp]
         L.ho_findi.restype = ci
         L.ho_findi.argtypes = [dp, cd, ci]
         _lib = L
@@ -204,6 +206,14 @@ class Dynamics(_Fields):
         return dict(zip(ENERGY_KEYS, e))
 
     def lstopimp(self): return bool(self.L.ho_dyn_lstopimp(self.h))
+
+    OBSERVABLES = ("n", "xcm", "ycm", "zcm", "lx", "ly", "lz", "vcomx", "vcomy", "vcomz",
+                   "r2x", "r2y", "r2z")
+
+    def observables(self, npart):
+        out = np.zeros(13)
+        self.L.ho_dyn_observables(self.h, int(npart), _dp(out))
+        return dict(zip(self.OBSERVABLES, out))
 
     def ring(self, values=None):
         """Get (or set) ioldp(3), ioldh(2), ioldr(3), ioldv(3), iolda(2)."""
