@@ -64,6 +64,13 @@ struct he_ctx {
   double w1[13], w2[13];
   StencilGeom g1{}, g2{};
   cudaStream_t stream = nullptr, own = nullptr;
+  // Side stream for the classical-impurity work (the impurity field pass over den and the
+  // one-CTA integrator kernels), which overlaps the FFT chain and the He stencils.  Work on it
+  // is joined into `stream` before any kernel that reads uimp or the impurity state, writes den,
+  // or reduces through the shared partials, and before every host transfer or synchronisation.
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool aux_pending = false, on_aux = false;
   std::string err;
   long long launches = 0;
   size_t bytes = 0;
@@ -200,6 +207,49 @@ static int dalloc_t(he_ctx_t* ctx, T** p, size_t count) {
   return dalloc(ctx, reinterpret_cast<void**>(p), count * sizeof(T));
 }
 
+// ---- side stream (see he_ctx::aux) ----------------------------------------------------------
+static bool overlap_on(const he_ctx_t* ctx) {
+  return ctx->aux && ctx->mode == HE_MODE_DYNAMICS && ctx->n_imp > 0 && !ctx->timing;
+}
+static int join_aux(he_ctx_t* ctx) {
+  if (!ctx->aux_pending || ctx->on_aux) return HE_OK;
+  CK(cudaEventRecord(ctx->ev_join, ctx->aux));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  ctx->aux_pending = false;
+  return HE_OK;
+}
+// Orders the side stream after everything issued so far on the main stream.
+static int fork_aux(he_ctx_t* ctx) {
+  CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+  return HE_OK;
+}
+// Stream for an impurity-state kernel (the side stream when overlapping).
+static cudaStream_t imp_stream(he_ctx_t* ctx) {
+  if (!overlap_on(ctx)) return ctx->stream;
+  ctx->aux_pending = true;
+  return ctx->aux;
+}
+// Redirects the context's launches to the side stream for its lifetime.
+struct OnAux {
+  he_ctx_t* c;
+  cudaStream_t saved;
+  explicit OnAux(he_ctx_t* ctx) : c(ctx), saved(ctx->stream) {
+    c->stream = c->aux;
+    c->on_aux = true;
+  }
+  ~OnAux() {
+    c->stream = saved;
+    c->on_aux = false;
+    c->aux_pending = true;
+  }
+};
+static int sync_all(he_ctx_t* ctx) {
+  TRY(join_aux(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HE_OK;
+}
+
 static bool factor_ok(int n) {
   if (n < 1) return false;
   while (n % 2 == 0) n /= 2;
@@ -243,7 +293,7 @@ static int make_plan(he_ctx_t* ctx, int n, LinePlan* pl) {
   double2* d = nullptr;
   TRY(dalloc_t(ctx, &d, stw.size()));
   CK(cudaMemcpyAsync(d, stw.data(), stw.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   pl->tw = d;
   pl->stw = d;
   pl->stw_len = (int)stw.size();
@@ -327,6 +377,7 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
                             (int)smem));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<Op, kTX, kTY>, kTX * kTY, smem));
   }
+  TRY(join_aux(ctx));  // stencils read uimp / write den / reduce through the shared partials
   StencilGeom g = g0;
   g.zc = choose_zc(ctx, occ);
   dim3 grid = stencil_grid(ctx, g), block(kTX, kTY);
@@ -519,13 +570,15 @@ static size_t wf_elem(const he_ctx_t* ctx) {
 }
 
 static int imp_pull(he_ctx_t* ctx, ImpDev* h) {
+  TRY(join_aux(ctx));
   CK(cudaMemcpyAsync(h, ctx->imp, sizeof(ImpDev), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 static int imp_push(he_ctx_t* ctx, const ImpDev* h) {
+  TRY(join_aux(ctx));
   CK(cudaMemcpyAsync(ctx->imp, h, sizeof(ImpDev), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 
@@ -797,8 +850,9 @@ static int stat_normalize(he_ctx_t* ctx, int n4) {
 }
 
 static int read_sums(he_ctx_t* ctx) {
+  TRY(join_aux(ctx));
   CK(cudaMemcpyAsync(ctx->hsum, ctx->sums, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 
@@ -1470,7 +1524,7 @@ static int q_kernel(he_ctx_t* ctx, const he_pairpot_t& v, int nspline, int nq, i
   tname(ctx, "uimp_k_spline");
   k_uimpk<<<kPwBlocks, 256, 0, ctx->stream>>>(u);
   LAUNCHED();
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 
@@ -1505,7 +1559,7 @@ static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
       std::vector<double> acc(N, 0.0), t(N);
       for (int i = 0; i < n; ++i) {
         CK(cudaMemcpyAsync(t.data(), ctx->denx[i], 8 * N, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        TRY(sync_all(ctx));
         for (size_t k = 0; k < N; ++k) acc[k] = acc[k] + t[k];
       }
       std::memcpy(host, acc.data(), 8 * N);
@@ -1526,7 +1580,7 @@ static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
     }
     h += p.second;
   }
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   if (up && field == HE_F_PSIX)
     for (int i = 0; i < n; ++i) TRY(q_cnorm2(ctx, i));
   if (up && (field == HE_F_PSIX || field == HE_F_UIMPK || field == HE_F_UIMPKK)) ctx->cglj_pending = false;
@@ -1602,6 +1656,13 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (e != cudaSuccess)
     return fail(ctx, HE_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
   ctx->stream = ctx->own;
+  if (mode == HE_MODE_DYNAMICS) {
+    e = cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      return fail(ctx, HE_ERR_CUDA, "side stream creation failed: %s", cudaGetErrorString(e));
+  }
 
   // FFT plans and shared-memory budgets
   TRY(make_plan(ctx, ctx->nx, &ctx->plx));
@@ -1675,17 +1736,21 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   TRY(dalloc_t(ctx, &ctx->sums, S_COUNT));
   CK(cudaMallocHost(&ctx->hsum, S_COUNT * sizeof(double)));
   TRY(autotune_tiles(ctx));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 
 void he_ctx_destroy(he_ctx_t* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->hsum) cudaFreeHost(ctx->hsum);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->own) cudaStreamDestroy(ctx->own);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   delete ctx;
 }
 
@@ -1695,14 +1760,14 @@ size_t he_device_bytes(const he_ctx_t* ctx) { return ctx ? ctx->bytes : 0; }
 
 int he_set_stream(he_ctx_t* ctx, void* stream) {
   if (!ctx) return HE_ERR_ARG;
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
   return HE_OK;
 }
 
 int he_synchronize(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 
@@ -1712,7 +1777,7 @@ int he_set_kernels(he_ctx_t* ctx, const double* fvlj4, const double* wcgk, const
   if (ctx->otc) CK(cudaMemcpyAsync(ctx->kalfs, kalfs, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->fvlj4, fvlj4, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->wcgk, wcgk, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   ctx->kernels_ok = true;
   return HE_OK;
 }
@@ -1728,7 +1793,7 @@ int he_compute_kernels(he_ctx_t* ctx) {
   tname(ctx, "kspace_kernels");
   k_kernels<<<kPwBlocks, 256, 0, ctx->stream>>>(a);
   LAUNCHED();
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   ctx->kernels_ok = true;
   return HE_OK;
 }
@@ -1740,7 +1805,7 @@ int he_set_absorber(he_ctx_t* ctx, const he_absorber_t* ab) {
     std::vector<double> t(n);
     for (int i = 0; i < n; ++i) t[i] = std::tanh((std::fabs(-xm + h * i) - mean) / surf);
     CK(cudaMemcpyAsync(dst, t.data(), 8 * n, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    TRY(sync_all(ctx));
     return HE_OK;
   };
   TRY(tab(ctx->nx, ctx->xmax, ctx->hx, ab->txmean, ab->txsurf, ctx->tabx));
@@ -1778,7 +1843,7 @@ int he_set_impurities(he_ctx_t* ctx, const he_impurities_t* im) {
     for (int k = 0; k < im->n_imp; ++k)
       for (int i = 0; i < im->npot; ++i) t[(size_t)k * im->npot + i] = im->potion[k + (size_t)im->n_imp * i];
     CK(cudaMemcpyAsync(ctx->pot_tab, t.data(), 8 * t.size(), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    TRY(sync_all(ctx));
   }
   ctx->npot = im->npot;
   ctx->delinter = im->delinter;
@@ -1789,6 +1854,7 @@ int he_set_impurities(he_ctx_t* ctx, const he_impurities_t* im) {
 
 int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   if (!ctx || !host) return fail(ctx, HE_ERR_ARG, "null argument");
+  TRY(join_aux(ctx));
   if (qfield(field)) return q_xfer(ctx, field, const_cast<void*>(host), bytes, true);
   if (field >= HE_F_RIMP && field <= HE_F_QV) {
     if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "no impurities in statics");
@@ -1807,7 +1873,7 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   TRY(field_ref(ctx, field, &r));
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
   CK(cudaMemcpyAsync(r.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   if (field == HE_F_FVLJ4 || field == HE_F_WCGK) ctx->kernels_ok = true;
   if (field == HE_F_DEN) ctx->force_fresh = false;
   if (field == HE_F_DEN || field == HE_F_FDEN || field == HE_F_FVLJ4 || field == HE_F_WCGK)
@@ -1817,6 +1883,7 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
 
 int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
   if (!ctx || !host) return fail(ctx, HE_ERR_ARG, "null argument");
+  TRY(join_aux(ctx));
   if (qfield(field)) return q_xfer(ctx, field, host, bytes, false);
   if (field == HE_F_RING) {
     if (bytes != 13 * 8) return fail(ctx, HE_ERR_ARG, "ring: expected 104 bytes");
@@ -1847,7 +1914,7 @@ int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
   TRY(field_ref(ctx, field, &r));
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
   CK(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   return HE_OK;
 }
 
@@ -1897,10 +1964,20 @@ int he_potenimp(he_ctx_t* ctx) {
     return HE_OK;
   }
   int st;
-  if (ctx->n_imp <= 1) st = launch_impfield<1>(ctx);
-  else if (ctx->n_imp <= 2) st = launch_impfield<2>(ctx);
-  else if (ctx->n_imp <= 4) st = launch_impfield<4>(ctx);
-  else st = launch_impfield<8>(ctx);
+  auto launch = [&]() {
+    if (ctx->n_imp <= 1) return launch_impfield<1>(ctx);
+    if (ctx->n_imp <= 2) return launch_impfield<2>(ctx);
+    if (ctx->n_imp <= 4) return launch_impfield<4>(ctx);
+    return launch_impfield<8>(ctx);
+  };
+  if (overlap_on(ctx)) {
+    // the field pass reads den (ready on the main stream) and the impurity state (side stream)
+    TRY(fork_aux(ctx));
+    OnAux on(ctx);
+    st = launch();
+  } else {
+    st = launch();
+  }
   if (st == HE_OK) ctx->force_fresh = true;
   return st;
 }
@@ -1913,7 +1990,7 @@ int he_forceimp(he_ctx_t* ctx, double* F) {
   // rimp; redo it if either changed since.
   if (!ctx->force_fresh) TRY(he_potenimp(ctx));
   tname(ctx, "impurity_force");
-  k_imp_force<<<1, 128, 0, ctx->stream>>>(ctx->imp, ctx->sums + S_FORCE, ctx->dxyz);
+  k_imp_force<<<1, 128, 0, imp_stream(ctx)>>>(ctx->imp, ctx->sums + S_FORCE, ctx->dxyz);
   LAUNCHED();
   if (F) {
     ImpDev h;
@@ -1928,7 +2005,7 @@ int he_set_accel(he_ctx_t* ctx) {
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "dynamics routine");
   if (ctx->n_imp == 0) return HE_OK;
   tname(ctx, "impurity_accel");
-  k_imp_accel<<<1, 128, 0, ctx->stream>>>(ctx->imp);
+  k_imp_accel<<<1, 128, 0, imp_stream(ctx)>>>(ctx->imp);
   LAUNCHED();
   return HE_OK;
 }
@@ -1972,7 +2049,7 @@ int he_steprk(he_ctx_t* ctx, double deltat) {
     ctx->force_fresh = false;
     if (ctx->n_imp > 0) {
       tname(ctx, "impurity_rk");
-      k_imp_rk<<<1, 128, 0, ctx->stream>>>(ctx->imp, jr, arun[jr], brun[jr], crun[jr], deltat);
+      k_imp_rk<<<1, 128, 0, imp_stream(ctx)>>>(ctx->imp, jr, arun[jr], brun[jr], crun[jr], deltat);
       LAUNCHED();
     }
     if (jr <= 2) TRY(field_eval(ctx));
@@ -2013,7 +2090,7 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   ctx->force_fresh = false;
   if (ctx->n_imp > 0) {
     tname(ctx, "impurity_predict");
-    k_imp_predict<<<1, 128, 0, ctx->stream>>>(ctx->imp, deltat);
+    k_imp_predict<<<1, 128, 0, imp_stream(ctx)>>>(ctx->imp, deltat);
     LAUNCHED();
   }
   TRY(field_eval(ctx));
@@ -2042,14 +2119,15 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   ctx->force_fresh = false;
   if (ctx->n_imp > 0) {
     tname(ctx, "impurity_correct");
-    k_imp_correct<<<1, 128, 0, ctx->stream>>>(ctx->imp, deltat);
+    k_imp_correct<<<1, 128, 0, imp_stream(ctx)>>>(ctx->imp, deltat);
     LAUNCHED();
   }
   if (errHe || errimp || errvimp) {
+    TRY(join_aux(ctx));
     CK(cudaMemcpyAsync(ctx->hsum, ctx->sums, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     ImpDev h;
     if (ctx->n_imp > 0) TRY(imp_pull(ctx, &h));
-    CK(cudaStreamSynchronize(ctx->stream));
+    TRY(sync_all(ctx));
     if (errHe) *errHe = c9 * ctx->hsum[S_ERRHE] / (double)ctx->N;
     if (errimp) *errimp = ctx->n_imp > 0 ? h.errimp : 0.0;
     if (errvimp) *errvimp = ctx->n_imp > 0 ? h.errvimp : 0.0;
@@ -2080,8 +2158,9 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
     TRY(run_stencil_red(ctx, ctx->g1, (const double*)ctx->psi, op, S_EN));
   }
   if (ctx->otc) TRY(alfa_energy_sum(ctx));
+  TRY(join_aux(ctx));
   CK(cudaMemcpyAsync(ctx->hsum, ctx->sums, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   const double* s = ctx->hsum + S_EN;
   const double dxyz = ctx->dxyz;
   he_energies_t e{};
@@ -2292,7 +2371,7 @@ int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu) {
 
 int he_timing(he_ctx_t* ctx, int enable) {
   if (!ctx) return HE_ERR_ARG;
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   ctx->trec.clear();
   ctx->evnext = 0;
   ctx->timing = enable != 0;
@@ -2307,7 +2386,7 @@ int he_timing(he_ctx_t* ctx, int enable) {
 
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n) {
   if (!ctx || !n) return fail(ctx, HE_ERR_ARG, "null argument");
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   std::vector<he_kernel_time_t> agg;
   for (const auto& r : ctx->trec) {
     if (!r.b) continue;
@@ -2393,7 +2472,7 @@ int he_set_quantum_impurities(he_ctx_t* ctx, const he_qimpurities_t* q) {
       }
       TRY(q_kernel(ctx, q->x_x[i + n * j], nspline, q->nq, q->parabolic, kk));
     }
-  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(sync_all(ctx));
   for (int i = 0; i < n; ++i) TRY(q_cnorm2(ctx, i));
   for (int i = 0; i < 3; ++i) ctx->ioldp[i] = i + 1;
   ctx->ioldh[0] = 1; ctx->ioldh[1] = 2;
