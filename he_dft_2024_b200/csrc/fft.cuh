@@ -32,6 +32,7 @@ struct LinePlan {
   const double2* tw;     // device table exp(-2 pi i m / n), m = 0..n-1
   const double2* stw;    // per-stage twiddles [stage][r-1][k], k < ns(stage)
   int stw_len;           // entries in stw
+  const double2* tw2;    // register y pass (fft_reg.cuh): W_N^(a k1) at [k1 N2 + a], N entries
 };
 
 // Greedy radix choice shared by host and device: 8, then 4, 2, 3, 5.

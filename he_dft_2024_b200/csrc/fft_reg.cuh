@@ -1,0 +1,246 @@
+// fft_reg.cuh -- y pass of the half spectrum for the common line lengths with the line transform
+// held in registers (binary64).  Same result as k_ypass (fft_kernels.cuh): every (kx, z) line of
+// the (nx/2+1, ny, nz) array is transformed along y, forward (exp(-i)) or inverse (exp(+i),
+// unscaled), in place.
+//
+// N = N1 * N2, n = a + N2 m, k = k1 + N1 k2:
+//   phase A: thread (c, a) loads x[a + N2 m], m < N1, of column kx0 + c straight from HBM/L2
+//            (consecutive threads hold consecutive kx: each load instruction reads TK*16
+//            contiguous bytes), does the N1-point DFT over m in registers, multiplies by
+//            W_N^(a k1) and stores T[k1][a][c] to shared memory;
+//   phase B: thread (c, k1) reads T[k1][a][c], a < N2, does the N2-point DFT over a in registers
+//            and stores X[k1 + N1 k2] straight to memory.
+// One shared-memory exchange per line and no staging copies: the pass is a load, two register
+// DFTs and a store per element.  The small DFTs are composed from radix 2, 3, 4, 5 with constant
+// twiddles (exact for the quarter turns).
+#pragma once
+#include "fft_kernels.cuh"
+
+namespace he {
+
+template <int N> struct Split;
+template <> struct Split<32> { static constexpr int N1 = 4, N2 = 8; };
+template <> struct Split<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct Split<96> { static constexpr int N1 = 8, N2 = 12; };
+template <> struct Split<128> { static constexpr int N1 = 8, N2 = 16; };
+template <> struct Split<160> { static constexpr int N1 = 10, N2 = 16; };
+template <> struct Split<192> { static constexpr int N1 = 12, N2 = 16; };
+template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+
+// Host-side mirror of Split (0 when n has no register path).
+HE_HD constexpr int split_n1(int n) {
+  return n == 32 ? 4 : n == 64 ? 8 : n == 96 ? 8 : n == 128 ? 8 : n == 160 ? 10 : n == 192 ? 12 : n == 256 ? 16 : 0;
+}
+
+// cos(2 pi j / m), sin(2 pi j / m) for m dividing 16, 12 or 10 (decimal expansions of the
+// algebraic values cos(pi/8), cos(pi/6), cos(pi/5), ...).
+HE_HD constexpr double c16(int j) {
+  switch (((j % 16) + 16) % 16) {
+    case 0: return 1.0;
+    case 1: case 15: return 0.92387953251128675613;
+    case 2: case 14: return 0.70710678118654752440;
+    case 3: case 13: return 0.38268343236508977173;
+    case 4: case 12: return 0.0;
+    case 5: case 11: return -0.38268343236508977173;
+    case 6: case 10: return -0.70710678118654752440;
+    case 7: case 9: return -0.92387953251128675613;
+    default: return -1.0;
+  }
+}
+HE_HD constexpr double c12(int j) {
+  switch (((j % 12) + 12) % 12) {
+    case 0: return 1.0;
+    case 1: case 11: return 0.86602540378443864676;
+    case 2: case 10: return 0.5;
+    case 3: case 9: return 0.0;
+    case 4: case 8: return -0.5;
+    case 5: case 7: return -0.86602540378443864676;
+    default: return -1.0;
+  }
+}
+HE_HD constexpr double c10(int j) {
+  switch (((j % 10) + 10) % 10) {
+    case 0: return 1.0;
+    case 1: case 9: return 0.80901699437494742410;
+    case 2: case 8: return 0.30901699437494742410;
+    case 3: case 7: return -0.30901699437494742410;
+    case 4: case 6: return -0.80901699437494742410;
+    default: return -1.0;
+  }
+}
+HE_HD constexpr double s10(int j) {
+  switch (((j % 10) + 10) % 10) {
+    case 1: case 4: return 0.58778525229247312917;
+    case 2: case 3: return 0.95105651629515357212;
+    case 6: case 9: return -0.58778525229247312917;
+    case 7: case 8: return -0.95105651629515357212;
+    default: return 0.0;
+  }
+}
+HE_HD constexpr double cos2pi(int j, int m) {
+  return (16 % m == 0) ? c16(j * (16 / m)) : (12 % m == 0) ? c12(j * (12 / m)) : c10(j * (10 / m));
+}
+HE_HD constexpr double sin2pi(int j, int m) {
+  return (16 % m == 0) ? c16(j * (16 / m) + 12) : (12 % m == 0) ? c12(j * (12 / m) + 9) : s10(j * (10 / m));
+}
+
+// x * W_M^E (forward W = exp(-2 pi i E / M); INV conjugates).
+template <int M, int E, bool INV>
+HE_D double2 twc(double2 x) {
+  constexpr int e = ((E % M) + M) % M;
+  if constexpr (e == 0) return x;
+  else if constexpr (2 * e == M) return make_double2(-x.x, -x.y);
+  else if constexpr (4 * e == M) return INV ? cpi(x) : cmi(x);
+  else if constexpr (4 * e == 3 * M) return INV ? cmi(x) : cpi(x);
+  else {
+    constexpr double c = cos2pi(e, M);
+    constexpr double s = INV ? sin2pi(e, M) : -sin2pi(e, M);
+    return make_double2(x.x * c - x.y * s, x.x * s + x.y * c);
+  }
+}
+
+// In-register DFT of length M (natural order in and out).
+template <int M, bool INV> struct RDft;
+
+template <bool INV> struct RDft<2, INV> {
+  static HE_D void run(double2* v) {
+    const double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+template <bool INV> struct RDft<3, INV> {
+  static HE_D void run(double2* v) {
+    const double c = -0.5, s = 0.86602540378443864676;
+    const double2 t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    const double2 m = make_double2(v[0].x + c * t.x, v[0].y + c * t.y);
+    const double2 sd = cscale(s, d);
+    const double2 isd = INV ? cpi(sd) : cmi(sd);
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(m, isd);
+    v[2] = csub(m, isd);
+  }
+};
+template <bool INV> struct RDft<4, INV> {
+  static HE_D void run(double2* v) {
+    const double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const double2 t2 = cadd(v[1], v[3]), u = csub(v[1], v[3]);
+    const double2 mu = INV ? cpi(u) : cmi(u);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, mu);
+    v[3] = csub(t1, mu);
+  }
+};
+template <bool INV> struct RDft<5, INV> {
+  static HE_D void run(double2* v) {
+    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+    const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const double2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+    const double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const double2 b1 = make_double2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
+    const double2 b2 = make_double2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
+    const double2 ib1 = INV ? cpi(b1) : cmi(b1);
+    const double2 ib2 = INV ? cpi(b2) : cmi(b2);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, ib1);
+    v[4] = csub(a1, ib1);
+    v[2] = cadd(a2, ib2);
+    v[3] = csub(a2, ib2);
+  }
+};
+
+// Composite length A*B with n = a + B m, k = k1 + A k2.
+template <int A, int B, bool INV, int AA, int K1>
+HE_D void rdft_tw(const double2 (&u)[A], double2 (&t)[A * B]) {
+  if constexpr (K1 < A) {
+    t[K1 * B + AA] = twc<A * B, AA * K1, INV>(u[K1]);
+    rdft_tw<A, B, INV, AA, K1 + 1>(u, t);
+  }
+}
+template <int A, int B, bool INV, int AA = 0>
+HE_D void rdft_rows(const double2* v, double2 (&t)[A * B]) {
+  if constexpr (AA < B) {
+    double2 u[A];
+#pragma unroll
+    for (int m = 0; m < A; ++m) u[m] = v[AA + B * m];
+    RDft<A, INV>::run(u);
+    rdft_tw<A, B, INV, AA, 0>(u, t);
+    rdft_rows<A, B, INV, AA + 1>(v, t);
+  }
+}
+template <int A, int B, bool INV, int K1 = 0>
+HE_D void rdft_cols(double2* v, const double2 (&t)[A * B]) {
+  if constexpr (K1 < A) {
+    double2 w[B];
+#pragma unroll
+    for (int a = 0; a < B; ++a) w[a] = t[K1 * B + a];
+    RDft<B, INV>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) v[K1 + A * k2] = w[k2];
+    rdft_cols<A, B, INV, K1 + 1>(v, t);
+  }
+}
+template <int A, int B, bool INV> struct RDftComp {
+  static HE_D void run(double2* v) {
+    double2 t[A * B];
+    rdft_rows<A, B, INV>(v, t);
+    rdft_cols<A, B, INV>(v, t);
+  }
+};
+template <bool INV> struct RDft<8, INV> : RDftComp<2, 4, INV> {};
+template <bool INV> struct RDft<10, INV> : RDftComp<2, 5, INV> {};
+template <bool INV> struct RDft<12, INV> : RDftComp<4, 3, INV> {};
+template <bool INV> struct RDft<16, INV> : RDftComp<4, 4, INV> {};
+
+// Threads of a y-pass CTA: TK columns x N2.
+HE_HD constexpr int yreg_threads(int n, int tk) { return tk * (n / split_n1(n)); }
+
+template <int N, int TK, bool INV>
+HE_D void ypass_reg_body(const YZArgs& a, const double2* __restrict__ tw2, double2* T) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  const int tid = threadIdx.x;
+  const int nxh = a.nxh;
+  const int kx0 = blockIdx.x * TK;
+  double2* arr = a.arr[blockIdx.z];
+  const long base = (long)nxh * N * blockIdx.y;
+  {
+    const int c = tid % TK, am = tid / TK;  // phase A: column c, a = am
+    const int kx = kx0 + c;
+    const bool ok = kx < nxh;
+    const double2* src = arr + base + (ok ? kx : 0) + (long)nxh * am;
+    double2 v[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) v[m] = ok ? src[(long)nxh * N2 * m] : make_double2(0.0, 0.0);
+    RDft<N1, INV>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul_conj_if(v[k1], __ldg(&tw2[k1 * N2 + am]), INV);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) T[(k1 * N2 + am) * TK + c] = v[k1];
+  }
+  __syncthreads();
+  if (tid < TK * N1) {
+    const int c = tid % TK, k1 = tid / TK;  // phase B: column c, k1
+    const int kx = kx0 + c;
+    double2 u[N2];
+#pragma unroll
+    for (int q = 0; q < N2; ++q) u[q] = T[(k1 * N2 + q) * TK + c];
+    RDft<N2, INV>::run(u);
+    if (kx < nxh) {
+      double2* dst = arr + base + kx + (long)nxh * k1;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) dst[(long)nxh * N1 * k2] = u[k2];
+    }
+  }
+}
+
+template <int N, int TK>
+__global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs a, const double2* tw2) {
+  extern __shared__ double2 T[];
+  if (a.inv) ypass_reg_body<N, TK, true>(a, tw2, T);
+  else ypass_reg_body<N, TK, false>(a, tw2, T);
+}
+
+}  // namespace he

@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "fft_kernels.cuh"
+#include "fft_reg.cuh"
 #include "ops.cuh"
 #include "setup.cuh"
 #include "quantum.cuh"
@@ -297,6 +298,21 @@ static int make_plan(he_ctx_t* ctx, int n, LinePlan* pl) {
   pl->tw = d;
   pl->stw = d;
   pl->stw_len = (int)stw.size();
+  pl->tw2 = nullptr;
+  const int n1 = split_n1(n);
+  if (n1 > 0) {  // register y pass: W_n^(a k1) at [k1 n2 + a]
+    const int n2 = n / n1;
+    std::vector<double2> t2((size_t)n);
+    for (int k1 = 0; k1 < n1; ++k1)
+      for (int a = 0; a < n2; ++a) {
+        long double ang = -2.0L * 3.14159265358979323846264338327950288L * ((long)a * k1) / (long double)n;
+        t2[(size_t)k1 * n2 + a] = make_double2((double)cosl(ang), (double)sinl(ang));
+      }
+    double2* d2 = nullptr;
+    TRY(dalloc_t(ctx, &d2, t2.size()));
+    CK(cudaMemcpyAsync(d2, t2.data(), t2.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    pl->tw2 = d2;
+  }
   return HE_OK;
 }
 
@@ -482,9 +498,16 @@ static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
   const size_t smem = fft_smem(ctx->ply, tk, 2);
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->nz, narr);
-  CK(cudaFuncSetAttribute(k_ypass<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, "fft_y");
-  k_ypass<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
+  if constexpr (N > 0) {
+    // register line transform (fft_reg.cuh): TK columns x N2 threads, T[k1][a][c] in shared memory
+    const size_t rsmem = sizeof(double2) * (size_t)N * tk;
+    CK(cudaFuncSetAttribute(k_ypass_reg<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+    k_ypass_reg<N, TILE><<<grid, yreg_threads(N, TILE), rsmem, ctx->stream>>>(a, ctx->ply.tw2);
+  } else {
+    CK(cudaFuncSetAttribute(k_ypass<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_ypass<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
+  }
   LAUNCHED();
   return HE_OK;
 }
