@@ -253,6 +253,36 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launches - launches0
     t_max = reduce_max(ms / 1e3, ws)
+    e_f64 = ctx.energy()["etot"] / w.n4 if args.mixed_compare else None
+
+    # ---- the mixed-precision path on the same trajectory (same steps from the same state) ----
+    mixed = None
+    if args.mixed_compare:
+        cm = Context(w, precision="mixed")
+        cm.set_stream(stream.cuda_stream)
+        prepare_state(cm, w)
+        itm = 4
+        for _ in range(args.warmup):
+            device_iteration(cm, w, itm)
+            itm += 1
+        barrier(ws)
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            device_iteration(cm, w, itm)
+            itm += 1
+        m1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        tm = reduce_max(m0.elapsed_time(m1) / 1e3, ws)
+        e_mixed = cm.energy()["etot"] / w.n4
+        cm.close()
+        mixed = {"value": N * args.steps * ws / tm, "unit": UNIT, "ms_per_step": tm * 1e3 / args.steps,
+                 "speedup_vs_f64": t_max / tm, "E_per_N_f64": e_f64, "E_per_N_mixed": e_mixed,
+                 "abs_dE_per_N_K": abs(e_mixed - e_f64), "steps_compared": 3 + args.warmup + args.steps,
+                 "note": "mean-field FFT chain in binary32, wave function, stencils and reductions "
+                         "in binary64 (HE_PREC_MIXED)"}
     value = N * args.steps * ws / t_max
 
     # ---- e2e: the driver's host-facing calls every iteration ----
@@ -315,6 +345,7 @@ def run_ours(args):
         "step_roofline_frac": (744.0 * N * args.steps / (t_max / ws)) / 1e9 / peak,
         "kernels": breakdown,
         "fft_tiles_xyz": list(tiles),
+        "mixed": mixed,
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu:
@@ -547,6 +578,8 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-iters", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", dest="mixed_compare", action="store_false",
+                    help="skip the mixed-precision comparison run")
     ap.add_argument("--workload", default="classical", choices=["classical", "quantum", "serving"])
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--requests", type=int, default=128)

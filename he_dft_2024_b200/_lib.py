@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "he_dft.h")
 HE_OK, HE_ERR_ARG, HE_ERR_CUDA, HE_ERR_STATE, HE_ERR_NOMEM = 0, 1, 2, 3, 4
 HE_MODE_DYNAMICS, HE_MODE_STATICS, HE_MODE_QUANTUM = 0, 1, 2
 HE_MAX_QIMP = 4
-HE_PREC_F64 = 0
+HE_PREC_F64, HE_PREC_MIXED = 0, 1
 
 FIELDS = dict(
     psi=0, den=1, pot4=2, dencg=3, delj4=4, uimp=5, fden=6, pc=7, q=8, psiold1=9, psiold2=10,

@@ -20,16 +20,17 @@ MODES = {"dynamics": _lib.HE_MODE_DYNAMICS, "statics": _lib.HE_MODE_STATICS,
 
 
 class Context:
-    def __init__(self, w: Workload, mode="dynamics", compute_kernels=True):
+    def __init__(self, w: Workload, mode="dynamics", compute_kernels=True, precision="f64"):
         self.L = _lib.load()
         self.w = w
         self.mode = MODES[mode]
+        self.precision = {"f64": _lib.HE_PREC_F64, "mixed": _lib.HE_PREC_MIXED}[precision]
         g = _lib.HeGrid(w.nx, w.ny, w.nz, w.xmax, w.ymax, w.zmax, w.npd, w.icon)
         core = {"OT": b"OT ", "OP": b"OP ", "OTC": b"OTC"}[w.core]
         f = _lib.HeFunctional(core, w.h4, w.eps4, w.sigma4, w.cp4, w.cpp4, w.den4c, w.alphas,
                               w.l, w.den0s, w.h2o2m4, w.lsolid, w.C, w.beta, w.den_m)
         h = ctypes.c_void_p()
-        st = self.L.he_ctx_create(ctypes.byref(g), ctypes.byref(f), self.mode, _lib.HE_PREC_F64,
+        st = self.L.he_ctx_create(ctypes.byref(g), ctypes.byref(f), self.mode, self.precision,
                                   ctypes.byref(h))
         self.h = h.value
         if st != 0:

@@ -27,6 +27,30 @@ HE_HD double2 cmi(double2 a) { return make_double2(a.y, -a.x); }
 // +i * a
 HE_HD double2 cpi(double2 a) { return make_double2(-a.y, a.x); }
 
+// ---- complex binary32 (the mixed-precision FFT chain) -------------------------------------------
+HE_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+HE_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+HE_HD float2 cscale(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+HE_HD float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+HE_HD float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+HE_HD float2 cmul_conj_if(float2 a, float2 w, bool conj_w) {
+  float wy = conj_w ? -w.y : w.y;
+  return make_float2(a.x * w.x - a.y * wy, a.x * wy + a.y * w.x);
+}
+HE_HD float2 cmi(float2 a) { return make_float2(a.y, -a.x); }
+HE_HD float2 cpi(float2 a) { return make_float2(-a.y, a.x); }
+
+// Complex type of a real type: Cx<double>::T = double2, Cx<float>::T = float2.
+template <typename R> struct Cx;
+template <> struct Cx<double> {
+  using T = double2;
+  static HE_HD double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <> struct Cx<float> {
+  using T = float2;
+  static HE_HD float2 make(float a, float b) { return make_float2(a, b); }
+};
+
 // Generic helpers so stencil code can be written once for real and complex fields.
 HE_HD double zero_of(double) { return 0.0; }
 HE_HD double2 zero_of(double2) { return make_double2(0.0, 0.0); }

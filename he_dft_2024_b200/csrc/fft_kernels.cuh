@@ -51,6 +51,8 @@ struct XArgs {
   const double* extra;       // C2R_POT: potx4 added after the correlation term (null: none)
   const double* extra2;      // C2R_POT: ualphas (alpha_s term) added next (null: none)
   double renor, cp4, cpp4, a0, a1;
+  double renor1;             // C2R2 out1 and C2R_POT sto1: renor over the scale of the kernel
+                             // that made specA (the mixed chain scales its wcgk copy)
   int lsolid;
   double C, beta, den_m;
 };
@@ -60,38 +62,54 @@ HE_D double corr_source(double den, double dcg, double cp4, double cpp4) {
 }
 
 // Hermitian-extended packed value Z[k] = A[k] + i B[k] of two half-spectrum rows.
-HE_D double2 packed_c2r(const double2* ra, const double2* rb, int k, int n) {
+template <typename C>
+HE_D C packed_c2r(const C* ra, const C* rb, int k, int n) {
+  using X = Cx<decltype(ra[0].x)>;
   const int nh = n / 2;
   if (k <= nh) {
-    double2 a = ra[k], b = rb[k];
-    if (k == 0 || k == nh) { a.y = 0.0; b.y = 0.0; }
-    return make_double2(a.x - b.y, a.y + b.x);
+    C a = ra[k], b = rb[k];
+    if (k == 0 || k == nh) { a.y = 0; b.y = 0; }
+    return X::make(a.x - b.y, a.y + b.x);
   }
-  double2 a = ra[n - k], b = rb[n - k];
-  return make_double2(a.x + b.y, -a.y + b.x);
+  C a = ra[n - k], b = rb[n - k];
+  return X::make(a.x + b.y, -a.y + b.x);
 }
 
 // Split a transformed packed line into the half spectra of its real and imaginary rows.
-template <int N>
-HE_D double2 split_r2c(const double2* L, int k, int n, bool second) {
-  const double2 z = L[sw<N>(k)];
-  const double2 zc = cconj(L[sw<N>((n - k) % n)]);
-  if (!second) return make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
-  return make_double2(0.5 * (z.y - zc.y), -0.5 * (z.x - zc.x));
+template <int N, typename C>
+HE_D C split_r2c(const C* L, int k, int n, bool second) {
+  using Rt = decltype(L[0].x);
+  using X = Cx<Rt>;
+  const C z = L[sw<N>(k)];
+  const C zc = cconj(L[sw<N>((n - k) % n)]);
+  if (!second) return X::make(Rt(0.5) * (z.x + zc.x), Rt(0.5) * (z.y + zc.y));
+  return X::make(Rt(0.5) * (z.y - zc.y), Rt(-0.5) * (z.x - zc.x));
 }
 
-template <int MODE, int N, int TILE>
+// Dynamic shared memory viewed as the chain's complex type.
+template <typename C>
+HE_D C* smem_as() {
+  extern __shared__ __align__(16) unsigned char he_smem_raw[];
+  return reinterpret_cast<C*>(he_smem_raw);
+}
+
+// Rt = double: the binary64 chain; Rt = float: spectra and transforms in binary32 (the mixed
+// chain), real-space inputs and outputs still binary64.
+template <int MODE, int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
-  extern __shared__ double2 smem[];
+  using C = typename Cx<Rt>::T;
+  C* smem = smem_as<C>();
+  C* specA = reinterpret_cast<C*>(a.specA);
+  const C* specB = reinterpret_cast<const C*>(a.specB);
   const int n = (N > 0) ? N : a.nx;
   const int nxh = n / 2 + 1;
   const int ls = line_stride(n);
   const int RB = (N > 0) ? TILE : a.rb;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const long r0 = (long)blockIdx.x * RB;
-  double2* tw = smem;
-  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
-  double2* P1 = P0 + RB * ls;
+  C* tw = smem;
+  C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  C* P1 = P0 + RB * ls;
   load_twiddles(tw, a.pl);
 
   if constexpr (MODE == X_R2C_DEN || MODE == X_R2C_CORR) {
@@ -100,13 +118,13 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
       const int row = e / n, x = e - row * n;
       double v = a.den[g0 + e];
       if constexpr (MODE == X_R2C_CORR) v = corr_source(v, a.dencg_in[g0 + e], a.cp4, a.cpp4);
-      reinterpret_cast<double*>(&P0[(row >> 1) * ls + sw<N>(x)])[row & 1] = v;
+      reinterpret_cast<Rt*>(&P0[(row >> 1) * ls + sw<N>(x)])[row & 1] = Rt(v);
     }
     __syncthreads();
-    double2* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, false);
+    C* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, false);
     for (int e = tid; e < RB * nxh; e += nthr) {
       const int row = e / nxh, k = e - row * nxh;
-      a.specA[(r0 + row) * nxh + k] = split_r2c<N>(R + (row >> 1) * ls, k, n, row & 1);
+      specA[(r0 + row) * nxh + k] = split_r2c<N>(R + (row >> 1) * ls, k, n, row & 1);
     }
     return;
   }
@@ -114,31 +132,31 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
   if constexpr (MODE == X_C2R2 || MODE == X_C2R2_CORR) {
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, k = e - row * n;
-      const double2* ra = a.specA + (r0 + row) * nxh;
-      const double2* rbp = a.specB + (r0 + row) * nxh;
+      const C* ra = specA + (r0 + row) * nxh;
+      const C* rbp = specB + (r0 + row) * nxh;
       P0[row * ls + sw<N>(k)] = packed_c2r(ra, rbp, k, n);
     }
     __syncthreads();
-    double2* R = fft_lines<N>(P0, P1, RB, ls, a.pl, tw, true);
-    double2* O = (R == P0) ? P1 : P0;
+    C* R = fft_lines<N>(P0, P1, RB, ls, a.pl, tw, true);
+    C* O = (R == P0) ? P1 : P0;
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
       const long g = (r0 + row) * n + x;
-      const double2 z = R[row * ls + sw<N>(x)];
-      const double dcg = z.x * a.renor;
+      const C z = R[row * ls + sw<N>(x)];
+      const double dcg = double(z.x) * a.renor1;
       a.out1[g] = dcg;
-      a.out2[g] = z.y * a.renor;
+      a.out2[g] = double(z.y) * a.renor;
       if constexpr (MODE == X_C2R2_CORR)
-        reinterpret_cast<double*>(&O[(row >> 1) * ls + sw<N>(x)])[row & 1] =
-            corr_source(a.den[g], dcg, a.cp4, a.cpp4);
+        reinterpret_cast<Rt*>(&O[(row >> 1) * ls + sw<N>(x)])[row & 1] =
+            Rt(corr_source(a.den[g], dcg, a.cp4, a.cpp4));
     }
     if constexpr (MODE == X_C2R2) return;
     __syncthreads();
-    double2* S = (O == P0) ? P1 : P0;
-    double2* R2 = fft_lines<N>(O, S, RB / 2, ls, a.pl, tw, false);
+    C* S = (O == P0) ? P1 : P0;
+    C* R2 = fft_lines<N>(O, S, RB / 2, ls, a.pl, tw, false);
     for (int e = tid; e < RB * nxh; e += nthr) {
       const int row = e / nxh, k = e - row * nxh;
-      a.specA[(r0 + row) * nxh + k] = split_r2c<N>(R2 + (row >> 1) * ls, k, n, row & 1);
+      specA[(r0 + row) * nxh + k] = split_r2c<N>(R2 + (row >> 1) * ls, k, n, row & 1);
     }
     return;
   }
@@ -147,21 +165,21 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
     // rows 2p and 2p+1 share complex line p
     for (int e = tid; e < (RB / 2) * n; e += nthr) {
       const int p = e / n, k = e - p * n;
-      const double2* ra = a.specA + (r0 + 2 * p) * nxh;
-      const double2* rbp = a.specA + (r0 + 2 * p + 1) * nxh;
+      const C* ra = specA + (r0 + 2 * p) * nxh;
+      const C* rbp = specA + (r0 + 2 * p + 1) * nxh;
       P0[p * ls + sw<N>(k)] = packed_c2r(ra, rbp, k, n);
     }
     __syncthreads();
-    double2* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, true);
+    C* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, true);
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
       const long g = (r0 + row) * n + x;
-      const double2 z = R[(row >> 1) * ls + sw<N>(x)];
-      const double sto1 = ((row & 1) ? z.y : z.x) * a.renor;
+      const C z = R[(row >> 1) * ls + sw<N>(x)];
       if constexpr (MODE == X_C2R1) {
-        a.out1[g] = sto1;
+        a.out1[g] = double((row & 1) ? z.y : z.x) * a.renor;
         continue;
       }
+      const double sto1 = double((row & 1) ? z.y : z.x) * a.renor1;
       const double dc = a.dencg_in[g];
       double pot = a.delj4_in[g] + dc * dc * (a.a0 + a.a1 * dc) + sto1;
       if (a.extra) pot = pot + a.extra[g];
@@ -188,11 +206,14 @@ struct YZArgs {
   double2* fden_out;         // forward spectrum store (may be null)
   const double* k1;
   const double* k2;          // null: single kernel
+  const float* k1f;          // binary32 copies of k1, k2 (the mixed chain)
+  const float* k2f;
 };
 
-template <int N, int TILE>
+template <int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
-  extern __shared__ double2 smem[];
+  using C = typename Cx<Rt>::T;
+  C* smem = smem_as<C>();
   const int n = (N > 0) ? N : a.ny;
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
@@ -200,19 +221,19 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int z = blockIdx.y;
-  double2* arr = a.arr[blockIdx.z];
-  double2* tw = smem;
-  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
-  double2* P1 = P0 + TK * ls;
+  C* arr = reinterpret_cast<C*>(a.arr[blockIdx.z]);
+  C* tw = smem;
+  C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  C* P1 = P0 + TK * ls;
   load_twiddles(tw, a.pl);
   const long base = (long)nxh * n * z;
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    P0[c * ls + sw<N>(j)] = (kx < nxh) ? arr[base + kx + (long)nxh * j] : make_double2(0.0, 0.0);
+    P0[c * ls + sw<N>(j)] = (kx < nxh) ? arr[base + kx + (long)nxh * j] : Cx<Rt>::make(0, 0);
   }
   __syncthreads();
-  double2* R = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, a.inv);
+  C* R = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, a.inv);
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
@@ -220,9 +241,16 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
   }
 }
 
-template <int N, int TILE>
+template <int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a) {
-  extern __shared__ double2 smem[];
+  using C = typename Cx<Rt>::T;
+  using X = Cx<Rt>;
+  constexpr bool F32 = sizeof(Rt) == 4;
+  C* smem = smem_as<C>();
+  C* io = reinterpret_cast<C*>(a.io);
+  C* out2 = reinterpret_cast<C*>(a.out2);
+  C* fden_out = reinterpret_cast<C*>(a.fden_out);
+  const bool two = F32 ? a.k2f != nullptr : a.k2 != nullptr;
   const int n = (N > 0) ? N : a.nz;
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
@@ -230,55 +258,55 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int ky = blockIdx.y;
-  double2* tw = smem;
-  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
-  double2* P1 = P0 + TK * ls;
-  double2* P2 = P1 + TK * ls;
+  C* tw = smem;
+  C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  C* P1 = P0 + TK * ls;
+  C* P2 = P1 + TK * ls;
   load_twiddles(tw, a.pl);
   const long plane = (long)nxh * a.ny;
   const long base = (long)nxh * ky;
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    P0[c * ls + sw<N>(j)] = (kx < nxh) ? a.io[base + kx + plane * j] : make_double2(0.0, 0.0);
+    P0[c * ls + sw<N>(j)] = (kx < nxh) ? io[base + kx + plane * j] : X::make(0, 0);
   }
   __syncthreads();
-  double2* F = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, false);
-  double2* O = (F == P0) ? P1 : P0;
+  C* F = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, false);
+  C* O = (F == P0) ? P1 : P0;
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
     const int s = c * ls + sw<N>(j);
     if (kx >= nxh) {
-      F[s] = make_double2(0.0, 0.0);
-      if (a.k2) P2[s] = make_double2(0.0, 0.0);
+      F[s] = X::make(0, 0);
+      if (two) P2[s] = X::make(0, 0);
       continue;
     }
     const long g = base + kx + plane * j;
-    const double2 f = F[s];
-    if (a.fden_out) a.fden_out[g] = f;
-    if (a.k2) {
-      const double w2 = a.k2[g];
-      P2[s] = make_double2(f.x * w2, f.y * w2);
+    const C f = F[s];
+    if (fden_out) fden_out[g] = f;
+    if (two) {
+      const Rt w2 = F32 ? Rt(a.k2f[g]) : Rt(a.k2[g]);
+      P2[s] = X::make(f.x * w2, f.y * w2);
     }
-    const double w1 = a.k1[g];
-    F[s] = make_double2(f.x * w1, f.y * w1);
+    const Rt w1 = F32 ? Rt(a.k1f[g]) : Rt(a.k1[g]);
+    F[s] = X::make(f.x * w1, f.y * w1);
   }
   __syncthreads();
-  double2* R1 = fft_lines<N>(F, O, TK, ls, a.pl, tw, true);
+  C* R1 = fft_lines<N>(F, O, TK, ls, a.pl, tw, true);
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) a.io[base + kx + plane * j] = R1[c * ls + sw<N>(j)];
+    if (kx < nxh) io[base + kx + plane * j] = R1[c * ls + sw<N>(j)];
   }
-  if (!a.k2) return;
+  if (!two) return;
   __syncthreads();
-  double2* S = (R1 == F) ? O : F;
-  double2* R2 = fft_lines<N>(P2, S, TK, ls, a.pl, tw, true);
+  C* S = (R1 == F) ? O : F;
+  C* R2 = fft_lines<N>(P2, S, TK, ls, a.pl, tw, true);
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) a.out2[base + kx + plane * j] = R2[c * ls + sw<N>(j)];
+    if (kx < nxh) out2[base + kx + plane * j] = R2[c * ls + sw<N>(j)];
   }
 }
 

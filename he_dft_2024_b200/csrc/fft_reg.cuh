@@ -84,48 +84,54 @@ HE_HD constexpr double sin2pi(int j, int m) {
   return (16 % m == 0) ? c16(j * (16 / m) + 12) : (12 % m == 0) ? c12(j * (12 / m) + 9) : s10(j * (10 / m));
 }
 
-// x * W_M^E (forward W = exp(-2 pi i E / M); INV conjugates).
-template <int M, int E, bool INV>
-HE_D double2 twc(double2 x) {
+// x * W_M^E (forward W = exp(-2 pi i E / M); INV conjugates), on double2 or float2.
+template <int M, int E, bool INV, typename C>
+HE_D C twc(C x) {
+  using Rt = decltype(x.x);
   constexpr int e = ((E % M) + M) % M;
   if constexpr (e == 0) return x;
-  else if constexpr (2 * e == M) return make_double2(-x.x, -x.y);
+  else if constexpr (2 * e == M) return Cx<Rt>::make(-x.x, -x.y);
   else if constexpr (4 * e == M) return INV ? cpi(x) : cmi(x);
   else if constexpr (4 * e == 3 * M) return INV ? cmi(x) : cpi(x);
   else {
-    constexpr double c = cos2pi(e, M);
-    constexpr double s = INV ? sin2pi(e, M) : -sin2pi(e, M);
-    return make_double2(x.x * c - x.y * s, x.x * s + x.y * c);
+    constexpr double cd = cos2pi(e, M);
+    constexpr double sd = INV ? sin2pi(e, M) : -sin2pi(e, M);
+    const Rt c = Rt(cd), sn = Rt(sd);
+    return Cx<Rt>::make(x.x * c - x.y * sn, x.x * sn + x.y * c);
   }
 }
 
-// In-register DFT of length M (natural order in and out).
+// In-register DFT of length M (natural order in and out) on double2 or float2.
 template <int M, bool INV> struct RDft;
 
 template <bool INV> struct RDft<2, INV> {
-  static HE_D void run(double2* v) {
-    const double2 a = v[0], b = v[1];
+  template <typename C>
+  static HE_D void run(C* v) {
+    const C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   }
 };
 template <bool INV> struct RDft<3, INV> {
-  static HE_D void run(double2* v) {
-    const double c = -0.5, s = 0.86602540378443864676;
-    const double2 t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    const double2 m = make_double2(v[0].x + c * t.x, v[0].y + c * t.y);
-    const double2 sd = cscale(s, d);
-    const double2 isd = INV ? cpi(sd) : cmi(sd);
+  template <typename C>
+  static HE_D void run(C* v) {
+    using Rt = decltype(v[0].x);
+    const Rt c = Rt(-0.5), sn = Rt(0.86602540378443864676);
+    const C t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    const C m = Cx<Rt>::make(v[0].x + c * t.x, v[0].y + c * t.y);
+    const C sd = cscale(sn, d);
+    const C isd = INV ? cpi(sd) : cmi(sd);
     v[0] = cadd(v[0], t);
     v[1] = cadd(m, isd);
     v[2] = csub(m, isd);
   }
 };
 template <bool INV> struct RDft<4, INV> {
-  static HE_D void run(double2* v) {
-    const double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-    const double2 t2 = cadd(v[1], v[3]), u = csub(v[1], v[3]);
-    const double2 mu = INV ? cpi(u) : cmi(u);
+  template <typename C>
+  static HE_D void run(C* v) {
+    const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const C t2 = cadd(v[1], v[3]), u = csub(v[1], v[3]);
+    const C mu = INV ? cpi(u) : cmi(u);
     v[0] = cadd(t0, t2);
     v[2] = csub(t0, t2);
     v[1] = cadd(t1, mu);
@@ -133,17 +139,20 @@ template <bool INV> struct RDft<4, INV> {
   }
 };
 template <bool INV> struct RDft<5, INV> {
-  static HE_D void run(double2* v) {
-    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-    const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-    const double2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
-    const double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
-    const double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
-    const double2 b1 = make_double2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
-    const double2 b2 = make_double2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
-    const double2 ib1 = INV ? cpi(b1) : cmi(b1);
-    const double2 ib2 = INV ? cpi(b2) : cmi(b2);
+  template <typename C>
+  static HE_D void run(C* v) {
+    using Rt = decltype(v[0].x);
+    using X = Cx<Rt>;
+    const Rt c1 = Rt(0.30901699437494742410), c2 = Rt(-0.80901699437494742410);
+    const Rt s1 = Rt(0.95105651629515357212), s2 = Rt(0.58778525229247312917);
+    const C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const C d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+    const C a1 = X::make(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const C a2 = X::make(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const C b1 = X::make(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
+    const C b2 = X::make(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
+    const C ib1 = INV ? cpi(b1) : cmi(b1);
+    const C ib2 = INV ? cpi(b2) : cmi(b2);
     v[0] = cadd(v[0], cadd(t1, t2));
     v[1] = cadd(a1, ib1);
     v[4] = csub(a1, ib1);
@@ -153,17 +162,17 @@ template <bool INV> struct RDft<5, INV> {
 };
 
 // Composite length A*B with n = a + B m, k = k1 + A k2.
-template <int A, int B, bool INV, int AA, int K1>
-HE_D void rdft_tw(const double2 (&u)[A], double2 (&t)[A * B]) {
+template <int A, int B, bool INV, int AA, int K1, typename C>
+HE_D void rdft_tw(const C (&u)[A], C (&t)[A * B]) {
   if constexpr (K1 < A) {
     t[K1 * B + AA] = twc<A * B, AA * K1, INV>(u[K1]);
     rdft_tw<A, B, INV, AA, K1 + 1>(u, t);
   }
 }
-template <int A, int B, bool INV, int AA = 0>
-HE_D void rdft_rows(const double2* v, double2 (&t)[A * B]) {
+template <int A, int B, bool INV, int AA = 0, typename C>
+HE_D void rdft_rows(const C* v, C (&t)[A * B]) {
   if constexpr (AA < B) {
-    double2 u[A];
+    C u[A];
 #pragma unroll
     for (int m = 0; m < A; ++m) u[m] = v[AA + B * m];
     RDft<A, INV>::run(u);
@@ -171,10 +180,10 @@ HE_D void rdft_rows(const double2* v, double2 (&t)[A * B]) {
     rdft_rows<A, B, INV, AA + 1>(v, t);
   }
 }
-template <int A, int B, bool INV, int K1 = 0>
-HE_D void rdft_cols(double2* v, const double2 (&t)[A * B]) {
+template <int A, int B, bool INV, int K1 = 0, typename C>
+HE_D void rdft_cols(C* v, const C (&t)[A * B]) {
   if constexpr (K1 < A) {
-    double2 w[B];
+    C w[B];
 #pragma unroll
     for (int a = 0; a < B; ++a) w[a] = t[K1 * B + a];
     RDft<B, INV>::run(w);
@@ -184,8 +193,9 @@ HE_D void rdft_cols(double2* v, const double2 (&t)[A * B]) {
   }
 }
 template <int A, int B, bool INV> struct RDftComp {
-  static HE_D void run(double2* v) {
-    double2 t[A * B];
+  template <typename C>
+  static HE_D void run(C* v) {
+    C t[A * B];
     rdft_rows<A, B, INV>(v, t);
     rdft_cols<A, B, INV>(v, t);
   }
@@ -198,22 +208,23 @@ template <bool INV> struct RDft<16, INV> : RDftComp<4, 4, INV> {};
 // Threads of a y-pass CTA: TK columns x N2.
 HE_HD constexpr int yreg_threads(int n, int tk) { return tk * (n / split_n1(n)); }
 
-template <int N, int TK, bool INV>
-HE_D void ypass_reg_body(const YZArgs& a, const double2* __restrict__ tw2, double2* T) {
+template <int N, int TK, bool INV, typename C>
+HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
+  using Rt = decltype(T[0].x);
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   const int tid = threadIdx.x;
   const int nxh = a.nxh;
   const int kx0 = blockIdx.x * TK;
-  double2* arr = a.arr[blockIdx.z];
+  C* arr = reinterpret_cast<C*>(a.arr[blockIdx.z]);
   const long base = (long)nxh * N * blockIdx.y;
   {
     const int c = tid % TK, am = tid / TK;  // phase A: column c, a = am
     const int kx = kx0 + c;
     const bool ok = kx < nxh;
-    const double2* src = arr + base + (ok ? kx : 0) + (long)nxh * am;
-    double2 v[N1];
+    const C* src = arr + base + (ok ? kx : 0) + (long)nxh * am;
+    C v[N1];
 #pragma unroll
-    for (int m = 0; m < N1; ++m) v[m] = ok ? src[(long)nxh * N2 * m] : make_double2(0.0, 0.0);
+    for (int m = 0; m < N1; ++m) v[m] = ok ? src[(long)nxh * N2 * m] : Cx<Rt>::make(0, 0);
     RDft<N1, INV>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul_conj_if(v[k1], __ldg(&tw2[k1 * N2 + am]), INV);
@@ -224,21 +235,23 @@ HE_D void ypass_reg_body(const YZArgs& a, const double2* __restrict__ tw2, doubl
   if (tid < TK * N1) {
     const int c = tid % TK, k1 = tid / TK;  // phase B: column c, k1
     const int kx = kx0 + c;
-    double2 u[N2];
+    C u[N2];
 #pragma unroll
     for (int q = 0; q < N2; ++q) u[q] = T[(k1 * N2 + q) * TK + c];
     RDft<N2, INV>::run(u);
     if (kx < nxh) {
-      double2* dst = arr + base + kx + (long)nxh * k1;
+      C* dst = arr + base + kx + (long)nxh * k1;
 #pragma unroll
       for (int k2 = 0; k2 < N2; ++k2) dst[(long)nxh * N1 * k2] = u[k2];
     }
   }
 }
 
-template <int N, int TK>
-__global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs a, const double2* tw2) {
-  extern __shared__ double2 T[];
+template <int N, int TK, typename Rt = double>
+__global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs a,
+                                                                   const typename Cx<Rt>::T* tw2) {
+  using C = typename Cx<Rt>::T;
+  C* T = smem_as<C>();
   if (a.inv) ypass_reg_body<N, TK, true>(a, tw2, T);
   else ypass_reg_body<N, TK, false>(a, tw2, T);
 }

@@ -85,6 +85,15 @@ struct he_ctx {
   // k space
   double2 *fden = nullptr, *wA = nullptr, *wB = nullptr;
   double *fvlj4 = nullptr, *wcgk = nullptr, *kalfs = nullptr;
+  // mixed precision (HE_PREC_MIXED): the FFT chain of the mean field in binary32, reading
+  // binary32 copies of the kernels; spectra (fden, wA, wB) then hold float2
+  bool mixed = false;
+  float *fvlj4f = nullptr, *wcgkf = nullptr;
+  // The C2R x pass packs dencg (~den) and delj4 (~den x |fvlj4(0)|, about 1e3 larger) into one
+  // complex line; in binary32 the rounding noise of delj4 would swamp dencg.  The binary32 wcgk
+  // copy is therefore scaled by the power of two nearest |fvlj4(0)/wcgk(0)| (exact), and every
+  // C2R of a wcgk product divides it out again (XArgs::renor1).  1 in binary64.
+  double cg_scale = 1.0;
   bool kernels_ok = false;
   // real fields
   double *den = nullptr, *pot4 = nullptr, *dencg = nullptr, *delj4 = nullptr, *uimp = nullptr;
@@ -294,6 +303,15 @@ static int make_plan(he_ctx_t* ctx, int n, LinePlan* pl) {
   double2* d = nullptr;
   TRY(dalloc_t(ctx, &d, stw.size()));
   CK(cudaMemcpyAsync(d, stw.data(), stw.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  {
+    std::vector<float2> sf(stw.size());
+    for (size_t i = 0; i < stw.size(); ++i) sf[i] = make_float2((float)stw[i].x, (float)stw[i].y);
+    float2* df = nullptr;
+    TRY(dalloc_t(ctx, &df, sf.size()));
+    CK(cudaMemcpyAsync(df, sf.data(), sf.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
+    TRY(sync_all(ctx));
+    pl->stwf = df;
+  }
   TRY(sync_all(ctx));
   pl->tw = d;
   pl->stw = d;
@@ -312,6 +330,13 @@ static int make_plan(he_ctx_t* ctx, int n, LinePlan* pl) {
     TRY(dalloc_t(ctx, &d2, t2.size()));
     CK(cudaMemcpyAsync(d2, t2.data(), t2.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
     pl->tw2 = d2;
+    std::vector<float2> t2f(t2.size());
+    for (size_t i = 0; i < t2.size(); ++i) t2f[i] = make_float2((float)t2[i].x, (float)t2[i].y);
+    float2* d2f = nullptr;
+    TRY(dalloc_t(ctx, &d2f, t2f.size()));
+    CK(cudaMemcpyAsync(d2f, t2f.data(), t2f.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
+    TRY(sync_all(ctx));
+    pl->tw2f = d2f;
   }
   return HE_OK;
 }
@@ -430,6 +455,7 @@ static XArgs xargs(he_ctx_t* ctx) {
   a.rb = ctx->x_rb;
   a.pl = ctx->plx;
   a.renor = ctx->renor;
+  a.renor1 = ctx->renor / ctx->cg_scale;
   a.cp4 = ctx->fn.cp4; a.cpp4 = ctx->fn.cpp4;
   a.a0 = ctx->fn.cp4 / 2.0; a.a1 = ctx->fn.cpp4 / 3.0;
   a.lsolid = ctx->fn.lsolid;
@@ -440,8 +466,8 @@ static XArgs xargs(he_ctx_t* ctx) {
 // kernels with run-time sizes (N = 0).
 #define HE_FFT_SIZES(X) X(32) X(64) X(96) X(128) X(160) X(192) X(256)
 
-static size_t fft_smem(const LinePlan& pl, int lines, int nbuf) {
-  return sizeof(double2) * (((size_t)pl.stw_len + 1) / 2 * 2 + (size_t)nbuf * lines * line_stride(pl.n));
+static size_t fft_smem(const LinePlan& pl, int lines, int nbuf, size_t elem = sizeof(double2)) {
+  return elem * (((size_t)pl.stw_len + 1) / 2 * 2 + (size_t)nbuf * lines * line_stride(pl.n));
 }
 static bool x_fast(const he_ctx_t* ctx, int tile) {
   switch (ctx->nx) {
@@ -464,52 +490,74 @@ static bool yz_fast(int n) {
 
 // Tile variants of the compile-time kernels: 16 lines per CTA (256 threads) or 8 (128 threads).
 // he_ctx_create times both for each pass family on the context's grid and keeps the faster.
-template <int MODE, int N, int TILE>
+// Rt: the chain's arithmetic (double, or float in the mixed-precision mode).
+template <int MODE, int N, int TILE, typename Rt>
 static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   const int rb = (N > 0) ? TILE : a.rb;
   const unsigned nb = (unsigned)((a.rows + rb - 1) / rb);
-  const size_t smem = fft_smem(ctx->plx, rb, 2);
+  const size_t smem = fft_smem(ctx->plx, rb, 2, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   static const char* names[6] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
                                  "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4", "fft_x_c2r"};
-  CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, names[MODE]);
-  k_xpass<MODE, N, TILE><<<nb, nthr, smem, ctx->stream>>>(a);
+  k_xpass<MODE, N, TILE, Rt><<<nb, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
-template <int MODE>
-static int xpass(he_ctx_t* ctx, const XArgs& a) {
+template <int MODE, typename Rt>
+static int xpass_t(he_ctx_t* ctx, const XArgs& a) {
   const int tile = ctx->tile_x;
   if (x_fast(ctx, tile)) {
     switch (ctx->nx) {
 #define HE_CASE(N) \
-  case N: return tile == 8 ? xpass_n<MODE, N, 8>(ctx, a) : xpass_n<MODE, N, 16>(ctx, a);
+  case N: return tile == 8 ? xpass_n<MODE, N, 8, Rt>(ctx, a) : xpass_n<MODE, N, 16, Rt>(ctx, a);
       HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
     }
   }
-  return xpass_n<MODE, 0, 16>(ctx, a);
+  return xpass_n<MODE, 0, 16, Rt>(ctx, a);
+}
+template <int MODE>
+static int xpass(he_ctx_t* ctx, const XArgs& a) {
+  return ctx->mixed ? xpass_t<MODE, float>(ctx, a) : xpass_t<MODE, double>(ctx, a);
 }
 
-template <int N, int TILE>
+template <int N, int TILE, typename Rt>
 static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
+  using C = typename Cx<Rt>::T;
   const int tk = (N > 0) ? TILE : ctx->tkx;
-  const size_t smem = fft_smem(ctx->ply, tk, 2);
+  const size_t smem = fft_smem(ctx->ply, tk, 2, sizeof(C));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->nz, narr);
   tname(ctx, "fft_y");
   if constexpr (N > 0) {
     // register line transform (fft_reg.cuh): TK columns x N2 threads, T[k1][a][c] in shared memory
-    const size_t rsmem = sizeof(double2) * (size_t)N * tk;
-    CK(cudaFuncSetAttribute(k_ypass_reg<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
-    k_ypass_reg<N, TILE><<<grid, yreg_threads(N, TILE), rsmem, ctx->stream>>>(a, ctx->ply.tw2);
+    const size_t rsmem = sizeof(C) * (size_t)N * tk;
+    const C* tw2;
+    if constexpr (sizeof(Rt) == 4) tw2 = ctx->ply.tw2f;
+    else tw2 = ctx->ply.tw2;
+    CK(cudaFuncSetAttribute(k_ypass_reg<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+    k_ypass_reg<N, TILE, Rt><<<grid, yreg_threads(N, TILE), rsmem, ctx->stream>>>(a, tw2);
   } else {
-    CK(cudaFuncSetAttribute(k_ypass<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_ypass<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
+    CK(cudaFuncSetAttribute(k_ypass<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_ypass<N, TILE, Rt><<<grid, nthr, smem, ctx->stream>>>(a);
   }
   LAUNCHED();
   return HE_OK;
+}
+template <typename Rt>
+static int ypass_t(he_ctx_t* ctx, const YZArgs& a, int narr) {
+  const int tile = ctx->tile_y;
+  if (yz_fast(ctx->ny)) {
+    switch (ctx->ny) {
+#define HE_CASE(N) \
+  case N: return tile == 8 ? ypass_n<N, 8, Rt>(ctx, a, narr) : ypass_n<N, 16, Rt>(ctx, a, narr);
+      HE_FFT_SIZES(HE_CASE)
+#undef HE_CASE
+    }
+  }
+  return ypass_n<0, 16, Rt>(ctx, a, narr);
 }
 static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
   YZArgs a{};
@@ -518,29 +566,40 @@ static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
   a.arr[0] = a0; a.arr[1] = a1 ? a1 : a0;
   a.inv = inv;
   const int narr = a1 ? 2 : 1;
-  const int tile = ctx->tile_y;
-  if (yz_fast(ctx->ny)) {
-    switch (ctx->ny) {
+  return ctx->mixed ? ypass_t<float>(ctx, a, narr) : ypass_t<double>(ctx, a, narr);
+}
+
+template <int N, int TILE, typename Rt>
+static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
+  const int tk = (N > 0) ? TILE : ctx->tkx;
+  const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
+  const int nthr = (N > 0) ? tile_threads(TILE) : 256;
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
+  CK(cudaFuncSetAttribute(k_zconv<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
+  k_zconv<N, TILE, Rt><<<grid, nthr, smem, ctx->stream>>>(a);
+  LAUNCHED();
+  return HE_OK;
+}
+template <typename Rt>
+static int zconv_t(he_ctx_t* ctx, const YZArgs& a) {
+  const int tile = ctx->tile_z;
+  if (yz_fast(ctx->nz)) {
+    switch (ctx->nz) {
 #define HE_CASE(N) \
-  case N: return tile == 8 ? ypass_n<N, 8>(ctx, a, narr) : ypass_n<N, 16>(ctx, a, narr);
+  case N: return tile == 8 ? zconv_n<N, 8, Rt>(ctx, a) : zconv_n<N, 16, Rt>(ctx, a);
       HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
     }
   }
-  return ypass_n<0, 16>(ctx, a, narr);
+  return zconv_n<0, 16, Rt>(ctx, a);
 }
-
-template <int N, int TILE>
-static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
-  const int tk = (N > 0) ? TILE : ctx->tkx;
-  const size_t smem = fft_smem(ctx->plz, tk, 3);
-  const int nthr = (N > 0) ? tile_threads(TILE) : 256;
-  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
-  CK(cudaFuncSetAttribute(k_zconv<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
-  k_zconv<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
-  LAUNCHED();
-  return HE_OK;
+// binary32 copy of a binary64 k-space kernel (the mixed chain reads these)
+static const float* kernel_f32(const he_ctx_t* ctx, const double* k) {
+  if (!k) return nullptr;
+  if (k == ctx->wcgk) return ctx->wcgkf;
+  if (k == ctx->fvlj4) return ctx->fvlj4f;
+  return nullptr;
 }
 static int zconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, const double* k2,
                  double2* fden_out) {
@@ -548,16 +607,11 @@ static int zconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, co
   a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
   a.pl = ctx->plz;
   a.io = io; a.out2 = out2; a.fden_out = fden_out; a.k1 = k1; a.k2 = k2;
-  const int tile = ctx->tile_z;
-  if (yz_fast(ctx->nz)) {
-    switch (ctx->nz) {
-#define HE_CASE(N) \
-  case N: return tile == 8 ? zconv_n<N, 8>(ctx, a) : zconv_n<N, 16>(ctx, a);
-      HE_FFT_SIZES(HE_CASE)
-#undef HE_CASE
-    }
-  }
-  return zconv_n<0, 16>(ctx, a);
+  if (!ctx->mixed) return zconv_t<double>(ctx, a);
+  a.k1f = kernel_f32(ctx, k1);
+  a.k2f = kernel_f32(ctx, k2);
+  if (!a.k1f || (k2 && !a.k2f)) return fail(ctx, HE_ERR_STATE, "no binary32 copy of a k-space kernel");
+  return zconv_t<float>(ctx, a);
 }
 
 // fden = R2C(den); wA <- fden*wcgk and wB <- fden*fvlj4 back in (x-transformed) row space.
@@ -1610,6 +1664,33 @@ static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
   return HE_OK;
 }
 
+__global__ void __launch_bounds__(256) k_to_f32(const double* __restrict__ a, float* __restrict__ b,
+                                                long n, double scale) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    b[i] = (float)(a[i] * scale);
+}
+// Refreshes the binary32 kernel copies of the mixed chain after the binary64 kernels changed;
+// wcgk's copy carries the power-of-two scale cg_scale (see he_ctx).
+static int kernels_to_f32(he_ctx_t* ctx) {
+  if (!ctx->mixed) return HE_OK;
+  double k0[2];
+  CK(cudaMemcpyAsync(&k0[0], ctx->fvlj4, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&k0[1], ctx->wcgk, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  TRY(sync_all(ctx));
+  ctx->cg_scale = 1.0;
+  if (std::isfinite(k0[0]) && std::isfinite(k0[1]) && k0[0] != 0.0 && k0[1] != 0.0) {
+    const int e = (int)std::lround(std::log2(std::fabs(k0[0] / k0[1])));
+    ctx->cg_scale = std::ldexp(1.0, std::max(-30, std::min(30, e)));
+  }
+  tname(ctx, "kernels_to_f32");
+  k_to_f32<<<kPwBlocks, 256, 0, ctx->stream>>>(ctx->fvlj4, ctx->fvlj4f, ctx->Nk, 1.0);
+  LAUNCHED();
+  tname(ctx, "kernels_to_f32");
+  k_to_f32<<<kPwBlocks, 256, 0, ctx->stream>>>(ctx->wcgk, ctx->wcgkf, ctx->Nk, ctx->cg_scale);
+  LAUNCHED();
+  return HE_OK;
+}
+
 extern "C" {
 
 int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, int precision,
@@ -1625,7 +1706,11 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   };
   if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS && mode != HE_MODE_QUANTUM)
     bad(HE_ERR_ARG, "unknown mode");
-  else if (precision != HE_PREC_F64) bad(HE_ERR_ARG, "unknown precision");
+  else if (precision != HE_PREC_F64 && precision != HE_PREC_MIXED) bad(HE_ERR_ARG, "unknown precision");
+  else if (precision == HE_PREC_MIXED && mode != HE_MODE_DYNAMICS)
+    bad(HE_ERR_ARG, "HE_PREC_MIXED is built for HE_MODE_DYNAMICS");
+  else if (precision == HE_PREC_MIXED && std::strncmp(fun->core4, "OTC", 3) == 0)
+    bad(HE_ERR_ARG, "HE_PREC_MIXED does not cover core4='OTC'");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
   else if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18 &&
            grid->icon != 24)
@@ -1651,6 +1736,7 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   }
   ctx->mode = mode;
   ctx->prec = precision;
+  ctx->mixed = precision == HE_PREC_MIXED;
   ctx->nx = grid->nx; ctx->ny = grid->ny; ctx->nz = grid->nz;
   ctx->nxh = grid->nx / 2 + 1;
   ctx->N = (long)grid->nx * grid->ny * grid->nz;
@@ -1710,6 +1796,10 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   TRY(dalloc_t(ctx, &ctx->wB, Nk));
   TRY(dalloc_t(ctx, &ctx->fvlj4, Nk));
   TRY(dalloc_t(ctx, &ctx->wcgk, Nk));
+  if (ctx->mixed) {
+    TRY(dalloc_t(ctx, &ctx->fvlj4f, Nk));
+    TRY(dalloc_t(ctx, &ctx->wcgkf, Nk));
+  }
   TRY(dalloc_t(ctx, &ctx->den, N));
   TRY(dalloc_t(ctx, &ctx->pot4, N));
   TRY(dalloc_t(ctx, &ctx->dencg, N));
@@ -1800,6 +1890,7 @@ int he_set_kernels(he_ctx_t* ctx, const double* fvlj4, const double* wcgk, const
   if (ctx->otc) CK(cudaMemcpyAsync(ctx->kalfs, kalfs, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->fvlj4, fvlj4, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->wcgk, wcgk, 8 * ctx->Nk, cudaMemcpyHostToDevice, ctx->stream));
+  TRY(kernels_to_f32(ctx));
   TRY(sync_all(ctx));
   ctx->kernels_ok = true;
   return HE_OK;
@@ -1816,6 +1907,7 @@ int he_compute_kernels(he_ctx_t* ctx) {
   tname(ctx, "kspace_kernels");
   k_kernels<<<kPwBlocks, 256, 0, ctx->stream>>>(a);
   LAUNCHED();
+  TRY(kernels_to_f32(ctx));
   TRY(sync_all(ctx));
   ctx->kernels_ok = true;
   return HE_OK;
@@ -1895,9 +1987,15 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   FieldRef r;
   TRY(field_ref(ctx, field, &r));
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
+  if (field == HE_F_FDEN && ctx->mixed) return fail(ctx, HE_ERR_STATE, "fden holds binary32 in HE_PREC_MIXED");
   CK(cudaMemcpyAsync(r.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
   TRY(sync_all(ctx));
-  if (field == HE_F_FVLJ4 || field == HE_F_WCGK) ctx->kernels_ok = true;
+  if (field == HE_F_FVLJ4 || field == HE_F_WCGK) {
+    ctx->kernels_ok = true;
+    TRY(kernels_to_f32(ctx));
+    TRY(sync_all(ctx));
+  }
+
   if (field == HE_F_DEN) ctx->force_fresh = false;
   if (field == HE_F_DEN || field == HE_F_FDEN || field == HE_F_FVLJ4 || field == HE_F_WCGK)
     ctx->cglj_pending = false;
@@ -1936,6 +2034,14 @@ int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
   FieldRef r;
   TRY(field_ref(ctx, field, &r));
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
+  if (field == HE_F_FDEN && ctx->mixed) {  // the mixed chain keeps fden as float2
+    std::vector<float2> t(ctx->Nk);
+    CK(cudaMemcpyAsync(t.data(), r.ptr, 8 * ctx->Nk, cudaMemcpyDeviceToHost, ctx->stream));
+    TRY(sync_all(ctx));
+    double2* o = (double2*)host;
+    for (long i = 0; i < ctx->Nk; ++i) o[i] = make_double2(t[i].x, t[i].y);
+    return HE_OK;
+  }
   CK(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   TRY(sync_all(ctx));
   return HE_OK;

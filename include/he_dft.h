@@ -38,7 +38,12 @@ typedef struct he_ctx he_ctx_t;
 /* HE_MODE_QUANTUM: real-time dynamics with quantum impurities (Dynamics_quantum_impurities):
  * complex psi plus impurity wave functions psix_i (he_set_quantum_impurities). */
 enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1, HE_MODE_QUANTUM = 2 };
-enum he_precision { HE_PREC_F64 = 0 };
+/* HE_PREC_F64: binary64 throughout.  HE_PREC_MIXED (HE_MODE_DYNAMICS, OT/OP cores): the FFT chain
+ * of the mean field (poten's convolutions) runs in binary32 on binary32 copies of the k-space
+ * kernels, with binary64 inputs and outputs (den in; dencg, delj4, pot4 out); the wave function,
+ * its history, the stencils, the impurity field and every reduction stay binary64.  fden is then
+ * held as binary32 (downloads convert; uploads are refused). */
+enum he_precision { HE_PREC_F64 = 0, HE_PREC_MIXED = 1 };
 
 /* Grid: Dynamics_TDDFT/modules.f90:88-105 (grid), deriva npd/icon :31-37.  h = 2*xmax/n and
  * x_i = -xmax + h*(i-1) (DFT4He3d.f90:265-329).  npd must be 13; icon 13 (zero padding), 8

@@ -1,0 +1,72 @@
+"""The mixed-precision path (HE_PREC_MIXED: the mean field's FFT chain in binary32, wave function,
+stencils and reductions in binary64) against the binary64 path on the same inputs.
+
+Accuracy bar: the metric's |delta E/N| < 1e-5 K between the mixed and the FP64 runs of the
+classical-impurity workload, checked here over 200 driver iterations at 64^3 (and fields after one
+evaluation to binary32 accuracy)."""
+import numpy as np
+import pytest
+
+from he_dft_2024_b200 import config as C
+from he_dft_2024_b200 import driver as D
+from he_dft_2024_b200.context import Context
+
+pytestmark = pytest.mark.gpu
+
+
+def workload(n=64):
+    w = C.tddft_1000(n=n)
+    return C.replace(w, xmax=20.0 * n / 64, ymax=20.0 * n / 64, zmax=20.0 * n / 64, n4=300,
+                     rimp0=((0.5, -0.3, 8.0),), deltatps=2e-4)
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+def test_mixed_field_matches_f64_to_binary32_accuracy():
+    w = workload(32)
+    den = C.woods_saxon(w)
+    out = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, precision=prec) as ctx:
+            ctx.upload("den", den)
+            ctx.poten()
+            out[prec] = {k: ctx.download(k) for k in ("pot4", "dencg", "delj4", "fden")}
+    # binary32 rounding (not binary64, and not wrong): the FFT outputs carry a few ulp of binary32
+    # relative to their largest value.  dencg is packed with the ~1e3 larger delj4 in one
+    # complex line of the C2R pass; without the power-of-two scale of the binary32 wcgk copy its
+    # error would be ~1e-5 of its maximum
+    bound = {"pot4": 2e-6, "dencg": 2e-6, "delj4": 2e-6, "fden": 2e-6}
+    for k, b in bound.items():
+        r = rel(out["mixed"][k], out["f64"][k])
+        assert 1e-12 < r < b, (k, r)
+
+
+def test_mixed_energy_per_atom_within_1e5_K_over_200_steps():
+    w = workload(64)
+    den = C.woods_saxon(w)
+    psi = D.initial_wavefunction(w, den)
+    e = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, precision=prec) as ctx:
+            D.dynamics_setup(ctx, psi, w.n_imp)
+            hist = []
+            for it in range(1, 201):
+                D.dynamics_iteration(ctx, it, w.deltat, w.n_imp)
+                if it % 50 == 0:
+                    hist.append(ctx.energy()["etot"] / w.n4)
+            e[prec] = (np.array(hist), ctx.download("rimp"), np.sum(ctx.download("den") ** 2))
+    de = np.max(np.abs(e["mixed"][0] - e["f64"][0]))
+    assert de < 1e-5, de
+    assert np.max(np.abs(e["mixed"][1] - e["f64"][1])) < 1e-6
+    assert abs(e["mixed"][2] - e["f64"][2]) < 1e-6 * e["f64"][2]
+
+
+def test_mixed_rejects_unsupported_modes():
+    from he_dft_2024_b200._lib import HeError
+    w = workload(32)
+    with pytest.raises(HeError):
+        Context(w, mode="statics", precision="mixed")
+    with pytest.raises(HeError):
+        Context(C.replace(w, core="OTC", lsolid=0), precision="mixed")
