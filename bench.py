@@ -36,6 +36,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "TDDFT grid-pt-steps/s (FP64, 128^3 classical-impurity steppc loop)"
+
+
+def metric_for(w):
+    """The metric line of a classical workload (METRIC for the default 128^3 one)."""
+    return f"TDDFT grid-pt-steps/s (FP64, {w.nx}^3 classical-impurity steppc loop)"
 METRIC_Q = "TDDFT grid-pt-steps/s (FP64, 192^3 quantum impurity, batch of trajectories)"
 REF_MAX_STEPS = 40
 UNIT = "grid-pt-steps/s"
@@ -147,7 +152,11 @@ def barrier(ws):
 
 
 def build_workload(args):
+    """--n 256: 4He_5000 on 256^3 at h = 0.5 A (the large mixed-precision case); otherwise 4He_1000
+    with the box scaled to n (128: h = 0.625 A, the default line)."""
     from he_dft_2024_b200 import config as C
+    if args.n == 256:
+        return C.tddft_5000_256()
     return C.tddft_1000(n=args.n)
 
 
@@ -212,6 +221,24 @@ def cpu_sample(ctx, w, iters, threads):
     return dt, diff
 
 
+COMPARE_STEPS = 2000
+
+
+def advance_to(ctx, w, it, total):
+    """Untimed driver iterations until `total` have run (iterations are numbered from 1)."""
+    while it <= total:
+        device_iteration(ctx, w, it)
+        it += 1
+    return it
+
+
+def trajectory_summary(ctx, w):
+    """E/N (K), the L2 norm of den and the first impurity's z (A) of a context's current state."""
+    den = ctx.download("den")
+    return {"E_per_N": ctx.energy()["etot"] / w.n4, "rho_L2": float(np.sqrt(np.sum(den * den))),
+            "z_imp": float(ctx.download("rimp")[0, 2]) if w.n_imp else None}
+
+
 def run_ours(args):
     import torch
     from he_dft_2024_b200.context import Context
@@ -253,7 +280,10 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launches - launches0
     t_max = reduce_max(ms / 1e3, ws)
-    e_f64 = ctx.energy()["etot"] / w.n4 if args.mixed_compare else None
+    if args.mixed_compare:
+        # both trajectories are compared after COMPARE_STEPS driver iterations
+        it = advance_to(ctx, w, it, COMPARE_STEPS)
+        ref = trajectory_summary(ctx, w)
 
     # ---- the mixed-precision path on the same trajectory (same steps from the same state) ----
     mixed = None
@@ -276,11 +306,16 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier(ws)
         tm = reduce_max(m0.elapsed_time(m1) / 1e3, ws)
-        e_mixed = cm.energy()["etot"] / w.n4
+        itm = advance_to(cm, w, itm, COMPARE_STEPS)
+        got = trajectory_summary(cm, w)
         cm.close()
         mixed = {"value": N * args.steps * ws / tm, "unit": UNIT, "ms_per_step": tm * 1e3 / args.steps,
-                 "speedup_vs_f64": t_max / tm, "E_per_N_f64": e_f64, "E_per_N_mixed": e_mixed,
-                 "abs_dE_per_N_K": abs(e_mixed - e_f64), "steps_compared": 3 + args.warmup + args.steps,
+                 "speedup_vs_f64": t_max / tm, "E_per_N_f64": ref["E_per_N"],
+                 "E_per_N_mixed": got["E_per_N"],
+                 "abs_dE_per_N_K": abs(got["E_per_N"] - ref["E_per_N"]),
+                 "rel_d_rho_L2": abs(got["rho_L2"] - ref["rho_L2"]) / ref["rho_L2"],
+                 "abs_d_z_imp_A": abs(got["z_imp"] - ref["z_imp"]) if w.n_imp else None,
+                 "steps_compared": itm - 1,
                  "note": "mean-field FFT chain in binary32, wave function, stencils and reductions "
                          "in binary64 (HE_PREC_MIXED)"}
     value = N * args.steps * ws / t_max
@@ -321,19 +356,19 @@ def run_ours(args):
                  for k, v in sorted(rep.items(), key=lambda kv: -kv[1][1])}
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
+    if os.path.exists(tp) and (w.nx, w.ny, w.nz) == (128, 128, 128):  # captured at 128^3
         try:
             traffic = json.load(open(tp)).get(name)
         except Exception:
             traffic = None
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "metric": metric_for(w), "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "h_A": w.h[0], "n4": w.n4,
                    "n_imp": w.n_imp, "deltat_ps": w.deltatps, "parallelism": f"replicas{ws}",
-                   "l2": "per-step working set 0.45 GB > 126 MB L2 (no flush)"},
+                   "l2": f"per-step working set {ctx.device_bytes / 1e9:.2f} GB > 126 MB L2 (no flush)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * 3 * w.n_imp,
                 "d2h_bytes_per_step": 8 * (3 + 3 * w.n_imp * 3), "wall_s": wall_e2e},
         "gpu_launches": launches,
@@ -552,7 +587,7 @@ def run_reference(args):
     secs = time.perf_counter() - t0
     v = w.n * steps / secs
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+        "impl": "reference", "metric": metric_for(w), "value": v, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
