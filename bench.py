@@ -316,8 +316,9 @@ def run_ours(args):
                  "rel_d_rho_L2": abs(got["rho_L2"] - ref["rho_L2"]) / ref["rho_L2"],
                  "abs_d_z_imp_A": abs(got["z_imp"] - ref["z_imp"]) if w.n_imp else None,
                  "steps_compared": itm - 1,
-                 "note": "mean-field FFT chain in binary32, wave function, stencils and reductions "
-                         "in binary64 (HE_PREC_MIXED)"}
+                 "note": "HE_PREC_MIXED: FFT chain, stencils and H psi in binary32, psi and psiold "
+                         "as compensated binary32 pairs, reductions and impurity integration in "
+                         "binary64; compared with the binary64 run of the same workload"}
     value = N * args.steps * ws / t_max
 
     # ---- e2e: the driver's host-facing calls every iteration ----

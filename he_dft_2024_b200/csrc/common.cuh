@@ -60,6 +60,65 @@ HE_HD double2 axpy(double w, double2 f, double2 acc) {
 }
 HE_HD double neg_if(double v, bool n) { return n ? -v : v; }
 HE_HD double2 neg_if(double2 v, bool n) { return n ? make_double2(-v.x, -v.y) : v; }
+HE_HD float zero_of(float) { return 0.0f; }
+HE_HD float2 zero_of(float2) { return make_float2(0.0f, 0.0f); }
+HE_HD float axpy(float w, float f, float acc) { return fmaf(w, f, acc); }
+HE_HD float2 axpy(float w, float2 f, float2 acc) {
+  return make_float2(fmaf(w, f.x, acc.x), fmaf(w, f.y, acc.y));
+}
+HE_HD float neg_if(float v, bool n) { return n ? -v : v; }
+HE_HD float2 neg_if(float2 v, bool n) { return n ? make_float2(-v.x, -v.y) : v; }
+HE_HD float cnorm2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// Real type of a stencil field type (double for double/double2, float for float/float2): the
+// operand fields of a stencil consumer have the precision of the field it differentiates.
+template <typename T> struct RealOf { using R = double; using Z = double2; };
+template <> struct RealOf<float> { using R = float; using Z = float2; };
+template <> struct RealOf<float2> { using R = float; using Z = float2; };
+
+// ---- compensated binary32 pairs (hi, lo): value hi + lo, |lo| <= ulp(hi)/2 -----------------------
+// The mixed path keeps psi and its history as such pairs (about 48 significant bits) and updates
+// them with error-free transformations; the _rn intrinsics keep the compiler from contracting or
+// reassociating the steps.
+struct HL {
+  float hi, lo;
+};
+// Knuth's TwoSum: s + e = a + b exactly.
+HE_D void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+// Dekker's FastTwoSum (|a| >= |b| or a = 0): s + e = a + b exactly.
+HE_D HL fast_two_sum(float a, float b) {
+  const float s = __fadd_rn(a, b);
+  return HL{s, __fsub_rn(b, __fsub_rn(s, a))};
+}
+// (hi, lo) + b
+HE_D HL hl_add(HL a, float b) {
+  float s, e;
+  two_sum(a.hi, b, s, e);
+  return fast_two_sum(s, __fadd_rn(e, a.lo));
+}
+// (hi, lo) + (hi, lo)
+HE_D HL hl_add(HL a, HL b) {
+  float s, e;
+  two_sum(a.hi, b.hi, s, e);
+  return fast_two_sum(s, __fadd_rn(e, __fadd_rn(a.lo, b.lo)));
+}
+HE_D HL hl_neg(HL a) { return HL{-a.hi, -a.lo}; }
+// c * (hi, lo) with a binary32 constant c (the product hi*c split exactly by an fma)
+HE_D HL hl_mul(float c, HL a) {
+  const float p = __fmul_rn(c, a.hi);
+  const float e = __fmaf_rn(c, a.lo, __fmaf_rn(c, a.hi, -p));
+  return fast_two_sum(p, e);
+}
+// binary64 <-> pair (host and device)
+HE_HD HL hl_from(double v) {
+  const float h = (float)v;
+  return HL{h, (float)(v - (double)h)};
+}
+HE_HD double hl_value(HL a) { return (double)a.hi + (double)a.lo; }
 
 // ---- block reduction of NV doubles (fixed order => deterministic) ------------------------------
 template <int NV>

@@ -1,4 +1,5 @@
-// fft_kernels.cuh -- pencil passes of the mean-field convolutions (binary64).
+// fft_kernels.cuh -- pencil passes of the mean-field convolutions (binary64, or binary32 in the
+// mixed path).
 //
 // x pass (k_xpass): CTA = RB consecutive rows (y,z) of the grid; rows are contiguous in HBM.
 //   R2C: two real rows are packed as one complex line (a + i b), transformed, and split with
@@ -93,11 +94,20 @@ HE_D C* smem_as() {
   return reinterpret_cast<C*>(he_smem_raw);
 }
 
-// Rt = double: the binary64 chain; Rt = float: spectra and transforms in binary32 (the mixed
-// chain), real-space inputs and outputs still binary64.
+// Rt = double: the binary64 chain; Rt = float: the mixed path, spectra, transforms and the
+// real-space fields (den, dencg, delj4, pot4) in binary32, the pointwise prologue and epilogue
+// arithmetic in binary64.
 template <int MODE, int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
   using C = typename Cx<Rt>::T;
+  using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
+  const Rs* den = reinterpret_cast<const Rs*>(a.den);
+  const Rs* dencg_in = reinterpret_cast<const Rs*>(a.dencg_in);
+  const Rs* delj4_in = reinterpret_cast<const Rs*>(a.delj4_in);
+  const Rs* extra = reinterpret_cast<const Rs*>(a.extra);
+  const Rs* extra2 = reinterpret_cast<const Rs*>(a.extra2);
+  Rs* out1 = reinterpret_cast<Rs*>(a.out1);
+  Rs* out2 = reinterpret_cast<Rs*>(a.out2);
   C* smem = smem_as<C>();
   C* specA = reinterpret_cast<C*>(a.specA);
   const C* specB = reinterpret_cast<const C*>(a.specB);
@@ -116,8 +126,8 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
     const long g0 = r0 * n;
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
-      double v = a.den[g0 + e];
-      if constexpr (MODE == X_R2C_CORR) v = corr_source(v, a.dencg_in[g0 + e], a.cp4, a.cpp4);
+      double v = den[g0 + e];
+      if constexpr (MODE == X_R2C_CORR) v = corr_source(v, dencg_in[g0 + e], a.cp4, a.cpp4);
       reinterpret_cast<Rt*>(&P0[(row >> 1) * ls + sw<N>(x)])[row & 1] = Rt(v);
     }
     __syncthreads();
@@ -144,11 +154,11 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
       const long g = (r0 + row) * n + x;
       const C z = R[row * ls + sw<N>(x)];
       const double dcg = double(z.x) * a.renor1;
-      a.out1[g] = dcg;
-      a.out2[g] = double(z.y) * a.renor;
+      out1[g] = Rs(dcg);
+      out2[g] = Rs(double(z.y) * a.renor);
       if constexpr (MODE == X_C2R2_CORR)
         reinterpret_cast<Rt*>(&O[(row >> 1) * ls + sw<N>(x)])[row & 1] =
-            Rt(corr_source(a.den[g], dcg, a.cp4, a.cpp4));
+            Rt(corr_source(den[g], dcg, a.cp4, a.cpp4));
     }
     if constexpr (MODE == X_C2R2) return;
     __syncthreads();
@@ -176,20 +186,20 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
       const long g = (r0 + row) * n + x;
       const C z = R[(row >> 1) * ls + sw<N>(x)];
       if constexpr (MODE == X_C2R1) {
-        a.out1[g] = double((row & 1) ? z.y : z.x) * a.renor;
+        out1[g] = Rs(double((row & 1) ? z.y : z.x) * a.renor);
         continue;
       }
       const double sto1 = double((row & 1) ? z.y : z.x) * a.renor1;
-      const double dc = a.dencg_in[g];
-      double pot = a.delj4_in[g] + dc * dc * (a.a0 + a.a1 * dc) + sto1;
-      if (a.extra) pot = pot + a.extra[g];
-      if (a.extra2) pot = pot + a.extra2[g];
+      const double dc = dencg_in[g];
+      double pot = delj4_in[g] + dc * dc * (a.a0 + a.a1 * dc) + sto1;
+      if (extra) pot = pot + extra[g];
+      if (extra2) pot = pot + extra2[g];
       if (a.lsolid) {
-        const double d = a.den[g];
+        const double d = den[g];
         const double t = tanh(a.beta * (d - a.den_m));
         pot = pot + a.C * (1.0 + t + a.beta * d * (1.0 - t * t));
       }
-      a.out1[g] = pot;
+      out1[g] = Rs(pot);
     }
   }
 }

@@ -368,7 +368,10 @@ static void make_geom(he_ctx_t* ctx, int id, StencilGeom* g) {
   for (int a = 0; a < 3; ++a) {
     g->axis_on[a] = ns[a] >= 13 ? 1 : 0;
     const double sto = (id == 1) ? 1.0 / hs[a] : 1.0 / (hs[a] * hs[a]);
-    for (int m = 0; m < 13; ++m) g->w[a][m] = ((id == 1) ? ctx->w1[m] : ctx->w2[m]) * sto;
+    for (int m = 0; m < 13; ++m) {
+      g->w[a][m] = ((id == 1) ? ctx->w1[m] : ctx->w2[m]) * sto;
+      g->wf[a][m] = (float)g->w[a][m];
+    }
   }
 }
 
@@ -439,6 +442,10 @@ static int run_stencil_red(he_ctx_t* ctx, const StencilGeom& g, const typename O
                            const Op& op, int slot) {
   return run_stencil(ctx, g, f, op, slot);
 }
+
+// Planes of a compensated pair buffer of the mixed path (psi, psiold, scratch): hi, then lo.
+static float2* hi_plane(void* b) { return (float2*)b; }
+static float2* lo_plane(const he_ctx_t* ctx, void* b) { return (float2*)b + ctx->N; }
 
 static Timec timec_view(const he_ctx_t* ctx) {
   Timec t;
@@ -717,6 +724,57 @@ static int field_ref(he_ctx_t* ctx, int field, FieldRef* r) {
   return fail(ctx, HE_ERR_ARG, "field %d is not available in this context", field);
 }
 
+// Device format of a module array.  binary64 everywhere except in the mixed path, where psi and
+// psiold are compensated binary32 pairs (hi plane, then lo plane), pc, q, hpsiold and fden are
+// float2, and den, pot4, dencg, delj4, uimp are float.  he_upload / he_download convert; the
+// host side is always binary64.
+enum FieldFmt { FMT_F64 = 0, FMT_R32 = 1, FMT_C32 = 2, FMT_HL = 3 };
+static FieldFmt field_fmt(const he_ctx_t* ctx, int field) {
+  if (!ctx->mixed) return FMT_F64;
+  switch (field) {
+    case HE_F_PSI: case HE_F_PSIOLD1: case HE_F_PSIOLD2: case HE_F_PSIOLD3: return FMT_HL;
+    case HE_F_PC: case HE_F_Q: case HE_F_HPSIOLD1: case HE_F_HPSIOLD2: case HE_F_FDEN: return FMT_C32;
+    case HE_F_DEN: case HE_F_POT4: case HE_F_DENCG: case HE_F_DELJ4: case HE_F_UIMP: return FMT_R32;
+    default: return FMT_F64;
+  }
+}
+// binary64 host array of `bytes` bytes -> the device format's bytes in dev
+static void to_device_fmt(FieldFmt f, const void* host, size_t bytes, std::vector<unsigned char>& dev) {
+  const double* h = (const double*)host;
+  const size_t nv = bytes / 8;
+  if (f == FMT_R32 || f == FMT_C32) {
+    dev.resize(nv * 4);
+    float* d = (float*)dev.data();
+    for (size_t i = 0; i < nv; ++i) d[i] = (float)h[i];
+  } else {  // FMT_HL: (re, im) per point -> hi plane (re, im), lo plane (re, im)
+    dev.resize(bytes);
+    const size_t np = nv / 2;
+    float* hi = (float*)dev.data();
+    float* lo = hi + 2 * np;
+    for (size_t i = 0; i < nv; ++i) {
+      const HL v = hl_from(h[i]);
+      hi[i] = v.hi;
+      lo[i] = v.lo;
+    }
+  }
+}
+static void from_device_fmt(FieldFmt f, const std::vector<unsigned char>& dev, void* host, size_t bytes) {
+  double* h = (double*)host;
+  const size_t nv = bytes / 8;
+  if (f == FMT_R32 || f == FMT_C32) {
+    const float* d = (const float*)dev.data();
+    for (size_t i = 0; i < nv; ++i) h[i] = (double)d[i];
+  } else {
+    const size_t np = nv / 2;
+    const float* hi = (const float*)dev.data();
+    const float* lo = hi + 2 * np;
+    for (size_t i = 0; i < nv; ++i) h[i] = hl_value(HL{hi[i], lo[i]});
+  }
+}
+static size_t device_fmt_bytes(FieldFmt f, size_t host_bytes) {
+  return (f == FMT_R32 || f == FMT_C32) ? host_bytes / 2 : host_bytes;
+}
+
 static double* imp_member(ImpDev* h, int field, size_t* count) {
   const int n = h->n;
   switch (field) {
@@ -873,15 +931,19 @@ static int pw_blocks(const he_ctx_t* ctx) {
   return (int)(b < kPwBlocks ? b : kPwBlocks);
 }
 
-template <int NI>
-static int launch_impfield(he_ctx_t* ctx) {
-  OpImpField<NI> op{};
-  op.tab = ctx->pot_tab; op.imp = ctx->imp; op.uimp = ctx->uimp;
+template <int NI, typename TT>
+static int launch_impfield_t(he_ctx_t* ctx) {
+  OpImpField<NI, TT> op{};
+  op.tab = ctx->pot_tab; op.imp = ctx->imp; op.uimp = (TT*)ctx->uimp;
   op.n = ctx->n_imp; op.npot = ctx->npot;
   op.delinter = ctx->delinter; op.rmax = ctx->rmaxinterpol;
   op.xmax = ctx->xmax; op.ymax = ctx->ymax; op.zmax = ctx->zmax;
   op.hx = ctx->hx; op.hy = ctx->hy; op.hz = ctx->hz;
-  return run_stencil_red(ctx, ctx->g1, ctx->den, op, S_FORCE);
+  return run_stencil_red(ctx, ctx->g1, (const TT*)ctx->den, op, S_FORCE);
+}
+template <int NI>
+static int launch_impfield(he_ctx_t* ctx) {
+  return ctx->mixed ? launch_impfield_t<NI, float>(ctx) : launch_impfield_t<NI, double>(ctx);
 }
 
 static int field_eval(he_ctx_t* ctx) {  // potenimp; poten; forceimp
@@ -1987,9 +2049,16 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   FieldRef r;
   TRY(field_ref(ctx, field, &r));
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
-  if (field == HE_F_FDEN && ctx->mixed) return fail(ctx, HE_ERR_STATE, "fden holds binary32 in HE_PREC_MIXED");
-  CK(cudaMemcpyAsync(r.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  TRY(sync_all(ctx));
+  const FieldFmt fmt = field_fmt(ctx, field);
+  if (fmt == FMT_F64) {
+    CK(cudaMemcpyAsync(r.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TRY(sync_all(ctx));
+  } else {
+    std::vector<unsigned char> dev;
+    to_device_fmt(fmt, host, bytes, dev);
+    CK(cudaMemcpyAsync(r.ptr, dev.data(), dev.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TRY(sync_all(ctx));
+  }
   if (field == HE_F_FVLJ4 || field == HE_F_WCGK) {
     ctx->kernels_ok = true;
     TRY(kernels_to_f32(ctx));
@@ -2034,12 +2103,12 @@ int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
   FieldRef r;
   TRY(field_ref(ctx, field, &r));
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
-  if (field == HE_F_FDEN && ctx->mixed) {  // the mixed chain keeps fden as float2
-    std::vector<float2> t(ctx->Nk);
-    CK(cudaMemcpyAsync(t.data(), r.ptr, 8 * ctx->Nk, cudaMemcpyDeviceToHost, ctx->stream));
+  const FieldFmt fmt = field_fmt(ctx, field);
+  if (fmt != FMT_F64) {
+    std::vector<unsigned char> dev(device_fmt_bytes(fmt, bytes));
+    CK(cudaMemcpyAsync(dev.data(), r.ptr, dev.size(), cudaMemcpyDeviceToHost, ctx->stream));
     TRY(sync_all(ctx));
-    double2* o = (double2*)host;
-    for (long i = 0; i < ctx->Nk; ++i) o[i] = make_double2(t[i].x, t[i].y);
+    from_device_fmt(fmt, dev, host, bytes);
     return HE_OK;
   }
   CK(cudaMemcpyAsync(host, r.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
@@ -2152,17 +2221,32 @@ int he_steprk(he_ctx_t* ctx, double deltat) {
   const double brun[4] = {2.0, 1.0, 1.0, 2.0};
   const double crun[4] = {0.5, 1.0 - r2, 1.0 + r2, 0.5};
   for (int jr = 0; jr < 4; ++jr) {
-    OpRK op{};
-    op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
-    op.s16[0] = (const double2*)ctx->q;
-    op.q = (double2*)ctx->q;
-    op.out = (double2*)(jr == 0 ? ctx->psiold[2] : ctx->scratch);
-    op.hsave = jr == 0 ? (double2*)ctx->hpsiold[1] : nullptr;
-    op.den = ctx->den;
-    op.tm = timec_view(ctx);
-    op.h2o2m = ctx->fn.h2o2m4;
-    op.a = arun[jr]; op.b = brun[jr]; op.cc = crun[jr]; op.dt = deltat;
-    TRY(run_stencil(ctx, ctx->g2, (const double2*)ctx->psi, op));
+    void* ob = jr == 0 ? ctx->psiold[2] : ctx->scratch;
+    if (ctx->mixed) {
+      OpRKM op{};
+      op.s8[0] = (const float*)ctx->pot4; op.s8[1] = (const float*)ctx->uimp;
+      op.s16[0] = (const float2*)ctx->q; op.s16[1] = lo_plane(ctx, ctx->psi);
+      op.q = (float2*)ctx->q;
+      op.out_hi = hi_plane(ob); op.out_lo = lo_plane(ctx, ob);
+      op.hsave = jr == 0 ? (float2*)ctx->hpsiold[1] : nullptr;
+      op.den = (float*)ctx->den;
+      op.tm = timec_view(ctx);
+      op.h2o2m = (float)ctx->fn.h2o2m4;
+      op.a = (float)arun[jr]; op.b = (float)brun[jr]; op.cc = (float)crun[jr]; op.dt = (float)deltat;
+      TRY(run_stencil(ctx, ctx->g2, hi_plane(ctx->psi), op));
+    } else {
+      OpRK op{};
+      op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
+      op.s16[0] = (const double2*)ctx->q;
+      op.q = (double2*)ctx->q;
+      op.out = (double2*)ob;
+      op.hsave = jr == 0 ? (double2*)ctx->hpsiold[1] : nullptr;
+      op.den = ctx->den;
+      op.tm = timec_view(ctx);
+      op.h2o2m = ctx->fn.h2o2m4;
+      op.a = arun[jr]; op.b = brun[jr]; op.cc = crun[jr]; op.dt = deltat;
+      TRY(run_stencil(ctx, ctx->g2, (const double2*)ctx->psi, op));
+    }
     if (jr == 0) {
       // psiold(3)=psiold(2), psiold(2)=psiold(1), psiold(1)=psi; hpsiold(2)=hpsiold(1),
       // hpsiold(1)=H psi -- done by relabelling buffers (steprk.f90:251-257).
@@ -2197,7 +2281,26 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
   }
   if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "steppc is a dynamics routine");
   const double c112 = 112.0 / 121.0, c9 = 9.0 / 121.0, c4o3 = 4.0 / 3.0;
-  {
+  if (ctx->mixed) {
+    void* p3 = ctx->psiold[ctx->ioldp[2] - 1];
+    OpPredictM op{};
+    op.s8[0] = (const float*)ctx->pot4; op.s8[1] = (const float*)ctx->uimp;
+    op.po3_hi = hi_plane(p3); op.po3_lo = lo_plane(ctx, p3);
+    op.h2 = (float2*)ctx->hpsiold[ctx->ioldh[1] - 1];
+    op.s16[0] = op.po3_hi;
+    op.s16[1] = op.po3_lo;
+    op.s16[2] = (const float2*)ctx->hpsiold[ctx->ioldh[0] - 1];
+    op.s16[3] = op.h2;
+    op.s16[4] = (const float2*)ctx->pc;
+    op.den = (float*)ctx->den;
+    op.tm = timec_view(ctx);
+    op.h2o2m = (float)ctx->fn.h2o2m4;
+    op.s43 = (float)(c4o3 * deltat);
+    op.c112 = (float)c112;
+    TRY(run_stencil(ctx, ctx->g2, hi_plane(ctx->psi), op));
+    std::swap(ctx->psi, ctx->psiold[ctx->ioldp[2] - 1]);
+    std::swap(ctx->ioldh[0], ctx->ioldh[1]);
+  } else {
     OpPredict op{};
     op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
     op.po3 = (double2*)ctx->psiold[ctx->ioldp[2] - 1];
@@ -2223,7 +2326,32 @@ int he_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errimp, doubl
     LAUNCHED();
   }
   TRY(field_eval(ctx));
-  {
+  if (ctx->mixed) {
+    void* a3 = ctx->psiold[ctx->ioldp[2] - 1];
+    void* a2 = ctx->psiold[ctx->ioldp[1] - 1];
+    OpCorrectM op{};
+    op.s8[0] = (const float*)ctx->pot4; op.s8[1] = (const float*)ctx->uimp;
+    op.s16[0] = lo_plane(ctx, ctx->psi);
+    op.s16[1] = hi_plane(a3); op.s16[2] = lo_plane(ctx, a3);
+    op.s16[3] = hi_plane(a2); op.s16[4] = lo_plane(ctx, a2);
+    op.s16[5] = (const float2*)ctx->hpsiold[ctx->ioldh[0] - 1];
+    op.s16[6] = (const float2*)ctx->hpsiold[ctx->ioldh[1] - 1];
+    op.s16[7] = (const float2*)ctx->pc;
+    op.pc = (float2*)ctx->pc;
+    op.out_hi = hi_plane(ctx->scratch); op.out_lo = lo_plane(ctx, ctx->scratch);
+    op.den = (float*)ctx->den;
+    op.tm = timec_view(ctx);
+    op.h2o2m = (float)ctx->fn.h2o2m4;
+    op.s3 = (float)(3.0 * deltat);
+    op.c9 = (float)c9;
+    op.c112 = (float)c112;
+    TRY(run_stencil_red(ctx, ctx->g2, hi_plane(ctx->psi), op, S_ERRHE));
+    std::swap(ctx->psi, ctx->scratch);
+    const int a = ctx->ioldp[2];
+    ctx->ioldp[2] = ctx->ioldp[1];
+    ctx->ioldp[1] = ctx->ioldp[0];
+    ctx->ioldp[0] = a;
+  } else {
     OpCorrect op{};
     op.s8[0] = ctx->pot4; op.s8[1] = ctx->uimp;
     op.s16[0] = (const double2*)ctx->psiold[ctx->ioldp[2] - 1];
@@ -2271,7 +2399,15 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
     if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
     return q_energy(ctx, out);
   }
-  if (ctx->mode == HE_MODE_DYNAMICS) {
+  if (ctx->mode == HE_MODE_DYNAMICS && ctx->mixed) {
+    OpEnergy<float2> op{};
+    op.s8[0] = (const float*)ctx->den; op.s8[1] = (const float*)ctx->dencg;
+    op.s8[2] = (const float*)ctx->delj4; op.s8[3] = (const float*)ctx->uimp;
+    op.has_u = 1;
+    op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
+    op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
+    TRY(run_stencil_red(ctx, ctx->g1, hi_plane(ctx->psi), op, S_EN));
+  } else if (ctx->mode == HE_MODE_DYNAMICS) {
     OpEnergy<double2> op{};
     op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->uimp;
     op.has_u = 1;
@@ -2660,11 +2796,19 @@ int he_observables(he_ctx_t* ctx, int npart, double* out) {
   if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode == HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "observables need a complex psi");
   if (npart <= 0) return fail(ctx, HE_ERR_ARG, "npart must be positive");
-  OpObservables op{};
-  op.s8[0] = ctx->den;
-  op.x0 = -ctx->xmax; op.y0 = -ctx->ymax; op.z0 = -ctx->zmax;
-  op.hx = ctx->hx; op.hy = ctx->hy; op.hz = ctx->hz;
-  TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_OBS));
+  if (ctx->mixed) {
+    OpObservablesT<float2> op{};
+    op.s8[0] = (const float*)ctx->den;
+    op.x0 = -ctx->xmax; op.y0 = -ctx->ymax; op.z0 = -ctx->zmax;
+    op.hx = ctx->hx; op.hy = ctx->hy; op.hz = ctx->hz;
+    TRY(run_stencil_red(ctx, ctx->g1, hi_plane(ctx->psi), op, S_OBS));
+  } else {
+    OpObservables op{};
+    op.s8[0] = ctx->den;
+    op.x0 = -ctx->xmax; op.y0 = -ctx->ymax; op.z0 = -ctx->zmax;
+    op.hx = ctx->hx; op.hy = ctx->hy; op.hz = ctx->hz;
+    TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_OBS));
+  }
   TRY(read_sums(ctx));
   const double* s = ctx->hsum + S_OBS;
   const double dxyz = ctx->dxyz;

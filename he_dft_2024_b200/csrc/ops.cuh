@@ -144,28 +144,157 @@ using OpPredictQ = OpPredictT<true>;
 using OpCorrectQ = OpCorrectT<true>;
 using OpRKQ = OpRKT<true>;
 
+// ---- the mixed path (HE_PREC_MIXED, classical dynamics) --------------------------------------
+// psi and its history psiold are compensated binary32 pairs held as two float2 planes of one
+// allocation (hi at [0, N), lo at [N, 2N)); the stencil differentiates the hi plane.  H psi, the
+// history terms hpsiold, pc, q and the fields den, pot4, uimp are binary32.  The updates of psi
+// (the RK-Gill stage, the Milne predictor, the Hamming corrector) are done on the pairs with
+// error-free transformations, so psi keeps about 48 significant bits over the run while every
+// stream but psi is half as wide as in binary64.
+struct HL2 {
+  HL x, y;
+};
+HE_D HL2 hl2(float2 hi, float2 lo) { return HL2{HL{hi.x, lo.x}, HL{hi.y, lo.y}}; }
+HE_D HL2 hl2_add(HL2 a, float2 b) { return HL2{hl_add(a.x, b.x), hl_add(a.y, b.y)}; }
+HE_D void hl2_store(float2* hi, float2* lo, long i, HL2 v) {
+  hi[i] = make_float2(v.x.hi, v.y.hi);
+  lo[i] = make_float2(v.x.lo, v.y.lo);
+}
+HE_D float den_of(HL2 v) {  // |psi|^2 of the pair, rounded once
+  const double re = hl_value(v.x), im = hl_value(v.y);
+  return (float)(re * re + im * im);
+}
+
+// H psi in binary32 (the binary64 hpsi_rt with float operands).
+HE_D float2 hpsi_rt_f(float2 dx, float2 dy, float2 dz, float2 c, float pot, float u, float tr,
+                      float h2o2m) {
+  const float lx = dx.x + dy.x + dz.x, ly = dx.y + dy.y + dz.y;
+  const float ax = lx * h2o2m - pot * c.x;
+  const float ay = ly * h2o2m - pot * c.y;
+  return make_float2(tr * ax - ay + u * c.y, tr * ay + ax - u * c.x);
+}
+
+// One RK-Gill stage (steprk.f90:67-79) on the pair planes.
+struct OpRKM {
+  static const char* kname() { return "hpsi_rkgill_stage_f32"; }
+  using T = float2;
+  static constexpr int NV = 0, N8 = 2, N16 = 2;
+  const float* s8[N8];       // pot4, uimp
+  const float2* s16[N16];    // q, psi lo plane
+  float2* q;
+  float2* out_hi;
+  float2* out_lo;
+  float2* hsave;
+  float* den;
+  Timec tm;
+  float h2o2m, a, b, cc, dt;
+  HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
+               const float* v8, const float2* v16, int vs, double*) const {
+    const float2 s4 = hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], (float)tm.re(ix, iy, iz), h2o2m);
+    const float2 qq = v16[0];
+    const float2 s1 = make_float2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
+    q[i] = make_float2(qq.x + 3.0f * s1.x - cc * s4.x, qq.y + 3.0f * s1.y - cc * s4.y);
+    if (hsave) hsave[i] = s4;
+    const HL2 pn = hl2_add(hl2(c, v16[vs]), make_float2(dt * s1.x, dt * s1.y));
+    hl2_store(out_hi, out_lo, i, pn);
+    den[i] = den_of(pn);
+  }
+};
+
+// steppc predictor + modifier (steppc.f90:51-61) on the pair planes: psi_pred = po3 +
+// (s43 (2 H psi - hh1 + 2 hh2) - c112 pc), written over po3.  pc is not overwritten with the
+// unmodified prediction sto1 (a full-size value the binary32 pc could not hold); the corrector
+// rebuilds sto1 = psi_pred + c112 pc from the predicted pair instead.
+struct OpPredictM {
+  static const char* kname() { return "hpsi_pmc_predict_f32"; }
+  using T = float2;
+  static constexpr int NV = 0, N8 = 2, N16 = 5;
+  const float* s8[N8];       // pot4, uimp
+  const float2* s16[N16];    // po3 hi, po3 lo, hpsiold(ioldh(1)), hpsiold(ioldh(2)), pc
+  float2* po3_hi;
+  float2* po3_lo;
+  float2* h2;
+  float* den;
+  Timec tm;
+  float h2o2m, s43, c112;
+  HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
+               const float* v8, const float2* v16, int vs, double*) const {
+    const float2 s4 = hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], (float)tm.re(ix, iy, iz), h2o2m);
+    const float2 hh1 = v16[2 * vs], hh2 = v16[3 * vs], pcv = v16[4 * vs];
+    const float2 t = make_float2(2.0f * s4.x - hh1.x + 2.0f * hh2.x, 2.0f * s4.y - hh1.y + 2.0f * hh2.y);
+    const float2 d = make_float2(s43 * t.x - c112 * pcv.x, s43 * t.y - c112 * pcv.y);
+    const HL2 pn = hl2_add(hl2(v16[0], v16[vs]), d);
+    h2[i] = s4;
+    hl2_store(po3_hi, po3_lo, i, pn);
+    den[i] = den_of(pn);
+  }
+};
+
+// steppc corrector + final value (steppc.f90:118-127) on the pair planes; accumulates sum |pc|.
+//   s5 = (9 a3 - a2 + s3 (H psi_pred + 2 b1 - b2)) / 8          (pairs)
+//   pc = sto1 - s5 = (psi_pred - s5) + c112 pc_old              (a small difference, binary32)
+//   psi = s5 + c9 pc                                            (pair)
+struct OpCorrectM {
+  static const char* kname() { return "hpsi_pmc_correct_f32"; }
+  using T = float2;
+  static constexpr int NV = 1, N8 = 2, N16 = 8;
+  const float* s8[N8];       // pot4, uimp
+  const float2* s16[N16];    // psi_pred lo, a3 hi, a3 lo, a2 hi, a2 lo, hpsiold(ioldh(1)),
+                             // hpsiold(ioldh(2)), pc
+  float2* pc;
+  float2* out_hi;
+  float2* out_lo;
+  float* den;
+  Timec tm;
+  float h2o2m, s3, c9, c112;
+  HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
+               const float* v8, const float2* v16, int vs, double* acc) const {
+    const float2 s4 = hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], (float)tm.re(ix, iy, iz), h2o2m);
+    const HL2 pred = hl2(c, v16[0]);
+    const HL2 a3 = hl2(v16[vs], v16[2 * vs]), a2 = hl2(v16[3 * vs], v16[4 * vs]);
+    const float2 b1 = v16[5 * vs], b2 = v16[6 * vs], pco = v16[7 * vs];
+    const float2 inner = make_float2(s3 * (s4.x + 2.0f * b1.x - b2.x), s3 * (s4.y + 2.0f * b1.y - b2.y));
+    HL s5x = hl_add(hl_add(hl_mul(9.0f, a3.x), hl_neg(a2.x)), inner.x);
+    HL s5y = hl_add(hl_add(hl_mul(9.0f, a3.y), hl_neg(a2.y)), inner.y);
+    s5x = HL{0.125f * s5x.hi, 0.125f * s5x.lo};
+    s5y = HL{0.125f * s5y.hi, 0.125f * s5y.lo};
+    const HL dx_ = hl_add(pred.x, hl_neg(s5x)), dy_ = hl_add(pred.y, hl_neg(s5y));
+    const float2 pn = make_float2((dx_.hi + dx_.lo) + c112 * pco.x, (dy_.hi + dy_.lo) + c112 * pco.y);
+    pc[i] = pn;
+    const HL2 o = HL2{hl_add(s5x, c9 * pn.x), hl_add(s5y, c9 * pn.y)};
+    hl2_store(out_hi, out_lo, i, o);
+    den[i] = den_of(o);
+    acc[0] += hypot((double)pn.x, (double)pn.y);
+  }
+};
+
 // energy(): Dynamics_TDDFT/energy.f90:107-165 sums (first derivatives of psi).
 //   acc = {sum |grad psi|^2, sum delj4*den, sum den*dencg^2*(cp4/2+cpp4/3*dencg),
 //          sum den*(1+tanh(beta*(den-den_m))), sum uimp*den}
+// TT = float2 (the mixed path): gradients of the binary32 psi planes, the sums in binary64.
 template <typename TT>
 struct OpEnergy {
-  static const char* kname() { return "energy_reduce"; }
+  static const char* kname() { return sizeof(TT) == 8 ? "energy_reduce_f32" : "energy_reduce"; }
   using T = TT;
+  using R = typename RealOf<TT>::R;
+  using Z = typename RealOf<TT>::Z;
   static constexpr int NV = 5, N8 = 4, N16 = 0;
-  const double* s8[N8];      // den, dencg, delj4, uimp (den again when there is no uimp)
-  const double2* s16[1];
+  const R* s8[N8];           // den, dencg, delj4, uimp (den again when there is no uimp)
+  const Z* s16[1];
   double aux1, aux2, beta, den_m;
   int lsolid, has_u;
   HE_D static double n2(double v) { return v * v; }
   HE_D static double n2(double2 v) { return v.x * v.x + v.y * v.y; }
-  HE_D void at(int, int, int, long, T dx, T dy, T dz, T, const double* v8, const double2*, int vs,
+  HE_D static double n2(float v) { return (double)v * (double)v; }
+  HE_D static double n2(float2 v) { return (double)v.x * (double)v.x + (double)v.y * (double)v.y; }
+  HE_D void at(int, int, int, long, T dx, T dy, T dz, T, const R* v8, const Z*, int vs,
                double* acc) const {
     const double a3 = v8[0], a4 = v8[vs];
     acc[0] += n2(dx) + n2(dy) + n2(dz);
-    acc[1] += v8[2 * vs] * a3;
+    acc[1] += (double)v8[2 * vs] * a3;
     acc[2] += a3 * a4 * a4 * (aux1 + aux2 * a4);
     if (lsolid) acc[3] += a3 * (1.0 + tanh(beta * (a3 - den_m)));
-    if (has_u) acc[4] += v8[3 * vs] * a3;
+    if (has_u) acc[4] += (double)v8[3 * vs] * a3;
   }
 };
 
@@ -175,19 +304,24 @@ struct OpEnergy {
 //   [3..8]  Im sum y c_x, x c_y, x c_z, z c_x, z c_y, y c_z   (<L> about the origin; the
 //           shift to the centre of mass uses [0..2] on the host)
 //   [9..15] sum den, den x, den y, den z, den x^2, den y^2, den z^2     (N, r_cm, <r^2>)
-struct OpObservables {
-  static const char* kname() { return "observables_reduce"; }
-  using T = double2;
+// TT = float2: the mixed path's binary32 psi planes (products and sums in binary64).
+template <typename TT>
+struct OpObservablesT {
+  static const char* kname() { return sizeof(TT) == 8 ? "observables_reduce_f32" : "observables_reduce"; }
+  using T = TT;
+  using R = typename RealOf<TT>::R;
+  using Z = typename RealOf<TT>::Z;
   static constexpr int NV = 16, N8 = 1, N16 = 0;
-  const double* s8[N8];      // den
-  const double2* s16[1];
+  const R* s8[N8];           // den
+  const Z* s16[1];
   double x0, y0, z0, hx, hy, hz;
-  HE_D void at(int ix, int iy, int iz, long, double2 dx, double2 dy, double2 dz, double2 c,
-               const double* v8, const double2*, int, double* acc) const {
+  HE_D void at(int ix, int iy, int iz, long, T dx, T dy, T dz, T c, const R* v8, const Z*, int,
+               double* acc) const {
     const double x = x0 + hx * ix, y = y0 + hy * iy, z = z0 + hz * iz;
-    const double cx = c.x * dx.y - c.y * dx.x;  // Im conj(psi) d_x psi
-    const double cy = c.x * dy.y - c.y * dy.x;
-    const double cz = c.x * dz.y - c.y * dz.x;
+    const double cr = c.x, ci = c.y;
+    const double cx = cr * (double)dx.y - ci * (double)dx.x;  // Im conj(psi) d_x psi
+    const double cy = cr * (double)dy.y - ci * (double)dy.x;
+    const double cz = cr * (double)dz.y - ci * (double)dz.x;
     acc[0] += cx;
     acc[1] += cy;
     acc[2] += cz;
@@ -207,6 +341,7 @@ struct OpObservables {
     acc[15] += d * (z * z);
   }
 };
+using OpObservables = OpObservablesT<double2>;
 
 // derden(): dxden, dyden, dzden (derden.f90:26-28).
 struct OpDerden {
@@ -253,22 +388,23 @@ struct ImpDev {
 // up to an integer k although the exact quotient is below k, the reference takes bin k with a
 // fraction of ~1 (it interpolates one bin further out), and so does this kernel.  The remainder
 // r - i0*DelInter is one exact fma when i0 is the exact floor, else r - (i0-1)*DelInter.
-template <int NI>
+// TT = float: the mixed path (binary32 den and uimp; positions, table and sums in binary64).
+template <int NI, typename TT = double>
 struct OpImpField {
-  static const char* kname() { return "impurity_field_force"; }
-  using T = double;
+  static const char* kname() { return sizeof(TT) == 4 ? "impurity_field_force_f32" : "impurity_field_force"; }
+  using T = TT;
   static constexpr int NV = 3 * NI;
   const double* tab;  // (npot) per impurity, impurity-major
   ImpDev* imp;
-  double* uimp;
+  TT* uimp;
   int n, npot;
   double delinter, rmax;
   double xmax, ymax, zmax, hx, hy, hz;
   static constexpr int N8 = 0, N16 = 0;
-  const double* s8[1];
-  const double2* s16[1];
-  HE_D void at(int ix, int iy, int iz, long i, double dx, double dy, double dz, double,
-               const double*, const double2*, int, double* acc) const {
+  const TT* s8[1];
+  const typename RealOf<TT>::Z* s16[1];
+  HE_D void at(int ix, int iy, int iz, long i, TT dx, TT dy, TT dz, TT, const TT*,
+               const typename RealOf<TT>::Z*, int, double* acc) const {
     const double x = -xmax + hx * ix, y = -ymax + hy * iy, z = -zmax + hz * iz;
     const double* __restrict__ rp = imp->rimp;
     double u = 0.0;
@@ -292,12 +428,12 @@ struct OpImpField {
         const double* __restrict__ t = tab + (long)k * npot;
         const double uk = __ldg(t + i0) * (1.0 - rmod) + __ldg(t + i0 + 1) * rmod;
         u = u + uk;
-        acc[3 * k + 0] += dx * uk;
-        acc[3 * k + 1] += dy * uk;
-        acc[3 * k + 2] += dz * uk;
+        acc[3 * k + 0] += (double)dx * uk;
+        acc[3 * k + 1] += (double)dy * uk;
+        acc[3 * k + 2] += (double)dz * uk;
       }
     }
-    uimp[i] = u;
+    uimp[i] = (TT)u;
   }
 };
 

@@ -29,7 +29,15 @@ struct StencilGeom {
   int icon;          // 13, 8, 18 or 24
   int axis_on[3];    // 0 when n(axis) < npd
   double w[3][13];   // scaled weights per axis
+  float wf[3][13];   // the same in binary32 (stencils over binary32 fields)
 };
+
+// The weights of a field type: binary32 fields use wf.
+template <typename T>
+HE_D const auto& stencil_w(const StencilGeom& g) {
+  if constexpr (sizeof(typename RealOf<T>::R) == 4) return g.wf;
+  else return g.w;
+}
 
 // icon=24 (redef.f:245-279, then ICON=4 at :18-56): the boundary rows fold the centred row
 // onto the grid as an even reflection about the first and last points, f(1-m) = f(1+m) and
@@ -80,8 +88,12 @@ HE_D void cp_async_elem(T* dst_smem, const T* src, bool valid) {
   if constexpr (sizeof(T) == 16) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src),
                  "r"(nbytes));
-  } else {
+  } else if constexpr (sizeof(T) == 8) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src),
+                 "r"(nbytes));
+  } else {
+    static_assert(sizeof(T) == 4, "cp.async copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src),
                  "r"(nbytes));
   }
 }
@@ -121,12 +133,13 @@ __device__ void reduce_tail(const ReduceTail& rt, long nb) {
 }
 
 // Op interface:
-//   using T;                      field element type (double or double2)
+//   using T;                      field element type (double, double2, float or float2)
 //   static constexpr int NV;      number of FP64 block reductions (0 = none)
 //   static constexpr int N8, N16; number of real / complex pointwise operand fields
-//   const double* s8[N8]; const double2* s16[N16];  the operand fields (set by the host)
-//   HE_D void at(int ix,int iy,int iz,long idx,T dx,T dy,T dz,T c,const double* v8,
-//                const double2* v16,int vs,double* acc) const;
+//   const R* s8[N8]; const Z* s16[N16];  the operand fields (set by the host), R and Z the real
+//                                        and complex types of T's precision (RealOf<T>)
+//   HE_D void at(int ix,int iy,int iz,long idx,T dx,T dy,T dz,T c,const R* v8,
+//                const Z* v16,int vs,double* acc) const;
 //   where v8[k*vs] and v16[k*vs] are this point's operands of field k (staged in shared memory).
 // Minimum resident CTAs per SM for a stencil instantiation (caps registers at 64K/(256*m)).
 template <typename T>
@@ -138,8 +151,10 @@ constexpr int stencil_min_blocks() {
 // double-buffered operand stages.
 template <class Op, int TX, int TY>
 HE_HD constexpr size_t stencil_smem() {
+  using RT = RealOf<typename Op::T>;
   return 2 * (size_t)(TY + 12) * (TX + 12) * sizeof(typename Op::T) +
-         2 * (size_t)Op::N16 * TX * TY * sizeof(double2) + 2 * (size_t)Op::N8 * TX * TY * sizeof(double);
+         2 * (size_t)Op::N16 * TX * TY * sizeof(typename RT::Z) +
+         2 * (size_t)Op::N8 * TX * TY * sizeof(typename RT::R);
 }
 
 template <class Op, int TX, int TY>
@@ -147,6 +162,8 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<typename Op::T>())
     k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
               const ReduceTail rt) {
   using T = typename Op::T;
+  using R = typename RealOf<T>::R;
+  using Z = typename RealOf<T>::Z;
   constexpr int NT = TX * TY;
   constexpr int NH = 12 * (TX + TY);       // halo elements per plane
   constexpr int HK = (NH + NT - 1) / NT;   // halo elements per thread
@@ -154,8 +171,8 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<typename Op::T>())
   constexpr int TILE = (TY + 12) * (TX + 12);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tiles = reinterpret_cast<T*>(smem_raw);                                     // [2][TILE]
-  double2* st16 = reinterpret_cast<double2*>(smem_raw + 2 * TILE * sizeof(T));  // [2][N16][NT]
-  double* st8 = reinterpret_cast<double*>(st16 + 2 * Op::N16 * NT);             // [2][N8][NT]
+  Z* st16 = reinterpret_cast<Z*>(smem_raw + 2 * TILE * sizeof(T));  // [2][N16][NT]
+  R* st8 = reinterpret_cast<R*>(st16 + 2 * Op::N16 * NT);           // [2][N8][NT]
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + TX * ty;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -273,18 +290,19 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<typename Op::T>())
     fix_halo_sign(b, iz);
     __syncthreads();
     if (inside) {
+      const auto& W = stencil_w<T>(g);
       T dx = zero_of(T()), dy = zero_of(T()), dz = zero_of(T());
       if (g.axis_on[0]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dx = axpy(g.w[0][m], tb[(ty + 6) * (TX + 12) + tx + m], dx);
+        for (int m = 0; m < 13; ++m) dx = axpy(W[0][m], tb[(ty + 6) * (TX + 12) + tx + m], dx);
       }
       if (g.axis_on[1]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dy = axpy(g.w[1][m], tb[(ty + m) * (TX + 12) + tx + 6], dy);
+        for (int m = 0; m < 13; ++m) dy = axpy(W[1][m], tb[(ty + m) * (TX + 12) + tx + 6], dy);
       }
       if (g.axis_on[2]) {
 #pragma unroll
-        for (int m = 0; m < 13; ++m) dz = axpy(g.w[2][m], q[m], dz);
+        for (int m = 0; m < 13; ++m) dz = axpy(W[2][m], q[m], dz);
       }
       op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
             st16 + b * Op::N16 * NT + tid, NT, acc);

@@ -39,10 +39,13 @@ typedef struct he_ctx he_ctx_t;
  * complex psi plus impurity wave functions psix_i (he_set_quantum_impurities). */
 enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1, HE_MODE_QUANTUM = 2 };
 /* HE_PREC_F64: binary64 throughout.  HE_PREC_MIXED (HE_MODE_DYNAMICS, OT/OP cores): the FFT chain
- * of the mean field (poten's convolutions) runs in binary32 on binary32 copies of the k-space
- * kernels, with binary64 inputs and outputs (den in; dencg, delj4, pot4 out); the wave function,
- * its history, the stencils, the impurity field and every reduction stay binary64.  fden is then
- * held as binary32 (downloads convert; uploads are refused). */
+ * of the mean field, the 13-point stencils and H psi run in binary32; den, pot4, dencg, delj4,
+ * uimp, fden, pc, q and hpsiold are held in binary32; psi and psiold are held as compensated
+ * binary32 pairs (about 48 significant bits) and updated with error-free transformations; the
+ * reductions (energy, errHe, impurity forces) and the impurity's Newton integration stay binary64.
+ * he_upload / he_download convert (host arrays are binary64 in every mode).  Between the
+ * predictor and the corrector of he_steppc, pc keeps the corrector's value instead of the
+ * unmodified prediction. */
 enum he_precision { HE_PREC_F64 = 0, HE_PREC_MIXED = 1 };
 
 /* Grid: Dynamics_TDDFT/modules.f90:88-105 (grid), deriva npd/icon :31-37.  h = 2*xmax/n and

@@ -1,5 +1,6 @@
-"""The mixed-precision path (HE_PREC_MIXED: the mean field's FFT chain in binary32, wave function,
-stencils and reductions in binary64) against the binary64 path on the same inputs.
+"""The mixed-precision path (HE_PREC_MIXED) against the binary64 path on the same inputs: the
+mean field's FFT chain, the stencils and H psi in binary32; psi and its history as compensated
+binary32 pairs; reductions and the impurity's Newton integration in binary64.
 
 Accuracy bar: the metric's |delta E/N| < 1e-5 K between the mixed and the FP64 runs of the
 classical-impurity workload, checked here over 200 driver iterations at 64^3 (and fields after one
@@ -70,3 +71,27 @@ def test_mixed_rejects_unsupported_modes():
         Context(w, mode="statics", precision="mixed")
     with pytest.raises(HeError):
         Context(C.replace(w, core="OTC", lsolid=0), precision="mixed")
+
+
+def test_mixed_field_formats_round_trip():
+    """psi is held as a compensated pair (about 48 bits), pc as binary32, den as binary32; the
+    host side is binary64 either way."""
+    w = workload(32)
+    rng = np.random.default_rng(5)
+    shape = (w.nx, w.ny, w.nz)
+    z = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    r = rng.random(shape)
+    with Context(w, precision="mixed") as ctx:
+        for name in ("psi", "psiold2"):
+            ctx.upload(name, z)
+            back = ctx.download(name)
+            err = np.max(np.abs(back - z)) / np.max(np.abs(z))
+            assert 0 < err < 2.0 ** -45, (name, err)
+        for name in ("pc", "hpsiold1"):
+            ctx.upload(name, z)
+            back = ctx.download(name)
+            assert np.array_equal(back, z.astype(np.complex64).astype(np.complex128)), name
+        for name in ("den", "pot4"):
+            ctx.upload(name, r)
+            back = ctx.download(name)
+            assert np.array_equal(back, r.astype(np.float32).astype(np.float64)), name
