@@ -38,9 +38,10 @@ sys.path.insert(0, ROOT)
 METRIC = "TDDFT grid-pt-steps/s (FP64, 128^3 classical-impurity steppc loop)"
 
 
-def metric_for(w):
-    """The metric line of a classical workload (METRIC for the default 128^3 one)."""
-    return f"TDDFT grid-pt-steps/s (FP64, {w.nx}^3 classical-impurity steppc loop)"
+def metric_for(w, precision="f64"):
+    """The metric line of a classical workload (METRIC for the default 128^3 FP64 one)."""
+    p = "FP64" if precision == "f64" else "mixed"
+    return f"TDDFT grid-pt-steps/s ({p}, {w.nx}^3 classical-impurity steppc loop)"
 METRIC_Q = "TDDFT grid-pt-steps/s (FP64, 192^3 quantum impurity, batch of trajectories)"
 REF_MAX_STEPS = 40
 UNIT = "grid-pt-steps/s"
@@ -48,8 +49,31 @@ UNIT = "grid-pt-steps/s"
 # Algorithmic bytes per grid point of each kernel (binary64; N-sized field = 8 B real / 16 B
 # complex per point, half spectrum = (nx/2+1)/nx of that): reads + writes of the arrays the
 # kernel's reference counterpart consumes and produces.
-def kernel_bytes_per_point(nx):
+STEP_BYTES_PER_POINT = {"f64": 744.0, "mixed": 404.0}
+
+
+def kernel_bytes_per_point(nx, mixed=False):
+    """Algorithmic bytes per grid point of each kernel (each input read once, each output written
+    once).  mixed: binary32 fields (4 B real, 8 B complex) and psi / psiold as pairs (16 B)."""
     hk = (nx // 2 + 1) / nx  # half-spectrum fraction
+    if mixed:
+        c, r = 8.0, 4.0
+        return {
+            # psi hi, pot4, uimp, po3 pair, hpsiold x2, pc -> po3 pair, hpsiold, den
+            "hpsi_pmc_predict_f32": (c + r + r + 16 + 2 * c + c) + (16 + c + r),
+            # psi pair, pot4, uimp, psiold pairs x2, hpsiold x2, pc -> psi pair, pc, den
+            "hpsi_pmc_correct_f32": (16 + r + r + 2 * 16 + 2 * c + c) + (16 + c + r),
+            # psi pair, pot4, uimp, q -> q, psi pair, den (+ hpsiold on stage 1)
+            "hpsi_rkgill_stage_f32": (16 + r + r + c) + (c + 16 + r),
+            "impurity_field_force_f32": r + r,
+            "energy_reduce_f32": c + 4 * r,
+            "fft_x_r2c_den": r + c * hk,
+            "fft_x_c2r_cg_lj_r2c_corr": 2 * c * hk + r + 2 * r + c * hk,
+            "fft_x_c2r_pot4": c * hk + 3 * r + r,
+            "fft_y": 2 * c * hk,
+            "fft_z_conv1": 2 * c * hk + r * hk,
+            "fft_z_conv2": c * hk + 3 * c * hk + 2 * r * hk,
+        }
     c, r = 16.0, 8.0
     return {
         # psi, pot4, uimp, psiold(ioldp3), hpsiold x2, pc -> psi_new, pc, hpsiold, den
@@ -252,7 +276,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     w = build_workload(args)
     N = w.n
-    ctx = Context(w)
+    ctx = Context(w, precision=args.precision)
+    mixed_main = args.precision == "mixed"
     # A dedicated (non-default) stream: the library's kernels and the timing events share it.
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -280,14 +305,15 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launches - launches0
     t_max = reduce_max(ms / 1e3, ws)
-    if args.mixed_compare:
+    compare = args.mixed_compare and not mixed_main
+    if compare:
         # both trajectories are compared after COMPARE_STEPS driver iterations
         it = advance_to(ctx, w, it, COMPARE_STEPS)
         ref = trajectory_summary(ctx, w)
 
     # ---- the mixed-precision path on the same trajectory (same steps from the same state) ----
     mixed = None
-    if args.mixed_compare:
+    if compare:
         cm = Context(w, precision="mixed")
         cm.set_stream(stream.cuda_stream)
         prepare_state(cm, w)
@@ -306,6 +332,19 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier(ws)
         tm = reduce_max(m0.elapsed_time(m1) / 1e3, ws)
+        # per-kernel breakdown of the mixed step (short event-timed run)
+        cm.timing(True)
+        for _ in range(max(3, min(args.steps, 10))):
+            device_iteration(cm, w, itm)
+            itm += 1
+        mrep = cm.timing_report()
+        mtune = cm.autotune_report().strip().splitlines()
+        cm.timing(False)
+        mtot = sum(v[1] for v in mrep.values())
+        mbpp = kernel_bytes_per_point(w.nx, mixed=True)
+        mkern = {k: {"launches": v[0], "ms_per_launch": v[1] / v[0], "share": v[1] / mtot,
+                     "GB/s": (mbpp[k] * N / (v[1] / v[0] / 1e3) / 1e9) if k in mbpp else None}
+                 for k, v in sorted(mrep.items(), key=lambda kv: -kv[1][1])}
         itm = advance_to(cm, w, itm, COMPARE_STEPS)
         got = trajectory_summary(cm, w)
         cm.close()
@@ -316,6 +355,10 @@ def run_ours(args):
                  "rel_d_rho_L2": abs(got["rho_L2"] - ref["rho_L2"]) / ref["rho_L2"],
                  "abs_d_z_imp_A": abs(got["z_imp"] - ref["z_imp"]) if w.n_imp else None,
                  "steps_compared": itm - 1,
+                 "step_alg_bytes_per_point": STEP_BYTES_PER_POINT["mixed"],
+                 "step_roofline_frac": STEP_BYTES_PER_POINT["mixed"] * N / (tm / args.steps)
+                 / 1e9 / measured_peak()[0],
+                 "kernels": mkern, "fft_autotune": mtune,
                  "note": "HE_PREC_MIXED: FFT chain, stencils and H psi in binary32, psi and psiold "
                          "as compensated binary32 pairs, reductions and impurity integration in "
                          "binary64; compared with the binary64 run of the same workload"}
@@ -346,7 +389,8 @@ def run_ours(args):
     ctx.timing(False)
     tot = sum(v[1] for v in rep.values())
     tiles = ctx.tuned_tiles()
-    bpp = kernel_bytes_per_point(w.nx)
+    tune = ctx.autotune_report().strip().splitlines()
+    bpp = kernel_bytes_per_point(w.nx, mixed=mixed_main)
     top = max(rep.items(), key=lambda kv: kv[1][1])
     name, (nl, kms) = top
     peak, peak_kind = measured_peak()
@@ -364,9 +408,11 @@ def run_ours(args):
             traffic = None
 
     line = {
-        "metric": metric_for(w), "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "metric": metric_for(w, args.precision), "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f32x2" if mixed_main else "f64", "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "h_A": w.h[0], "n4": w.n4,
                    "n_imp": w.n_imp, "deltat_ps": w.deltatps, "parallelism": f"replicas{ws}",
                    "l2": f"per-step working set {ctx.device_bytes / 1e9:.2f} GB > 126 MB L2 (no flush)"},
@@ -377,9 +423,11 @@ def run_ours(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "alg_bytes_per_launch": alg,
                      "ms_per_launch": kms / nl},
-        "step_alg_bytes_per_point": 744.0,
-        "step_roofline_frac": (744.0 * N * args.steps / (t_max / ws)) / 1e9 / peak,
+        "step_alg_bytes_per_point": STEP_BYTES_PER_POINT[args.precision],
+        # per GPU: each rank moves the step's bytes of its own trajectory
+        "step_roofline_frac": (STEP_BYTES_PER_POINT[args.precision] * N * args.steps / t_max) / 1e9 / peak,
         "kernels": breakdown,
+        "fft_autotune": tune,
         "fft_tiles_xyz": list(tiles),
         "mixed": mixed,
         "clocks": clk.summary(),
@@ -616,6 +664,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", dest="mixed_compare", action="store_false",
                     help="skip the mixed-precision comparison run")
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
+                    help="precision of the timed classical line (mixed: HE_PREC_MIXED; the "
+                         "mixed-vs-FP64 comparison then runs only with the default f64)")
     ap.add_argument("--workload", default="classical", choices=["classical", "quantum", "serving"])
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--requests", type=int, default=128)

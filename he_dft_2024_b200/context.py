@@ -96,6 +96,12 @@ class Context:
         self._ck(self.L.he_tuned_tiles(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
+    def autotune_report(self):
+        """The FFT autotuner's trial times, one line per variant, and the x-pass variant chosen."""
+        buf = ctypes.create_string_buffer(4096)
+        self._ck(self.L.he_autotune_report(self.h, buf, len(buf)))
+        return buf.value.decode()
+
     def synchronize(self):
         self._ck(self.L.he_synchronize(self.h))
 

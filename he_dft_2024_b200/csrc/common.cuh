@@ -120,6 +120,40 @@ HE_HD HL hl_from(double v) {
 }
 HE_HD double hl_value(HL a) { return (double)a.hi + (double)a.lo; }
 
+// Asynchronous global -> shared copy of one element (cp.async, zero fill when src_bytes = 0).
+template <typename T>
+HE_D void cp_async_elem(T* dst_smem, const T* src, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_smem);
+  const int nbytes = valid ? (int)sizeof(T) : 0;
+  if constexpr (sizeof(T) == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src),
+                 "r"(nbytes));
+  } else if constexpr (sizeof(T) == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src),
+                 "r"(nbytes));
+  } else {
+    static_assert(sizeof(T) == 4, "cp.async copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src),
+                 "r"(nbytes));
+  }
+}
+HE_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+HE_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// 16 bytes global -> shared (both addresses 16-byte aligned).
+HE_D void cp_async16(void* dst_smem, const void* src) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src));
+}
+// A contiguous byte range global -> shared in 16-byte pieces spread over the CTA's threads
+// (bytes a multiple of 16, both ends 16-byte aligned).
+HE_D void cp_async_range(void* dst_smem, const void* src, long bytes, int tid, int nthr) {
+  char* d = static_cast<char*>(dst_smem);
+  const char* g = static_cast<const char*>(src);
+  for (long o = 16L * tid; o < bytes; o += 16L * nthr) cp_async16(d + o, g + o);
+}
+
 // ---- block reduction of NV doubles (fixed order => deterministic) ------------------------------
 template <int NV>
 __device__ void block_reduce_store(double (&v)[NV], double* __restrict__ out) {

@@ -94,11 +94,183 @@ HE_D C* smem_as() {
   return reinterpret_cast<C*>(he_smem_raw);
 }
 
+// Inputs of one row tile that the x pass stages in shared memory: the spectrum rows of the C2R
+// modes and the real rows of the R2C prologue / C2R epilogue (the quantum extras are read
+// directly).
+template <int MODE>
+struct XStage {
+  static constexpr int nspec = (MODE == X_C2R2 || MODE == X_C2R2_CORR) ? 2
+                               : (MODE == X_C2R_POT || MODE == X_C2R1) ? 1 : 0;
+  static constexpr int nreal = (MODE == X_R2C_DEN || MODE == X_C2R2_CORR) ? 1
+                               : MODE == X_R2C_CORR ? 2 : MODE == X_C2R_POT ? 3 : 0;
+};
+// Bytes of one staged tile of RB rows (a multiple of 16).
+template <int MODE, typename Rt>
+HE_HD size_t xstage_bytes(int rb, int n) {
+  return (size_t)XStage<MODE>::nspec * rb * (n / 2 + 1) * sizeof(typename Cx<Rt>::T) +
+         (size_t)XStage<MODE>::nreal * rb * n * sizeof(Rt);
+}
+// Dynamic shared memory of an x-pass CTA: twiddles, two line buffers, two staged tiles.
+template <int MODE, typename Rt>
+HE_HD size_t xpass_smem(int stw_len, int rb, int n) {
+  using C = typename Cx<Rt>::T;
+  return sizeof(C) * (((size_t)stw_len + 1) / 2 * 2 + 2 * (size_t)rb * line_stride(n)) +
+         2 * xstage_bytes<MODE, Rt>(rb, n);
+}
+
 // Rt = double: the binary64 chain; Rt = float: the mixed path, spectra, transforms and the
 // real-space fields (den, dencg, delj4, pot4) in binary32, the pointwise prologue and epilogue
 // arithmetic in binary64.
+//
+// Persistent and software-pipelined: CTA b transforms row tiles b, b + G, b + 2G, ... (G CTAs);
+// while it transforms one tile, the inputs of its next tile are already in flight (cp.async of the
+// tile's contiguous row ranges into the other stage buffer), so the load latency that bounds a
+// load-transform-store CTA is hidden behind the transform.
+constexpr int kXPipeThreads = 256;  // threads of a pipelined x-pass CTA, whatever its rows
 template <int MODE, int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
+__global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a) {
+  using C = typename Cx<Rt>::T;
+  using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
+  using ST = XStage<MODE>;
+  const Rs* extra = reinterpret_cast<const Rs*>(a.extra);
+  const Rs* extra2 = reinterpret_cast<const Rs*>(a.extra2);
+  Rs* out1 = reinterpret_cast<Rs*>(a.out1);
+  Rs* out2 = reinterpret_cast<Rs*>(a.out2);
+  C* smem = smem_as<C>();
+  C* specA = reinterpret_cast<C*>(a.specA);
+  const C* specB = reinterpret_cast<const C*>(a.specB);
+  const int n = (N > 0) ? N : a.nx;
+  const int nxh = n / 2 + 1;
+  const int ls = line_stride(n);
+  const int RB = (N > 0) ? TILE : a.rb;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const long ntiles = a.rows / RB;
+  C* tw = smem;
+  C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  C* P1 = P0 + RB * ls;
+  unsigned char* stage0 = reinterpret_cast<unsigned char*>(P1 + RB * ls);
+  const size_t sbytes = xstage_bytes<MODE, Rt>(RB, n);
+  const size_t spec_bytes = (size_t)RB * nxh * sizeof(C), real_bytes = (size_t)RB * n * sizeof(Rs);
+  // real arrays staged per mode (prologue or epilogue inputs)
+  const void* rsrc[3] = {nullptr, nullptr, nullptr};
+  if constexpr (MODE == X_R2C_DEN || MODE == X_C2R2_CORR) rsrc[0] = a.den;
+  if constexpr (MODE == X_R2C_CORR) { rsrc[0] = a.den; rsrc[1] = a.dencg_in; }
+  if constexpr (MODE == X_C2R_POT) { rsrc[0] = a.dencg_in; rsrc[1] = a.delj4_in; rsrc[2] = a.den; }
+  const int nreal = (MODE == X_C2R_POT && !a.lsolid) ? 2 : ST::nreal;  // den: penalty only
+  auto issue = [&](int buf, long t) {
+    unsigned char* st = stage0 + buf * sbytes;
+    const long r0 = t * RB;
+    if constexpr (ST::nspec >= 1) cp_async_range(st, specA + r0 * nxh, spec_bytes, tid, nthr);
+    if constexpr (ST::nspec >= 2) cp_async_range(st + spec_bytes, specB + r0 * nxh, spec_bytes, tid, nthr);
+#pragma unroll
+    for (int k = 0; k < ST::nreal; ++k)
+      if (k < nreal)
+        cp_async_range(st + ST::nspec * spec_bytes + k * real_bytes,
+                     static_cast<const Rs*>(rsrc[k]) + r0 * n, real_bytes, tid, nthr);
+  };
+  load_twiddles(tw, a.pl);
+
+  long t = blockIdx.x;
+  int buf = 0;
+  if (t < ntiles) issue(0, t);
+  cp_async_commit();
+  for (; t < ntiles; t += gridDim.x, buf ^= 1) {
+    if (t + gridDim.x < ntiles) issue(buf ^ 1, t + gridDim.x);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const unsigned char* st = stage0 + buf * sbytes;
+    const C* sA = reinterpret_cast<const C*>(st);
+    const C* sB = reinterpret_cast<const C*>(st + spec_bytes);
+    const Rs* sR0 = reinterpret_cast<const Rs*>(st + ST::nspec * spec_bytes);
+    const Rs* sR1 = sR0 + RB * n;
+    const Rs* sR2 = sR1 + RB * n;
+    const long r0 = t * RB;
+
+    if constexpr (MODE == X_R2C_DEN || MODE == X_R2C_CORR) {
+      for (int e = tid; e < RB * n; e += nthr) {
+        const int row = e / n, x = e - row * n;
+        double v = sR0[e];
+        if constexpr (MODE == X_R2C_CORR) v = corr_source(v, sR1[e], a.cp4, a.cpp4);
+        reinterpret_cast<Rt*>(&P0[(row >> 1) * ls + sw<N>(x)])[row & 1] = Rt(v);
+      }
+      __syncthreads();
+      C* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, false);
+      for (int e = tid; e < RB * nxh; e += nthr) {
+        const int row = e / nxh, k = e - row * nxh;
+        specA[(r0 + row) * nxh + k] = split_r2c<N>(R + (row >> 1) * ls, k, n, row & 1);
+      }
+    }
+
+    if constexpr (MODE == X_C2R2 || MODE == X_C2R2_CORR) {
+      for (int e = tid; e < RB * n; e += nthr) {
+        const int row = e / n, k = e - row * n;
+        P0[row * ls + sw<N>(k)] = packed_c2r(sA + row * nxh, sB + row * nxh, k, n);
+      }
+      __syncthreads();
+      C* R = fft_lines<N>(P0, P1, RB, ls, a.pl, tw, true);
+      C* O = (R == P0) ? P1 : P0;
+      for (int e = tid; e < RB * n; e += nthr) {
+        const int row = e / n, x = e - row * n;
+        const long g = (r0 + row) * n + x;
+        const C z = R[row * ls + sw<N>(x)];
+        const double dcg = double(z.x) * a.renor1;
+        out1[g] = Rs(dcg);
+        out2[g] = Rs(double(z.y) * a.renor);
+        if constexpr (MODE == X_C2R2_CORR)
+          reinterpret_cast<Rt*>(&O[(row >> 1) * ls + sw<N>(x)])[row & 1] =
+              Rt(corr_source(sR0[e], dcg, a.cp4, a.cpp4));
+      }
+      if constexpr (MODE == X_C2R2_CORR) {
+        __syncthreads();
+        C* S = (O == P0) ? P1 : P0;
+        C* R2 = fft_lines<N>(O, S, RB / 2, ls, a.pl, tw, false);
+        for (int e = tid; e < RB * nxh; e += nthr) {
+          const int row = e / nxh, k = e - row * nxh;
+          specA[(r0 + row) * nxh + k] = split_r2c<N>(R2 + (row >> 1) * ls, k, n, row & 1);
+        }
+      }
+    }
+
+    if constexpr (MODE == X_C2R_POT || MODE == X_C2R1) {
+      // rows 2p and 2p+1 share complex line p
+      for (int e = tid; e < (RB / 2) * n; e += nthr) {
+        const int p = e / n, k = e - p * n;
+        P0[p * ls + sw<N>(k)] = packed_c2r(sA + (2 * p) * nxh, sA + (2 * p + 1) * nxh, k, n);
+      }
+      __syncthreads();
+      C* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, true);
+      for (int e = tid; e < RB * n; e += nthr) {
+        const int row = e / n, x = e - row * n;
+        const long g = (r0 + row) * n + x;
+        const C z = R[(row >> 1) * ls + sw<N>(x)];
+        if constexpr (MODE == X_C2R1) {
+          out1[g] = Rs(double((row & 1) ? z.y : z.x) * a.renor);
+        } else {
+          const double sto1 = double((row & 1) ? z.y : z.x) * a.renor1;
+          const double dc = sR0[e];
+          double pot = double(sR1[e]) + dc * dc * (a.a0 + a.a1 * dc) + sto1;
+          if (extra) pot = pot + extra[g];
+          if (extra2) pot = pot + extra2[g];
+          if (a.lsolid) {
+            const double d = sR2[e];
+            // tanh in the chain's precision (binary32 in the mixed path)
+            const double th = tanh(Rt(a.beta) * (Rt(d) - Rt(a.den_m)));
+            pot = pot + a.C * (1.0 + th + a.beta * d * (1.0 - th * th));
+          }
+          out1[g] = Rs(pot);
+        }
+      }
+    }
+    __syncthreads();  // stage buf and the line buffers are reused by the next tile
+  }
+  cp_async_wait<0>();
+}
+
+// One-shot variant of k_xpass: one CTA per row tile, loading its inputs straight from global
+// memory (no staging buffers, so less shared memory per CTA; the autotuner picks between the two).
+template <int MODE, int N, int TILE, typename Rt = double>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a) {
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
   const Rs* den = reinterpret_cast<const Rs*>(a.den);
@@ -196,7 +368,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass(const XArgs a) {
       if (extra2) pot = pot + extra2[g];
       if (a.lsolid) {
         const double d = den[g];
-        const double t = tanh(a.beta * (d - a.den_m));
+        const double t = tanh(Rt(a.beta) * (Rt(d) - Rt(a.den_m)));  // binary32 in the mixed path
         pot = pot + a.C * (1.0 + t + a.beta * d * (1.0 - t * t));
       }
       out1[g] = Rs(pot);

@@ -81,6 +81,10 @@ struct he_ctx {
   int x_rb = 16, tkx = 16;
   int num_sms = 148;
   int tile_x = 16, tile_y = 16, tile_z = 16;  // autotuned tile variants (16 or 8 lines)
+  // x pass per mode (XMode): rows per tile and persistent pipelined (true) or one-shot
+  int xtile[6] = {16, 16, 16, 16, 16, 16};
+  bool xpipe[6] = {false, false, false, false, false, false};
+  std::string tune_log;                        // the autotuner's trials (he_autotune_report)
   size_t smem_x = 0, smem_y = 0, smem_z = 0;
   // k space
   double2 *fden = nullptr, *wA = nullptr, *wB = nullptr;
@@ -501,20 +505,40 @@ static bool yz_fast(int n) {
 template <int MODE, int N, int TILE, typename Rt>
 static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   const int rb = (N > 0) ? TILE : a.rb;
-  const unsigned nb = (unsigned)((a.rows + rb - 1) / rb);
-  const size_t smem = fft_smem(ctx->plx, rb, 2, sizeof(typename Cx<Rt>::T));
+  const long ntiles = a.rows / rb;  // rb divides ny*nz (x_fast, he_ctx_create)
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   static const char* names[6] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
                                  "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4", "fft_x_c2r"};
+  if (!ctx->xpipe[MODE] || N == 0) {
+    const size_t csmem = fft_smem(ctx->plx, rb, 2, sizeof(typename Cx<Rt>::T));
+    CK(cudaFuncSetAttribute(k_xpass_c<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
+    tname(ctx, names[MODE]);
+    k_xpass_c<MODE, N, TILE, Rt><<<(unsigned)ntiles, nthr, csmem, ctx->stream>>>(a);
+    LAUNCHED();
+    return HE_OK;
+  }
+  constexpr int pthr = kXPipeThreads;
+  const size_t smem = xpass_smem<MODE, Rt>(ctx->plx.stw_len, rb, ctx->nx);
+  // persistent grid: as many CTAs as fit on the device at once (the smem of the run-time-length
+  // kernel depends on the grid, so its occupancy is queried per launch size)
+  static size_t occ_smem = 0;
+  static int occ = 0;
+  if (occ_smem != smem) {
+    CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xpass<MODE, N, TILE, Rt>, pthr, smem));
+    occ_smem = smem;
+  }
+  if (occ < 1) return fail(ctx, HE_ERR_STATE, "x pass: %zu bytes of shared memory do not fit an SM", smem);
+  const unsigned nb = (unsigned)std::min<long>(ntiles, (long)occ * ctx->num_sms);
   CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, names[MODE]);
-  k_xpass<MODE, N, TILE, Rt><<<nb, nthr, smem, ctx->stream>>>(a);
+  k_xpass<MODE, N, TILE, Rt><<<nb, pthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
 template <int MODE, typename Rt>
 static int xpass_t(he_ctx_t* ctx, const XArgs& a) {
-  const int tile = ctx->tile_x;
+  const int tile = ctx->xtile[MODE];
   if (x_fast(ctx, tile)) {
     switch (ctx->nx) {
 #define HE_CASE(N) \
@@ -998,6 +1022,18 @@ static int read_sums(he_ctx_t* ctx) {
 // Tile autotuner: times the 16-line and 8-line variants of each FFT pass family on this
 // context's grid (zero-filled work arrays, one warm-up and three timed launches each) and keeps
 // the faster.  Runs once in he_ctx_create.
+// Shared memory of the pipelined x pass of `mode` with `rb` rows per tile in this context.
+static size_t xpipe_smem(const he_ctx_t* ctx, int mode, int rb) {
+  const int sl = ctx->plx.stw_len, n = ctx->nx;
+  switch (mode) {
+#define HE_XS(M) \
+  case M: return ctx->mixed ? xpass_smem<M, float>(sl, rb, n) : xpass_smem<M, double>(sl, rb, n);
+    HE_XS(X_R2C_DEN) HE_XS(X_R2C_CORR) HE_XS(X_C2R2) HE_XS(X_C2R2_CORR) HE_XS(X_C2R_POT) HE_XS(X_C2R1)
+#undef HE_XS
+    default: return 0;
+  }
+}
+
 static int autotune_tiles(he_ctx_t* ctx) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CK(cudaEventCreate(&e0));
@@ -1011,29 +1047,79 @@ static int autotune_tiles(he_ctx_t* ctx) {
     CK(cudaEventElapsedTime(ms, e0, e1));
     return HE_OK;
   };
-  auto pick = [&](int* knob, int (*fn)(he_ctx_t*)) -> int {
+  auto pick = [&](int* knob, int (*fn)(he_ctx_t*), const char* what) -> int {
     float t16 = 0.0f, t8 = 0.0f;
     *knob = 16;
     TRY(timed(fn, &t16));
     *knob = 8;
     TRY(timed(fn, &t8));
     *knob = (t8 < t16) ? 8 : 16;
+    char line[96];
+    snprintf(line, sizeof line, "%s 16: %.2f us\n%s 8: %.2f us\n", what, 1e3f * t16 / 3.0f, what,
+             1e3f * t8 / 3.0f);
+    ctx->tune_log += line;
     return HE_OK;
   };
   int st = HE_OK;
-  if (x_fast(ctx, 16) && x_fast(ctx, 8))
-    st = pick(&ctx->tile_x, [](he_ctx_t* c) -> int {
-      XArgs a = xargs(c);
-      a.specA = c->wA; a.specB = c->wB; a.den = c->den;
-      a.out1 = c->dencg; a.out2 = c->delj4;
-      return xpass<X_C2R2_CORR>(c, a);
-    });
+  // x pass, per mode the step uses: {one-shot, pipelined} x {16, 8 rows}; a pipelined variant
+  // whose shared memory does not fit an SM is skipped.  The trials run on the context's
+  // (not yet initialised) work arrays; only their times matter.
+  struct XTrial {
+    int mode;
+    const char* name;
+    int (*fn)(he_ctx_t*);
+  };
+  const XTrial dyn_trials[3] = {
+      {X_R2C_DEN, "x r2c den", [](he_ctx_t* c) -> int {
+         XArgs a = xargs(c);
+         a.den = c->den; a.specA = c->wA;
+         return xpass<X_R2C_DEN>(c, a);
+       }},
+      {X_C2R2_CORR, "x c2r2 corr", [](he_ctx_t* c) -> int {
+         XArgs a = xargs(c);
+         a.specA = c->wA; a.specB = c->wB; a.den = c->den;
+         a.out1 = c->dencg; a.out2 = c->delj4;
+         return xpass<X_C2R2_CORR>(c, a);
+       }},
+      {X_C2R_POT, "x c2r pot", [](he_ctx_t* c) -> int {
+         XArgs a = xargs(c);
+         a.specA = c->wA; a.den = c->den; a.dencg_in = c->dencg; a.delj4_in = c->delj4;
+         a.out1 = c->pot4;
+         return xpass<X_C2R_POT>(c, a);
+       }}};
+  if (x_fast(ctx, 16) && x_fast(ctx, 8) && ctx->mode != HE_MODE_STATICS) {
+    int maxsm = 0, dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    for (const XTrial& tr : dyn_trials) {
+      float best = 1e30f;
+      int best_tile = 16;
+      bool best_pipe = false;
+      for (int pipe = 0; pipe < 2 && st == HE_OK; ++pipe)
+        for (int tile : {16, 8}) {
+          if (pipe && (int)xpipe_smem(ctx, tr.mode, tile) > maxsm) continue;
+          ctx->xpipe[tr.mode] = pipe != 0;
+          ctx->xtile[tr.mode] = tile;
+          float ms = 0.0f;
+          st = timed(tr.fn, &ms);
+          if (st != HE_OK) break;
+          char line[96];
+          snprintf(line, sizeof line, "%s %s %d: %.2f us\n", tr.name, pipe ? "pipelined" : "one-shot",
+                   tile, 1e3f * ms / 3.0f);
+          ctx->tune_log += line;
+          if (ms < best) { best = ms; best_tile = tile; best_pipe = pipe != 0; }
+        }
+      ctx->xpipe[tr.mode] = best_pipe;
+      ctx->xtile[tr.mode] = best_tile;
+    }
+    ctx->tile_x = ctx->xtile[X_C2R2_CORR];
+  }
   if (st == HE_OK && yz_fast(ctx->ny))
-    st = pick(&ctx->tile_y, [](he_ctx_t* c) -> int { return ypass(c, c->wA, c->wB, true); });
+    st = pick(&ctx->tile_y, [](he_ctx_t* c) -> int { return ypass(c, c->wA, c->wB, true); }, "y");
   if (st == HE_OK && yz_fast(ctx->nz))
     st = pick(&ctx->tile_z, [](he_ctx_t* c) -> int {
       return zconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, nullptr);
-    });
+    }, "z");
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st == HE_OK) CK(cudaMemsetAsync(ctx->wA, 0, 16 * ctx->Nk, ctx->stream));
@@ -2670,6 +2756,13 @@ int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n) {
   }
   *n = (int)agg.size();
   for (int i = 0; i < (int)agg.size() && i < max; ++i) out[i] = agg[i];
+  return HE_OK;
+}
+
+int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len) {
+  if (!ctx || !buf || len == 0) return HE_ERR_ARG;
+  std::string t = ctx->tune_log;
+  snprintf(buf, len, "%s", t.c_str());
   return HE_OK;
 }
 

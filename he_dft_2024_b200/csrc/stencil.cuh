@@ -80,27 +80,6 @@ HE_D T load_bc(const T* __restrict__ f, const StencilGeom& g, int ix, int iy, in
   return neg_if(v, neg);
 }
 
-// Asynchronous global -> shared copy of one element (cp.async, zero fill when src_bytes = 0).
-template <typename T>
-HE_D void cp_async_elem(T* dst_smem, const T* src, bool valid) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_smem);
-  const int nbytes = valid ? (int)sizeof(T) : 0;
-  if constexpr (sizeof(T) == 16) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src),
-                 "r"(nbytes));
-  } else if constexpr (sizeof(T) == 8) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src),
-                 "r"(nbytes));
-  } else {
-    static_assert(sizeof(T) == 4, "cp.async copies 4, 8 or 16 bytes");
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src),
-                 "r"(nbytes));
-  }
-}
-HE_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-HE_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
 // Reductions: per-block partials, the last CTA to finish sums them in a fixed order.
 struct ReduceTail {
   double* partials;

@@ -284,6 +284,10 @@ int he_timing(he_ctx_t* ctx, int enable);
 /* Tile sizes (lines per CTA, 16 or 8) the context's autotuner chose for the x, y and z FFT
  * passes at creation. */
 int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z);
+/* Text report of the FFT-pass autotuner's trials (one line per variant with its time per pass
+ * and the x-pass variant chosen), NUL-terminated and truncated to len bytes.  No counterpart in
+ * the reference (FFTW plans are fixed by fftini). */
+int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
 /* ---- energy sums without device allocation ----
