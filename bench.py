@@ -581,16 +581,18 @@ def run_serving(args):
     torch.cuda.set_device(local)
     reqs = S.make_requests(count=args.requests, rate_hz=args.rate, steps=args.req_steps,
                            seed=1234 + rank)
-    srv = S.Server(lambda w: Context(w), hbm_budget_gb=args.hbm_gb,
+    srv = S.Server(lambda w: Context(w, precision=args.precision), hbm_budget_gb=args.hbm_gb,
                    max_active=args.max_active if args.max_active > 0 else None)
     with ClockSampler(local) as clk:
         rep = srv.run(reqs)
     launches = None
     line = {
-        "metric": "TDDFT serving: aggregate grid-pt-steps/s (FP64, continuous batching)",
+        "metric": "TDDFT serving: aggregate grid-pt-steps/s ("
+                  + ("FP64" if args.precision == "f64" else "mixed") + ", continuous batching)",
         "value": rep["grid_pt_steps_per_s"], "unit": UNIT, "n_gpus": ws, "steps": rep["ticks"],
         "warmup": 0, "ms_per_step": rep["step_ms_p50"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f32x2" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": f"serve-{args.requests}req-poisson{args.rate:g}hz-{args.req_steps}steps",
                    "requests": args.requests, "rate_hz": args.rate, "steps_per_request": args.req_steps,
                    "hbm_budget_gb": args.hbm_gb, "max_active": args.max_active,

@@ -2553,6 +2553,7 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
 
 int he_derden(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
+  if (ctx->mixed) return fail(ctx, HE_ERR_STATE, "derden is not part of the mixed-precision path");
   if (!ctx->dxden) {
     TRY(dalloc_t(ctx, &ctx->dxden, ctx->N));
     TRY(dalloc_t(ctx, &ctx->dyden, ctx->N));

@@ -121,9 +121,12 @@ __device__ void reduce_tail(const ReduceTail& rt, long nb) {
 //                const Z* v16,int vs,double* acc) const;
 //   where v8[k*vs] and v16[k*vs] are this point's operands of field k (staged in shared memory).
 // Minimum resident CTAs per SM for a stencil instantiation (caps registers at 64K/(256*m)).
-template <typename T>
+// (binary32 complex fields without reductions: 4, i.e. 64 registers; with binary64 reductions
+// the consumers would spill at 64, and the corrector measured faster at 3 on 256^3 grids)
+template <class Op>
 constexpr int stencil_min_blocks() {
-  return sizeof(T) == 16 ? 2 : 3;
+  using T = typename Op::T;
+  return sizeof(T) == 16 ? 2 : (sizeof(T) == 8 ? (Op::NV > 0 ? 3 : 4) : 3);
 }
 
 // Dynamic shared memory of one stencil CTA: the double-buffered halo tile and the
@@ -137,7 +140,7 @@ HE_HD constexpr size_t stencil_smem() {
 }
 
 template <class Op, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY, stencil_min_blocks<typename Op::T>())
+__global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
     k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
               const ReduceTail rt) {
   using T = typename Op::T;

@@ -67,6 +67,9 @@ def test_mixed_energy_per_atom_within_1e5_K_over_200_steps():
 def test_mixed_rejects_unsupported_modes():
     from he_dft_2024_b200._lib import HeError
     w = workload(32)
+    with Context(w, precision="mixed") as ctx:
+        with pytest.raises(HeError):
+            ctx.derden()
     with pytest.raises(HeError):
         Context(w, mode="statics", precision="mixed")
     with pytest.raises(HeError):

@@ -1,6 +1,7 @@
 """Served trajectories on the device (he_dft_2024_b200/serving.py): a trajectory advanced by the
 continuous-batching scheduler, on a context that served other trajectories before it, ends in
-the same state as the same request run alone in a fresh context."""
+the same state as the same request run alone in a fresh context, in binary64 and in the mixed
+precision path."""
 import numpy as np
 import pytest
 
@@ -20,25 +21,26 @@ def small_requests():
     return out
 
 
-def alone(r):
+def alone(r, precision="f64"):
     w = r.workload()
-    with Context(w) as ctx:
+    with Context(w, precision=precision) as ctx:
         S.start_trajectory(ctx, w)
         for it in range(1, r.steps + 1):
             D.dynamics_iteration(ctx, it, w.deltat, w.n_imp)
         return ctx.download("rimp"), ctx.energy()
 
 
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
 @pytest.mark.parametrize("budget_gb", [100.0, 1e-3])
-def test_served_trajectories_match_standalone_runs(budget_gb):
+def test_served_trajectories_match_standalone_runs(budget_gb, precision):
     reqs = small_requests()
-    srv = S.Server(lambda w: Context(w), hbm_budget_gb=budget_gb)
+    srv = S.Server(lambda w: Context(w, precision=precision), hbm_budget_gb=budget_gb)
     rep = srv.run(reqs)
     assert rep["requests"] == 3 and rep["grid_pt_steps_per_s"] > 0
     if budget_gb < 1:
         assert srv.peak_active == 1  # one context served all three, one after the other
     for r in reqs:
-        rimp, e = alone(r)
+        rimp, e = alone(r, precision)
         np.testing.assert_allclose(r.final["rimp"], rimp, rtol=1e-12, atol=1e-14)
         for k in ("etot", "etot4", "ekin4", "eHeX", "ekinx"):
             assert abs(r.final["energy"][k] - e[k]) <= 1e-12 * max(abs(e[k]), 1.0), (k, r.rid)
