@@ -154,6 +154,17 @@ HE_D void cp_async_range(void* dst_smem, const void* src, long bytes, int tid, i
   for (long o = 16L * tid; o < bytes; o += 16L * nthr) cp_async16(d + o, g + o);
 }
 
+// ---- programmatic dependent launch ------------------------------------------------------------
+// The FFT passes of the step chain are launched with programmatic stream serialisation: a pass
+// may be scheduled while its predecessor in the stream drains, and waits here, before its first
+// access to global memory, until the predecessor has completed and its writes are visible.
+// Without the launch attribute both instructions are no-ops.  The trigger lets the successor be
+// scheduled once every CTA of this kernel has started.
+HE_D void pdl_wait_and_trigger() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // ---- block reduction of NV doubles (fixed order => deterministic) ------------------------------
 template <int NV>
 __device__ void block_reduce_store(double (&v)[NV], double* __restrict__ out) {

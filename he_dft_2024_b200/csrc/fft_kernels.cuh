@@ -129,6 +129,7 @@ HE_HD size_t xpass_smem(int stw_len, int rb, int n) {
 constexpr int kXPipeThreads = 256;  // threads of a pipelined x-pass CTA, whatever its rows
 template <int MODE, int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a) {
+  pdl_wait_and_trigger();
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
   using ST = XStage<MODE>;
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a) {
 // memory (no staging buffers, so less shared memory per CTA; the autotuner picks between the two).
 template <int MODE, int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a) {
+  pdl_wait_and_trigger();
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
   const Rs* den = reinterpret_cast<const Rs*>(a.den);
@@ -394,6 +396,7 @@ struct YZArgs {
 
 template <int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
+  pdl_wait_and_trigger();
   using C = typename Cx<Rt>::T;
   C* smem = smem_as<C>();
   const int n = (N > 0) ? N : a.ny;
@@ -425,6 +428,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
 
 template <int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a) {
+  pdl_wait_and_trigger();
   using C = typename Cx<Rt>::T;
   using X = Cx<Rt>;
   constexpr bool F32 = sizeof(Rt) == 4;

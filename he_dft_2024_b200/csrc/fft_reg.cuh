@@ -250,6 +250,7 @@ HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
 template <int N, int TK, typename Rt = double>
 __global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs a,
                                                                    const typename Cx<Rt>::T* tw2) {
+  pdl_wait_and_trigger();
   using C = typename Cx<Rt>::T;
   C* T = smem_as<C>();
   if (a.inv) ypass_reg_body<N, TK, true>(a, tw2, T);
