@@ -50,6 +50,10 @@ UNIT = "grid-pt-steps/s"
 # complex per point, half spectrum = (nx/2+1)/nx of that): reads + writes of the arrays the
 # kernel's reference counterpart consumes and produces.
 STEP_BYTES_PER_POINT = {"f64": 744.0, "mixed": 404.0}
+# quantum step, one impurity, per trajectory: FP64 36 complex, 36 real, 16 half-complex and 10
+# half-real kernel accesses per point; mixed: the stencils' complex streams shrink as in the
+# classical step (256 -> 168 B per species and step), every other stream halves
+QSTEP_BYTES_PER_POINT = {"f64": 1032.0, "mixed": 606.0}
 
 
 def kernel_bytes_per_point(nx, mixed=False):
@@ -488,7 +492,7 @@ def run_quantum(args):
     ctxs = []
     t0 = time.perf_counter()
     for w in batch:
-        c = Context(w, mode="quantum")
+        c = Context(w, mode="quantum", precision=args.precision)
         c.set_stream(stream.cuda_stream)
         den = C.woods_saxon(w)
         D.quantum_setup(c, D.initial_wavefunction(w, den), [C.psix_initial(w, 0)])
@@ -543,9 +547,9 @@ def run_quantum(args):
     name, (nl, kms) = max(rep.items(), key=lambda kv: kv[1][1])
     achieved = bpp.get(name, 0.0) * N / (kms / nl / 1e3) / 1e9
     line = {
-        "metric": METRIC_Q, "value": value, "unit": UNIT, "n_gpus": ws_, "steps": args.steps,
+        "metric": METRIC_Q.replace("FP64", "mixed") if args.precision == "mixed" else METRIC_Q, "value": value, "unit": UNIT, "n_gpus": ws_, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f32x2" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": w.name, "trajectories": len(ctxs), "grid": [w.nx, w.ny, w.nz],
                    "n4": w.n4, "impurity": "23 u quantum, Morse He-X via FT_V_spline",
                    "deltat_ps": w.deltatps, "parallelism": f"replicas{ws_}",
@@ -558,8 +562,9 @@ def run_quantum(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "alg_bytes_per_launch": bpp.get(name, 0.0) * N,
                      "ms_per_launch": kms / nl},
-        "step_alg_bytes_per_point": 1032.0,
-        "step_roofline_frac": 1032.0 * N * args.steps * len(ctxs) / secs / 1e9 / peak,
+        "step_alg_bytes_per_point": QSTEP_BYTES_PER_POINT[args.precision],
+        "step_roofline_frac": QSTEP_BYTES_PER_POINT[args.precision] * N * args.steps * len(ctxs)
+        / secs / 1e9 / peak,
         "kernels": breakdown,
         "clocks": clk.summary(),
     }
@@ -667,8 +672,8 @@ def main():
     ap.add_argument("--no-mixed", dest="mixed_compare", action="store_false",
                     help="skip the mixed-precision comparison run")
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
-                    help="precision of the timed classical line (mixed: HE_PREC_MIXED; the "
-                         "mixed-vs-FP64 comparison then runs only with the default f64)")
+                    help="precision of the timed line (mixed: HE_PREC_MIXED; for the classical "
+                         "workload the mixed-vs-FP64 comparison runs only with the default f64)")
     ap.add_argument("--workload", default="classical", choices=["classical", "quantum", "serving"])
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--requests", type=int, default=128)

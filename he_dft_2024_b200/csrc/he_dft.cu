@@ -132,6 +132,8 @@ struct he_ctx {
   void *psixold[kMaxQImp][3] = {}, *hpsixold[kMaxQImp][2] = {};
   double *denx[kMaxQImp] = {}, *upotx[kMaxQImp] = {}, *uimpk[kMaxQImp] = {};
   double* uimpkk[kMaxQImp * kMaxQImp] = {};  // (i,j) at i + kMaxQImp*j; null = no kernel
+  float* uimpkf[kMaxQImp] = {};                // binary32 copies (mixed path)
+  float* uimpkkf[kMaxQImp * kMaxQImp] = {};
   double* potx4 = nullptr;
   double2 *wC = nullptr, *wD = nullptr, *sx[kMaxQImp] = {};
   bool cglj_pending = false;  // wA/wB hold fden*wcgk, fden*fvlj4 of the current fden (x,y domain)
@@ -652,6 +654,10 @@ static const float* kernel_f32(const he_ctx_t* ctx, const double* k) {
   if (!k) return nullptr;
   if (k == ctx->wcgk) return ctx->wcgkf;
   if (k == ctx->fvlj4) return ctx->fvlj4f;
+  for (int i = 0; i < kMaxQImp; ++i)
+    if (k == ctx->uimpk[i]) return ctx->uimpkf[i];
+  for (int i = 0; i < kMaxQImp * kMaxQImp; ++i)
+    if (k == ctx->uimpkk[i]) return ctx->uimpkkf[i];
   return nullptr;
 }
 static int zconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, const double* k2,
@@ -1155,9 +1161,10 @@ static int autotune_tiles(he_ctx_t* ctx) {
 // ------------------------------------------------------------------------------------------------
 // alpha_s term (core4 = 'OTC'): term_alfa.f90:5-117
 // ------------------------------------------------------------------------------------------------
-template <int N, int TILE>
+template <int N, int TILE, typename Rt>
 static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a);
 static int zmix(he_ctx_t* ctx, ZMixArgs a);
+static int qkernels_to_f32(he_ctx_t* ctx);
 
 // out[k] = C2R(R2C(in[k]) * ker) for n <= 3 real fields, through wB, wC, wD.
 static int conv_fields(he_ctx_t* ctx, const double* const* in, double* const* out, int n,
@@ -1259,31 +1266,43 @@ static double alfa_energy(const he_ctx_t* ctx) {
 // ------------------------------------------------------------------------------------------------
 // quantum impurities (HE_MODE_QUANTUM, Dynamics_quantum_impurities)
 // ------------------------------------------------------------------------------------------------
-template <int N, int TILE>
+template <int N, int TILE, typename Rt>
 static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a) {
   const int tk = (N > 0) ? TILE : ctx->tkx;
-  const size_t smem = fft_smem(ctx->plz, tk, 3);
+  const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
-  CK(cudaFuncSetAttribute(k_zmix<N, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_zmix<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   tname(ctx, a.nout == 0 ? "fft_z_fwd" : a.fwd_in ? "fft_z_mix_fwd" : "fft_z_mix");
-  k_zmix<N, TILE><<<grid, nthr, smem, ctx->stream>>>(a);
+  k_zmix<N, TILE, Rt><<<grid, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
-static int zmix(he_ctx_t* ctx, ZMixArgs a) {
-  a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
-  a.pl = ctx->plz;
+template <typename Rt>
+static int zmix_t(he_ctx_t* ctx, const ZMixArgs& a) {
   const int tile = ctx->tile_z;
   if (yz_fast(ctx->nz)) {
     switch (ctx->nz) {
 #define HE_CASE(N) \
-  case N: return tile == 8 ? zmix_n<N, 8>(ctx, a) : zmix_n<N, 16>(ctx, a);
+  case N: return tile == 8 ? zmix_n<N, 8, Rt>(ctx, a) : zmix_n<N, 16, Rt>(ctx, a);
       HE_FFT_SIZES(HE_CASE)
 #undef HE_CASE
     }
   }
-  return zmix_n<0, 16>(ctx, a);
+  return zmix_n<0, 16, Rt>(ctx, a);
+}
+static int zmix(he_ctx_t* ctx, ZMixArgs a) {
+  a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
+  a.pl = ctx->plz;
+  if (!ctx->mixed) return zmix_t<double>(ctx, a);
+  // the binary32 chain reads the kernels' binary32 copies (passed through the same slots)
+  for (int o = 0; o < a.nout; ++o)
+    for (int t = 0; t < a.nterm[o]; ++t) {
+      const float* kf = kernel_f32(ctx, a.ker[o][t]);
+      if (!kf) return fail(ctx, HE_ERR_STATE, "no binary32 copy of a k-space kernel");
+      a.ker[o][t] = reinterpret_cast<const double*>(kf);
+    }
+  return zmix_t<float>(ctx, a);
 }
 
 // One synthesis output: sum over terms of (spectrum x kernel), inverse-transformed into `out`.
@@ -1308,6 +1327,7 @@ static int q_synth(he_ctx_t* ctx, const QOut* o, int nout, const double2* fwd_in
   TRY(zmix(ctx, z));
   TRY(ypass(ctx, ctx->wC, nout > 1 ? ctx->wD : nullptr, true));
   XArgs a = xargs(ctx);
+  a.renor1 = a.renor;  // no wcgk product here (its binary32 copy is the scaled one)
   a.specA = ctx->wC;
   a.out1 = o[0].out;
   if (nout > 1) {
@@ -1420,7 +1440,11 @@ static int q_field(he_ctx_t* ctx) {
 
 static int q_cnorm2(he_ctx_t* ctx, int i) {
   tname(ctx, "impurity_density");
-  k_cnorm2<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double2*)ctx->psix[i], ctx->denx[i], ctx->N);
+  if (ctx->mixed)
+    k_cnorm2_pair<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
+        (const float2*)ctx->psix[i], (const float2*)ctx->psix[i] + ctx->N, (float*)ctx->denx[i], ctx->N);
+  else
+    k_cnorm2<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double2*)ctx->psix[i], ctx->denx[i], ctx->N);
   LAUNCHED();
   return HE_OK;
 }
@@ -1435,18 +1459,34 @@ static int q_steprk(he_ctx_t* ctx, double deltat) {
   for (int jr = 0; jr < 4; ++jr) {
     auto stage = [&](void*& f, void*& scratch, void* qq, void** po, void** ho, const double* pot,
                      double mu, double h2o2m, double* dens) -> int {
-      OpRKQ op{};
-      op.s8[0] = pot;
-      op.s16[0] = (const double2*)qq;
-      op.q = (double2*)qq;
-      op.out = (double2*)(jr == 0 ? po[2] : scratch);
-      op.hsave = jr == 0 ? (double2*)ho[1] : nullptr;
-      op.den = dens;
-      op.tm = timec_view(ctx);
-      op.h2o2m = h2o2m;
-      op.mu = mu;
-      op.a = arun[jr]; op.b = brun[jr]; op.cc = crun[jr]; op.dt = deltat;
-      TRY(run_stencil(ctx, ctx->g2, (const double2*)f, op));
+      if (ctx->mixed) {
+        void* ob = jr == 0 ? po[2] : scratch;
+        OpRKMQ op{};
+        op.s8[0] = (const float*)pot;
+        op.s16[0] = (const float2*)qq; op.s16[1] = lo_plane(ctx, f);
+        op.q = (float2*)qq;
+        op.out_hi = hi_plane(ob); op.out_lo = lo_plane(ctx, ob);
+        op.hsave = jr == 0 ? (float2*)ho[1] : nullptr;
+        op.den = (float*)dens;
+        op.tm = timec_view(ctx);
+        op.h2o2m = (float)h2o2m;
+        op.mu = (float)mu;
+        op.a = (float)arun[jr]; op.b = (float)brun[jr]; op.cc = (float)crun[jr]; op.dt = (float)deltat;
+        TRY(run_stencil(ctx, ctx->g2, hi_plane(f), op));
+      } else {
+        OpRKQ op{};
+        op.s8[0] = pot;
+        op.s16[0] = (const double2*)qq;
+        op.q = (double2*)qq;
+        op.out = (double2*)(jr == 0 ? po[2] : scratch);
+        op.hsave = jr == 0 ? (double2*)ho[1] : nullptr;
+        op.den = dens;
+        op.tm = timec_view(ctx);
+        op.h2o2m = h2o2m;
+        op.mu = mu;
+        op.a = arun[jr]; op.b = brun[jr]; op.cc = crun[jr]; op.dt = deltat;
+        TRY(run_stencil(ctx, ctx->g2, (const double2*)f, op));
+      }
       if (jr == 0) {
         void* o3 = po[2];
         po[2] = po[1];
@@ -1478,6 +1518,27 @@ static int q_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errpsix
   const double c112 = 112.0 / 121.0, c9 = 9.0 / 121.0, c4o3 = 4.0 / 3.0;
   auto predict = [&](void*& f, void* pcc, void** po, void** ho, const double* pot, double mu,
                      double h2o2m, double* dens) -> int {
+    if (ctx->mixed) {  // pc is left alone (see OpPredictMT)
+      void* p3 = po[ctx->ioldp[2] - 1];
+      OpPredictMQ op{};
+      op.s8[0] = (const float*)pot;
+      op.po3_hi = hi_plane(p3); op.po3_lo = lo_plane(ctx, p3);
+      op.h2 = (float2*)ho[ctx->ioldh[1] - 1];
+      op.s16[0] = op.po3_hi;
+      op.s16[1] = op.po3_lo;
+      op.s16[2] = (const float2*)ho[ctx->ioldh[0] - 1];
+      op.s16[3] = op.h2;
+      op.s16[4] = (const float2*)pcc;
+      op.den = (float*)dens;
+      op.tm = timec_view(ctx);
+      op.h2o2m = (float)h2o2m;
+      op.mu = (float)mu;
+      op.s43 = (float)(c4o3 * deltat);
+      op.c112 = (float)c112;
+      TRY(run_stencil(ctx, ctx->g2, hi_plane(f), op));
+      std::swap(f, po[ctx->ioldp[2] - 1]);
+      return HE_OK;
+    }
     OpPredictQ op{};
     op.s8[0] = pot;
     op.po3 = (double2*)po[ctx->ioldp[2] - 1];
@@ -1505,6 +1566,30 @@ static int q_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errpsix
   TRY(q_field(ctx));
   auto correct = [&](void*& f, void*& scratch, void* pcc, void** po, void** ho, const double* pot,
                      double mu, double h2o2m, double* dens, int slot) -> int {
+    if (ctx->mixed) {
+      void* a3 = po[ctx->ioldp[2] - 1];
+      void* a2 = po[ctx->ioldp[1] - 1];
+      OpCorrectMQ op{};
+      op.s8[0] = (const float*)pot;
+      op.s16[0] = lo_plane(ctx, f);
+      op.s16[1] = hi_plane(a3); op.s16[2] = lo_plane(ctx, a3);
+      op.s16[3] = hi_plane(a2); op.s16[4] = lo_plane(ctx, a2);
+      op.s16[5] = (const float2*)ho[ctx->ioldh[0] - 1];
+      op.s16[6] = (const float2*)ho[ctx->ioldh[1] - 1];
+      op.s16[7] = (const float2*)pcc;
+      op.pc = (float2*)pcc;
+      op.out_hi = hi_plane(scratch); op.out_lo = lo_plane(ctx, scratch);
+      op.den = (float*)dens;
+      op.tm = timec_view(ctx);
+      op.h2o2m = (float)h2o2m;
+      op.mu = (float)mu;
+      op.s3 = (float)(3.0 * deltat);
+      op.c9 = (float)c9;
+      op.c112 = (float)c112;
+      TRY(run_stencil_red(ctx, ctx->g2, hi_plane(f), op, slot));
+      std::swap(f, scratch);
+      return HE_OK;
+    }
     OpCorrectQ op{};
     op.s8[0] = pot;
     op.s16[0] = (const double2*)po[ctx->ioldp[2] - 1];
@@ -1547,23 +1632,41 @@ static int q_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errpsix
 
 static int q_dot(he_ctx_t* ctx, const double* x, const double* y, int slot) {
   tname(ctx, "dot_reduce");
-  k_dot<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(x, y, ctx->N, tail(ctx, slot));
+  if (ctx->mixed)
+    k_dot_f32<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const float*)x, (const float*)y, ctx->N,
+                                                        tail(ctx, slot));
+  else
+    k_dot<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(x, y, ctx->N, tail(ctx, slot));
   LAUNCHED();
   return HE_OK;
 }
 
 // energy (Dynamics_quantum_impurities/energy.f90:12-139).  sto2 of the reference lands in t4.
 static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
-  OpEnergy<double2> op{};
-  op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->den;
-  op.has_u = 0;
-  op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
-  op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
-  TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_EN));
   const int n = ctx->nq;
-  for (int k = 0; k < n; ++k) {
-    OpGrad2 g{};
-    TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psix[k], g, S_QEK + k));
+  if (ctx->mixed) {
+    OpEnergy<float2> op{};
+    op.s8[0] = (const float*)ctx->den; op.s8[1] = (const float*)ctx->dencg;
+    op.s8[2] = (const float*)ctx->delj4; op.s8[3] = (const float*)ctx->den;
+    op.has_u = 0;
+    op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
+    op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
+    TRY(run_stencil_red(ctx, ctx->g1, hi_plane(ctx->psi), op, S_EN));
+    for (int k = 0; k < n; ++k) {
+      OpGrad2T<float2> g{};
+      TRY(run_stencil_red(ctx, ctx->g1, hi_plane(ctx->psix[k]), g, S_QEK + k));
+    }
+  } else {
+    OpEnergy<double2> op{};
+    op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->den;
+    op.has_u = 0;
+    op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
+    op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
+    TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_EN));
+    for (int k = 0; k < n; ++k) {
+      OpGrad2 g{};
+      TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psix[k], g, S_QEK + k));
+    }
   }
   TRY(q_denx_spectra(ctx));
   QOut o{};
@@ -1804,9 +1907,16 @@ static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
       if (up) return fail(ctx, HE_ERR_ARG, "denx is derived from psix (download only)");
       if (bytes != 8 * N) return fail(ctx, HE_ERR_ARG, "denx: expected %zu bytes", 8 * N);
       std::vector<double> acc(N, 0.0), t(N);
+      std::vector<float> tf(ctx->mixed ? N : 0);
       for (int i = 0; i < n; ++i) {
-        CK(cudaMemcpyAsync(t.data(), ctx->denx[i], 8 * N, cudaMemcpyDeviceToHost, ctx->stream));
-        TRY(sync_all(ctx));
+        if (ctx->mixed) {
+          CK(cudaMemcpyAsync(tf.data(), ctx->denx[i], 4 * N, cudaMemcpyDeviceToHost, ctx->stream));
+          TRY(sync_all(ctx));
+          for (size_t k = 0; k < N; ++k) t[k] = tf[k];
+        } else {
+          CK(cudaMemcpyAsync(t.data(), ctx->denx[i], 8 * N, cudaMemcpyDeviceToHost, ctx->stream));
+          TRY(sync_all(ctx));
+        }
         for (size_t k = 0; k < N; ++k) acc[k] = acc[k] + t[k];
       }
       std::memcpy(host, acc.data(), 8 * N);
@@ -1817,9 +1927,28 @@ static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
   size_t total = 0;
   for (auto& p : parts) total += p.second;
   if (bytes != total) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, total, bytes);
+  // device format of the field (binary64 unless the mixed path holds it narrower)
+  FieldFmt fmt = FMT_F64;
+  if (ctx->mixed) {
+    if (field == HE_F_PSIX || field == HE_F_PSIXOLD) fmt = FMT_HL;
+    else if (field == HE_F_PCX || field == HE_F_QX || field == HE_F_HPSIXOLD) fmt = FMT_C32;
+    else if (field == HE_F_UPOTX || field == HE_F_POTX4) fmt = FMT_R32;
+  }
   char* h = (char*)host;
   for (auto& p : parts) {
-    if (up) {
+    if (fmt != FMT_F64 && p.first) {
+      std::vector<unsigned char> dev;
+      if (up) {
+        to_device_fmt(fmt, h, p.second, dev);
+        CK(cudaMemcpyAsync(p.first, dev.data(), dev.size(), cudaMemcpyHostToDevice, ctx->stream));
+        TRY(sync_all(ctx));
+      } else {
+        dev.resize(device_fmt_bytes(fmt, p.second));
+        CK(cudaMemcpyAsync(dev.data(), p.first, dev.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        TRY(sync_all(ctx));
+        from_device_fmt(fmt, dev, h, p.second);
+      }
+    } else if (up) {
       if (p.first) CK(cudaMemcpyAsync(p.first, h, p.second, cudaMemcpyHostToDevice, ctx->stream));
     } else {
       if (p.first) CK(cudaMemcpyAsync(h, p.first, p.second, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1828,6 +1957,7 @@ static int q_xfer(he_ctx_t* ctx, int field, void* host, size_t bytes, bool up) {
     h += p.second;
   }
   TRY(sync_all(ctx));
+  if (up && (field == HE_F_UIMPK || field == HE_F_UIMPKK)) TRY(qkernels_to_f32(ctx));
   if (up && field == HE_F_PSIX)
     for (int i = 0; i < n; ++i) TRY(q_cnorm2(ctx, i));
   if (up && (field == HE_F_PSIX || field == HE_F_UIMPK || field == HE_F_UIMPKK)) ctx->cglj_pending = false;
@@ -1861,6 +1991,27 @@ static int kernels_to_f32(he_ctx_t* ctx) {
   return HE_OK;
 }
 
+// Binary32 copies of the impurity kernels uimp_k_i and uimp_k_k(i,j) for the mixed path
+// (allocated on first use; refreshed whenever the binary64 tables change).
+static int qkernels_to_f32(he_ctx_t* ctx) {
+  if (!ctx->mixed) return HE_OK;
+  for (int i = 0; i < kMaxQImp; ++i) {
+    if (!ctx->uimpk[i]) continue;
+    if (!ctx->uimpkf[i]) TRY(dalloc_t(ctx, &ctx->uimpkf[i], ctx->Nk));
+    tname(ctx, "kernels_to_f32");
+    k_to_f32<<<kPwBlocks, 256, 0, ctx->stream>>>(ctx->uimpk[i], ctx->uimpkf[i], ctx->Nk, 1.0);
+    LAUNCHED();
+  }
+  for (int j = 0; j < kMaxQImp * kMaxQImp; ++j) {
+    if (!ctx->uimpkk[j]) continue;
+    if (!ctx->uimpkkf[j]) TRY(dalloc_t(ctx, &ctx->uimpkkf[j], ctx->Nk));
+    tname(ctx, "kernels_to_f32");
+    k_to_f32<<<kPwBlocks, 256, 0, ctx->stream>>>(ctx->uimpkk[j], ctx->uimpkkf[j], ctx->Nk, 1.0);
+    LAUNCHED();
+  }
+  return HE_OK;
+}
+
 extern "C" {
 
 int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, int precision,
@@ -1877,8 +2028,8 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS && mode != HE_MODE_QUANTUM)
     bad(HE_ERR_ARG, "unknown mode");
   else if (precision != HE_PREC_F64 && precision != HE_PREC_MIXED) bad(HE_ERR_ARG, "unknown precision");
-  else if (precision == HE_PREC_MIXED && mode != HE_MODE_DYNAMICS)
-    bad(HE_ERR_ARG, "HE_PREC_MIXED is built for HE_MODE_DYNAMICS");
+  else if (precision == HE_PREC_MIXED && mode == HE_MODE_STATICS)
+    bad(HE_ERR_ARG, "HE_PREC_MIXED is built for the real-time modes");
   else if (precision == HE_PREC_MIXED && std::strncmp(fun->core4, "OTC", 3) == 0)
     bad(HE_ERR_ARG, "HE_PREC_MIXED does not cover core4='OTC'");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
@@ -2855,6 +3006,7 @@ int he_set_quantum_impurities(he_ctx_t* ctx, const he_qimpurities_t* q) {
       TRY(q_kernel(ctx, q->x_x[i + n * j], nspline, q->nq, q->parabolic, kk));
     }
   TRY(sync_all(ctx));
+  TRY(qkernels_to_f32(ctx));
   for (int i = 0; i < n; ++i) TRY(q_cnorm2(ctx, i));
   for (int i = 0; i < 3; ++i) ctx->ioldp[i] = i + 1;
   ctx->ioldh[0] = 1; ctx->ioldh[1] = 2;
@@ -2868,9 +3020,14 @@ int he_qimp_moments(he_ctx_t* ctx, double* out) {
     return fail(ctx, HE_ERR_STATE, "no quantum impurities");
   for (int i = 0; i < ctx->nq; ++i) {
     tname(ctx, "impurity_moments");
-    k_moments<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
-        (const double2*)ctx->psix[i], ctx->nx, ctx->ny, ctx->N, -ctx->xmax, -ctx->ymax, -ctx->zmax,
-        ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i));
+    if (ctx->mixed)
+      k_moments<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
+          (const float2*)ctx->psix[i], ctx->nx, ctx->ny, ctx->N, -ctx->xmax, -ctx->ymax, -ctx->zmax,
+          ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i));
+    else
+      k_moments<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
+          (const double2*)ctx->psix[i], ctx->nx, ctx->ny, ctx->N, -ctx->xmax, -ctx->ymax, -ctx->zmax,
+          ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i));
     LAUNCHED();
   }
   TRY(read_sums(ctx));

@@ -174,12 +174,28 @@ HE_D float2 hpsi_rt_f(float2 dx, float2 dy, float2 dz, float2 c, float pot, floa
   return make_float2(tr * ax - ay + u * c.y, tr * ay + ax - u * c.x);
 }
 
-// One RK-Gill stage (steprk.f90:67-79) on the pair planes.
-struct OpRKM {
-  static const char* kname() { return "hpsi_rkgill_stage_f32"; }
+// H psi of the quantum-impurity path in binary32: timec*(lap*h2o2m - v psi), v = pot - mu.
+HE_D float2 hpsi_q_f(float2 dx, float2 dy, float2 dz, float2 c, float v, float tr, float h2o2m) {
+  const float lx = dx.x + dy.x + dz.x, ly = dx.y + dy.y + dz.y;
+  const float ax = lx * h2o2m - v * c.x;
+  const float ay = ly * h2o2m - v * c.y;
+  return make_float2(tr * ax - ay, tr * ay + ax);
+}
+// Either path from the staged operands: QU = false reads {pot4, uimp}, QU = true reads {pot}.
+template <bool QU>
+HE_D float2 hpsi_any_f(float2 dx, float2 dy, float2 dz, float2 c, const float* v8, int vs,
+                       float mu, float tr, float h2o2m) {
+  if constexpr (QU) return hpsi_q_f(dx, dy, dz, c, v8[0] - mu, tr, h2o2m);
+  else return hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], tr, h2o2m);
+}
+
+// One RK-Gill stage (steprk.f90:67-79; quantum path steprk.f90:68-104) on the pair planes.
+template <bool QU>
+struct OpRKMT {
+  static const char* kname() { return QU ? "hpsi_rkgill_stage_q_f32" : "hpsi_rkgill_stage_f32"; }
   using T = float2;
-  static constexpr int NV = 0, N8 = 2, N16 = 2;
-  const float* s8[N8];       // pot4, uimp
+  static constexpr int NV = 0, N8 = QU ? 1 : 2, N16 = 2;
+  const float* s8[N8];       // pot4, uimp (QU: pot4 or upotx_i)
   const float2* s16[N16];    // q, psi lo plane
   float2* q;
   float2* out_hi;
@@ -187,10 +203,10 @@ struct OpRKM {
   float2* hsave;
   float* den;
   Timec tm;
-  float h2o2m, a, b, cc, dt;
+  float h2o2m, a, b, cc, dt, mu;
   HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
                const float* v8, const float2* v16, int vs, double*) const {
-    const float2 s4 = hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], (float)tm.re(ix, iy, iz), h2o2m);
+    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
     const float2 qq = v16[0];
     const float2 s1 = make_float2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
     q[i] = make_float2(qq.x + 3.0f * s1.x - cc * s4.x, qq.y + 3.0f * s1.y - cc * s4.y);
@@ -205,21 +221,22 @@ struct OpRKM {
 // (s43 (2 H psi - hh1 + 2 hh2) - c112 pc), written over po3.  pc is not overwritten with the
 // unmodified prediction sto1 (a full-size value the binary32 pc could not hold); the corrector
 // rebuilds sto1 = psi_pred + c112 pc from the predicted pair instead.
-struct OpPredictM {
-  static const char* kname() { return "hpsi_pmc_predict_f32"; }
+template <bool QU>
+struct OpPredictMT {
+  static const char* kname() { return QU ? "hpsi_pmc_predict_q_f32" : "hpsi_pmc_predict_f32"; }
   using T = float2;
-  static constexpr int NV = 0, N8 = 2, N16 = 5;
-  const float* s8[N8];       // pot4, uimp
+  static constexpr int NV = 0, N8 = QU ? 1 : 2, N16 = 5;
+  const float* s8[N8];       // pot4, uimp (QU: pot4 or upotx_i)
   const float2* s16[N16];    // po3 hi, po3 lo, hpsiold(ioldh(1)), hpsiold(ioldh(2)), pc
   float2* po3_hi;
   float2* po3_lo;
   float2* h2;
   float* den;
   Timec tm;
-  float h2o2m, s43, c112;
+  float h2o2m, s43, c112, mu;
   HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
                const float* v8, const float2* v16, int vs, double*) const {
-    const float2 s4 = hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], (float)tm.re(ix, iy, iz), h2o2m);
+    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
     const float2 hh1 = v16[2 * vs], hh2 = v16[3 * vs], pcv = v16[4 * vs];
     const float2 t = make_float2(2.0f * s4.x - hh1.x + 2.0f * hh2.x, 2.0f * s4.y - hh1.y + 2.0f * hh2.y);
     const float2 d = make_float2(s43 * t.x - c112 * pcv.x, s43 * t.y - c112 * pcv.y);
@@ -234,11 +251,12 @@ struct OpPredictM {
 //   s5 = (9 a3 - a2 + s3 (H psi_pred + 2 b1 - b2)) / 8          (pairs)
 //   pc = sto1 - s5 = (psi_pred - s5) + c112 pc_old              (a small difference, binary32)
 //   psi = s5 + c9 pc                                            (pair)
-struct OpCorrectM {
-  static const char* kname() { return "hpsi_pmc_correct_f32"; }
+template <bool QU>
+struct OpCorrectMT {
+  static const char* kname() { return QU ? "hpsi_pmc_correct_q_f32" : "hpsi_pmc_correct_f32"; }
   using T = float2;
-  static constexpr int NV = 1, N8 = 2, N16 = 8;
-  const float* s8[N8];       // pot4, uimp
+  static constexpr int NV = 1, N8 = QU ? 1 : 2, N16 = 8;
+  const float* s8[N8];       // pot4, uimp (QU: pot4 or upotx_i)
   const float2* s16[N16];    // psi_pred lo, a3 hi, a3 lo, a2 hi, a2 lo, hpsiold(ioldh(1)),
                              // hpsiold(ioldh(2)), pc
   float2* pc;
@@ -246,10 +264,10 @@ struct OpCorrectM {
   float2* out_lo;
   float* den;
   Timec tm;
-  float h2o2m, s3, c9, c112;
+  float h2o2m, s3, c9, c112, mu;
   HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
                const float* v8, const float2* v16, int vs, double* acc) const {
-    const float2 s4 = hpsi_rt_f(dx, dy, dz, c, v8[0], v8[vs], (float)tm.re(ix, iy, iz), h2o2m);
+    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
     const HL2 pred = hl2(c, v16[0]);
     const HL2 a3 = hl2(v16[vs], v16[2 * vs]), a2 = hl2(v16[3 * vs], v16[4 * vs]);
     const float2 b1 = v16[5 * vs], b2 = v16[6 * vs], pco = v16[7 * vs];
@@ -267,6 +285,13 @@ struct OpCorrectM {
     acc[0] += hypot((double)pn.x, (double)pn.y);
   }
 };
+
+using OpRKM = OpRKMT<false>;
+using OpPredictM = OpPredictMT<false>;
+using OpCorrectM = OpCorrectMT<false>;
+using OpRKMQ = OpRKMT<true>;
+using OpPredictMQ = OpPredictMT<true>;
+using OpCorrectMQ = OpCorrectMT<true>;
 
 // energy(): Dynamics_TDDFT/energy.f90:107-165 sums (first derivatives of psi).
 //   acc = {sum |grad psi|^2, sum delj4*den, sum den*dencg^2*(cp4/2+cpp4/3*dencg),

@@ -1,4 +1,5 @@
-// quantum.cuh -- device side of the quantum-impurity path (Dynamics_quantum_impurities), binary64.
+// quantum.cuh -- device side of the quantum-impurity path (Dynamics_quantum_impurities), binary64
+// and the binary32 variants of the mixed path.
 //
 // The impurities are wave functions psix_i (nx,ny,nz) with their own Hamiltonians
 //   H_i psix_i = timec*(h2o2mx_i lap psix_i - upotx_i psix_i),  h2o2mx_i = h2o2m4*4.002603/m_i,
@@ -25,17 +26,23 @@ namespace he {
 constexpr int kMaxQImp = 4;
 constexpr int kMaxTerms = 4;
 
-struct OpGrad2 {
-  static const char* kname() { return "grad2_reduce"; }
-  using T = double2;
+// TT = float2: the mixed path's binary32 hi plane, summed in binary64.
+template <typename TT>
+struct OpGrad2T {
+  static const char* kname() { return sizeof(TT) == 8 ? "grad2_reduce_f32" : "grad2_reduce"; }
+  using T = TT;
+  using R = typename RealOf<TT>::R;
+  using Z = typename RealOf<TT>::Z;
   static constexpr int NV = 1, N8 = 0, N16 = 0;
-  const double* s8[1];
-  const double2* s16[1];
-  HE_D void at(int, int, int, long, double2 dx, double2 dy, double2 dz, double2, const double*,
-               const double2*, int, double* acc) const {
-    acc[0] += cnorm2(dx) + cnorm2(dy) + cnorm2(dz);
+  const R* s8[1];
+  const Z* s16[1];
+  HE_D static double n2(TT v) { return (double)v.x * (double)v.x + (double)v.y * (double)v.y; }
+  HE_D void at(int, int, int, long, TT dx, TT dy, TT dz, TT, const R*, const Z*, int,
+               double* acc) const {
+    acc[0] += n2(dx) + n2(dy) + n2(dz);
   }
 };
+using OpGrad2 = OpGrad2T<double2>;
 
 struct ZMixArgs {
   int nxh, ny, nz, tkx;
@@ -49,9 +56,13 @@ struct ZMixArgs {
   const double* ker[2][kMaxTerms];   // real kernels over the half spectrum
 };
 
-template <int N, int TILE>
+// Rt = float: the mixed path (binary32 spectra, kernels given as their binary32 copies).
+template <int N, int TILE, typename Rt = double>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
-  extern __shared__ double2 smem[];
+  using C = typename Cx<Rt>::T;
+  C* smem = smem_as<C>();
+  const C* fwd_in = reinterpret_cast<const C*>(a.fwd_in);
+  C* fwd_store = reinterpret_cast<C*>(a.fwd_store);
   const int n = (N > 0) ? N : a.nz;
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
@@ -59,31 +70,31 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int ky = blockIdx.y;
-  double2* tw = smem;
-  double2* P0 = smem + ((a.pl.stw_len + 1) & ~1);
-  double2* P1 = P0 + TK * ls;
-  double2* P2 = P1 + TK * ls;
+  C* tw = smem;
+  C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
+  C* P1 = P0 + TK * ls;
+  C* P2 = P1 + TK * ls;
   load_twiddles(tw, a.pl);
   const long plane = (long)nxh * a.ny;
   const long base = (long)nxh * ky;
-  double2* F = nullptr;
-  double2 *O0 = P0, *O1 = P1, *S = P2;
-  if (a.fwd_in) {
+  C* F = nullptr;
+  C *O0 = P0, *O1 = P1, *S = P2;
+  if (fwd_in) {
     for (int e = tid; e < TK * n; e += nthr) {
       const int j = e / TK, c = e - j * TK;
       const int kx = kx0 + c;
-      P0[c * ls + sw<N>(j)] = (kx < nxh) ? a.fwd_in[base + kx + plane * j] : make_double2(0.0, 0.0);
+      P0[c * ls + sw<N>(j)] = (kx < nxh) ? fwd_in[base + kx + plane * j] : Cx<Rt>::make(0, 0);
     }
     __syncthreads();
     F = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, false);
     O0 = (F == P0) ? P1 : P0;
     O1 = P2;
     S = F;
-    if (a.fwd_store) {
+    if (fwd_store) {
       for (int e = tid; e < TK * n; e += nthr) {
         const int j = e / TK, c = e - j * TK;
         const int kx = kx0 + c;
-        if (kx < nxh) a.fwd_store[base + kx + plane * j] = F[c * ls + sw<N>(j)];
+        if (kx < nxh) fwd_store[base + kx + plane * j] = F[c * ls + sw<N>(j)];
       }
     }
   }
@@ -94,11 +105,12 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
     const int s = c * ls + sw<N>(j);
     const long g = base + kx + plane * j;
     for (int o = 0; o < a.nout; ++o) {
-      double2 acc = make_double2(0.0, 0.0);
+      C acc = Cx<Rt>::make(0, 0);
       if (kx < nxh) {
         for (int t = 0; t < a.nterm[o]; ++t) {
-          const double2 v = a.src[o][t] ? a.src[o][t][g] : F[s];
-          const double w = a.ker[o][t][g];
+          const C* src = reinterpret_cast<const C*>(a.src[o][t]);
+          const C v = src ? src[g] : F[s];
+          const Rt w = reinterpret_cast<const Rt*>(a.ker[o][t])[g];
           acc.x += v.x * w;
           acc.y += v.y * w;
         }
@@ -107,20 +119,20 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
     }
   }
   __syncthreads();
-  double2* R0 = fft_lines<N>(O0, S, TK, ls, a.pl, tw, true);
+  C* R0 = fft_lines<N>(O0, S, TK, ls, a.pl, tw, true);
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) a.out[0][base + kx + plane * j] = R0[c * ls + sw<N>(j)];
+    if (kx < nxh) reinterpret_cast<C*>(a.out[0])[base + kx + plane * j] = R0[c * ls + sw<N>(j)];
   }
   if (a.nout < 2) return;
   __syncthreads();
-  double2* fr = (R0 == O0) ? S : O0;
-  double2* R1 = fft_lines<N>(O1, fr, TK, ls, a.pl, tw, true);
+  C* fr = (R0 == O0) ? S : O0;
+  C* R1 = fft_lines<N>(O1, fr, TK, ls, a.pl, tw, true);
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
-    if (kx < nxh) a.out[1][base + kx + plane * j] = R1[c * ls + sw<N>(j)];
+    if (kx < nxh) reinterpret_cast<C*>(a.out[1])[base + kx + plane * j] = R1[c * ls + sw<N>(j)];
   }
 }
 
@@ -140,8 +152,30 @@ __global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const
   reduce_tail<1>(rt, gridDim.x);
 }
 
+// The mixed path: |psix|^2 of the compensated pair (hi and lo planes), rounded once to binary32.
+__global__ void __launch_bounds__(256) k_cnorm2_pair(const float2* __restrict__ hi,
+                                                     const float2* __restrict__ lo,
+                                                     float* __restrict__ out, long N) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double re = (double)hi[i].x + (double)lo[i].x, im = (double)hi[i].y + (double)lo[i].y;
+    out[i] = (float)(re * re + im * im);
+  }
+}
+
+// sum a*b of binary32 fields, summed in binary64 (the mixed path's energy sums).
+__global__ void __launch_bounds__(256) k_dot_f32(const float* __restrict__ a, const float* __restrict__ b,
+                                                 long N, const ReduceTail rt) {
+  double acc[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    acc[0] += (double)a[i] * (double)b[i];
+  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
+  reduce_tail<1>(rt, gridDim.x);
+}
+
 // {sum |f|^2, sum |f|^2 x, sum |f|^2 y, sum |f|^2 z} (DFT4He3d.f90:682-700 of the quantum driver).
-__global__ void __launch_bounds__(256) k_moments(const double2* __restrict__ f, int nx, int ny, long N,
+// (C = float2: the hi plane of the mixed path's pair, summed in binary64.)
+template <typename C>
+__global__ void __launch_bounds__(256) k_moments(const C* __restrict__ f, int nx, int ny, long N,
                                                  double x0, double y0, double z0, double hx,
                                                  double hy, double hz, const ReduceTail rt) {
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -149,7 +183,7 @@ __global__ void __launch_bounds__(256) k_moments(const double2* __restrict__ f, 
     const long r = i / nx;
     const int ix = (int)(i - r * nx);
     const int iy = (int)(r % ny), iz = (int)(r / ny);
-    const double s = cnorm2(f[i]);
+    const double s = (double)f[i].x * (double)f[i].x + (double)f[i].y * (double)f[i].y;
     acc[0] += s;
     acc[1] += s * (x0 + hx * ix);
     acc[2] += s * (y0 + hy * iy);

@@ -98,3 +98,60 @@ def test_mixed_field_formats_round_trip():
             ctx.upload(name, r)
             back = ctx.download(name)
             assert np.array_equal(back, r.astype(np.float32).astype(np.float64)), name
+
+
+# ---- quantum impurities (Dynamics_quantum_impurities) in the mixed path ------------------------
+
+def quantum_workload(n=32, n_imp=2):
+    w = C.quantum_2000(n=n)
+    return C.replace(w, xmax=12.0, ymax=12.0, zmax=12.0, n4=300, n_spline=10001, deltatps=5e-4,
+                     nq_imp=n_imp, mq_imp_u=(23.0, 40.0)[:n_imp],
+                     psix_center=((0.0, 0.0, 0.0), (2.5, -1.0, 1.5))[:n_imp],
+                     psix_kick_aps=((0.0, 1.0, 2.0), (-1.5, 0.0, 0.5))[:n_imp])
+
+
+def test_mixed_quantum_trajectory_matches_f64():
+    """Two impurity wave functions with their X-X kernel, 40 driver iterations: energy per He
+    atom, the impurities' kinetic and interaction energies and their centres against the FP64
+    run of the same state."""
+    w = quantum_workload(32, 2)
+    den = C.woods_saxon(w)
+    psi = D.initial_wavefunction(w, den)
+    psix = [C.psix_initial(w, k) for k in range(w.nq_imp)]
+    res = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, mode="quantum", precision=prec) as ctx:
+            D.quantum_setup(ctx, psi, psix)
+            for it in range(1, 41):
+                D.quantum_iteration(ctx, it, w.deltat)
+            res[prec] = (ctx.energy(), ctx.qimp_moments(), np.sum(ctx.download("den") ** 2),
+                         ctx.download("psix"))
+    e64, em = res["f64"][0], res["mixed"][0]
+    assert abs(em["etot"] - e64["etot"]) / w.n4 < 1e-5, (em["etot"], e64["etot"])
+    for k in ("ekinx", "eHeX", "eimpu_impu"):
+        assert abs(em[k] - e64[k]) <= 1e-5 * max(abs(e64[k]), 1.0), (k, em[k], e64[k])
+    m64, mm = res["f64"][1], res["mixed"][1]
+    assert np.max(np.abs(mm - m64)) < 1e-6, np.max(np.abs(mm - m64))
+    assert abs(res["mixed"][2] - res["f64"][2]) < 1e-6 * res["f64"][2]
+    px = res["mixed"][3] - res["f64"][3]
+    assert 0 < np.max(np.abs(px)) < 1e-5 * np.max(np.abs(res["f64"][3]))
+
+
+def test_mixed_quantum_field_formats_round_trip():
+    w = quantum_workload(32, 2)
+    rng = np.random.default_rng(9)
+    shape = (w.nx, w.ny, w.nz, 2)
+    z = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    r = rng.random(shape)
+    with Context(w, mode="quantum", precision="mixed") as ctx:
+        D.quantum_setup(ctx, D.initial_wavefunction(w, C.woods_saxon(w)),
+                        [C.psix_initial(w, k) for k in range(2)])
+        ctx.upload("psix", z)
+        back = ctx.download("psix")
+        assert 0 < np.max(np.abs(back - z)) / np.max(np.abs(z)) < 2.0 ** -45
+        ctx.upload("pcx", z)
+        assert np.array_equal(ctx.download("pcx"), z.astype(np.complex64).astype(np.complex128))
+        ctx.upload("upotx", r)
+        assert np.array_equal(ctx.download("upotx"), r.astype(np.float32).astype(np.float64))
+        denx = ctx.download("denx")
+        assert np.allclose(denx, np.sum(np.abs(z) ** 2, axis=-1), rtol=1e-6)
