@@ -456,9 +456,26 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def quantum_bytes_per_point(nx):
-    """Algorithmic bytes per grid point of the quantum kernels (binary64, see kernel_bytes_per_point)."""
+def quantum_bytes_per_point(nx, mixed=False):
+    """Algorithmic bytes per grid point of the quantum kernels (see kernel_bytes_per_point)."""
     hk = (nx // 2 + 1) / nx
+    if mixed:
+        c, r, p = 8.0, 4.0, 16.0  # binary32 complex / real, compensated pair
+        return {
+            # psi hi, pot, po3 pair, hpsiold x2, pc -> po3 pair, hpsiold, den
+            "hpsi_pmc_predict_q_f32": (c + r + p + 2 * c + c) + (p + c + r),
+            # psi pair, pot, psiold pairs x2, hpsiold x2, pc -> psi pair, pc, den
+            "hpsi_pmc_correct_q_f32": (p + r + 2 * p + 2 * c + c) + (p + c + r),
+            "hpsi_rkgill_stage_q_f32": (p + r + c) + (c + p + r),
+            "fft_x_r2c_den": r + c * hk,
+            "fft_x_c2r_cg_lj_r2c_corr": 2 * c * hk + r + 2 * r + c * hk,
+            "fft_x_c2r_cg_lj": 2 * c * hk + 2 * r,
+            "fft_x_c2r_pot4": c * hk + 4 * r + r,
+            "fft_y": 2 * c * hk,
+            "fft_z_conv1": 2 * c * hk + r * hk,
+            "fft_z_conv2": c * hk + 3 * c * hk + 2 * r * hk,
+            "fft_z_mix_fwd": c * hk + 2 * c * hk + c * hk + r * hk,
+        }
     c, r = 16.0, 8.0
     return {
         # psi, pot, psiold(ioldp3), hpsiold x2, pc -> psi_new, pc, hpsiold, den
@@ -532,6 +549,24 @@ def run_quantum(args):
         it += 1
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t1
+    # mixed: the first trajectory run again in binary64 from the same start for as many driver
+    # iterations as its mixed run has taken, compared on E/N and the impurity's centre
+    vs_f64 = None
+    if args.precision == "mixed":
+        wc = batch[0]
+        ref = Context(wc, mode="quantum")
+        ref.set_stream(stream.cuda_stream)
+        D.quantum_setup(ref, D.initial_wavefunction(wc, C.woods_saxon(wc)), [C.psix_initial(wc, 0)])
+        for k in range(1, it):
+            D.quantum_iteration(ref, k, wc.deltat)
+        em, ef = ctxs[0].energy(), ref.energy()
+        mm, mf = ctxs[0].qimp_moments()[0], ref.qimp_moments()[0]  # norm, <x>, <y>, <z>
+        vs_f64 = {"steps_compared": it - 1, "E_per_N_f64": ef["etot"] / wc.n4,
+                  "E_per_N_mixed": em["etot"] / wc.n4,
+                  "abs_dE_per_N_K": abs(em["etot"] - ef["etot"]) / wc.n4,
+                  "abs_d_impurity_centre_A": float(np.max(np.abs(mm[1:] - mf[1:]))),
+                  "abs_d_impurity_norm": float(abs(mm[0] - mf[0]))}
+        ref.close()
     ctxs[0].timing(True)
     for _ in range(3):
         D.quantum_iteration(ctxs[0], it, w.deltat)
@@ -539,7 +574,7 @@ def run_quantum(args):
     rep = ctxs[0].timing_report()
     ctxs[0].timing(False)
     tot = sum(v[1] for v in rep.values())
-    bpp = quantum_bytes_per_point(w.nx)
+    bpp = quantum_bytes_per_point(w.nx, mixed=args.precision == "mixed")
     peak, peak_kind = measured_peak()
     breakdown = {k: {"launches": v[0], "ms_per_launch": v[1] / v[0], "share": v[1] / tot,
                      "GB/s": (bpp[k] * N / (v[1] / v[0] / 1e3) / 1e9) if k in bpp else None}
@@ -566,6 +601,7 @@ def run_quantum(args):
         "step_roofline_frac": QSTEP_BYTES_PER_POINT[args.precision] * N * args.steps * len(ctxs)
         / secs / 1e9 / peak,
         "kernels": breakdown,
+        "vs_f64": vs_f64,
         "clocks": clk.summary(),
     }
     for c in ctxs:

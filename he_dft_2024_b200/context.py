@@ -96,6 +96,11 @@ class Context:
         self._ck(self.L.he_tuned_tiles(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
+    def set_fft_variant(self, pass_, variant, tile):
+        """Override the autotuner for one pass family: pass_ 'x', 'y' or 'z'; variant 0/1 (x:
+        one-shot / pipelined, y: register only, z: shared memory / register); tile 8 or 16."""
+        self._ck(self.L.he_set_fft_variant(self.h, {"x": 0, "y": 1, "z": 2}[pass_], variant, tile))
+
     def autotune_report(self):
         """The FFT autotuner's trial times, one line per variant, and the x-pass variant chosen."""
         buf = ctypes.create_string_buffer(4096)

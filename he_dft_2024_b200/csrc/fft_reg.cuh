@@ -257,4 +257,119 @@ __global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs 
   else ypass_reg_body<N, TK, false>(a, tw2, T);
 }
 
+// z pass of a convolution with the line transform in registers (N = N1 x N2, TK columns kx):
+//   phase A  (thread c, a):  x[kz = a + N2 m] from HBM, DFT_N1 over m, twiddle W_N^(a k1),
+//                            exchange through shared memory;
+//   phase B  (thread c, k1): DFT_N2 over a -> X[k1 + N1 k2] for all k2 in registers (stored as
+//            fden when asked), times the kernel(s), inverse DFT_N2 over k2 -> n2, twiddle
+//            W_N^-(n2 k1), exchange;
+//   phase A' (thread c, n2): inverse DFT_N1 over k1 -> y[n2 + N2 n1], stored over the input (and
+//            into out2).
+// The forward spectrum never leaves registers between the two transforms, and a CTA needs one
+// (two for two kernels) N x TK exchange buffer instead of three line buffers.
+template <int N, int TK, typename C>
+HE_D void zconv_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T0, C* T1) {
+  using Rt = decltype(T0[0].x);
+  using X = Cx<Rt>;
+  constexpr bool F32 = sizeof(Rt) == 4;
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  const int tid = threadIdx.x;
+  const int nxh = a.nxh;
+  const int kx0 = blockIdx.x * TK;
+  const long plane = (long)nxh * a.ny;
+  const long base = (long)nxh * blockIdx.y;
+  C* io = reinterpret_cast<C*>(a.io);
+  C* out2 = reinterpret_cast<C*>(a.out2);
+  C* fden_out = reinterpret_cast<C*>(a.fden_out);
+  const bool two = F32 ? a.k2f != nullptr : a.k2 != nullptr;
+  {
+    const int c = tid % TK, am = tid / TK;
+    const int kx = kx0 + c;
+    const bool ok = kx < nxh;
+    const C* src = io + base + (ok ? kx : 0) + plane * am;
+    C v[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) v[m] = ok ? src[plane * N2 * m] : X::make(0, 0);
+    RDft<N1, false>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul_conj_if(v[k1], __ldg(&tw2[k1 * N2 + am]), false);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) T0[(k1 * N2 + am) * TK + c] = v[k1];
+  }
+  __syncthreads();
+  const bool actB = tid < TK * N1;
+  const int cB = tid % TK, k1 = tid / TK;
+  C u[N2], w[N2];
+  if (actB) {
+    const int kx = kx0 + cB;
+    const bool ok = kx < nxh;
+#pragma unroll
+    for (int q = 0; q < N2; ++q) u[q] = T0[(k1 * N2 + q) * TK + cB];
+    RDft<N2, false>::run(u);
+    const long g0 = base + (ok ? kx : 0) + plane * k1;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const long g = g0 + plane * N1 * k2;
+      if (ok && fden_out) fden_out[g] = u[k2];
+      if (two) {
+        const Rt w2 = ok ? (F32 ? Rt(a.k2f[g]) : Rt(a.k2[g])) : Rt(0);
+        w[k2] = X::make(u[k2].x * w2, u[k2].y * w2);
+      }
+      const Rt w1 = ok ? (F32 ? Rt(a.k1f[g]) : Rt(a.k1[g])) : Rt(0);
+      u[k2] = X::make(u[k2].x * w1, u[k2].y * w1);
+    }
+    RDft<N2, true>::run(u);
+#pragma unroll
+    for (int n2 = 1; n2 < N2; ++n2) u[n2] = cmul_conj_if(u[n2], __ldg(&tw2[k1 * N2 + n2]), true);
+    if (two) {
+      RDft<N2, true>::run(w);
+#pragma unroll
+      for (int n2 = 1; n2 < N2; ++n2) w[n2] = cmul_conj_if(w[n2], __ldg(&tw2[k1 * N2 + n2]), true);
+    }
+  }
+  __syncthreads();  // every phase-B thread has read T0
+  if (actB) {
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) T0[(k1 * N2 + n2) * TK + cB] = u[n2];
+    if (two) {
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) T1[(k1 * N2 + n2) * TK + cB] = w[n2];
+    }
+  }
+  __syncthreads();
+  {
+    const int c = tid % TK, n2 = tid / TK;
+    const int kx = kx0 + c;
+    const bool ok = kx < nxh;
+    C v[N1];
+#pragma unroll
+    for (int q = 0; q < N1; ++q) v[q] = T0[(q * N2 + n2) * TK + c];
+    RDft<N1, true>::run(v);
+    if (ok) {
+      C* dst = io + base + kx + plane * n2;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) dst[plane * N2 * n1] = v[n1];
+    }
+    if (two) {
+#pragma unroll
+      for (int q = 0; q < N1; ++q) v[q] = T1[(q * N2 + n2) * TK + c];
+      RDft<N1, true>::run(v);
+      if (ok) {
+        C* dst = out2 + base + kx + plane * n2;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) dst[plane * N2 * n1] = v[n1];
+      }
+    }
+  }
+}
+
+template <int N, int TK, typename Rt = double>
+__global__ void __launch_bounds__(yreg_threads(N, TK)) k_zconv_reg(const YZArgs a,
+                                                                   const typename Cx<Rt>::T* tw2) {
+  pdl_wait_and_trigger();
+  using C = typename Cx<Rt>::T;
+  C* T0 = smem_as<C>();
+  zconv_reg_body<N, TK>(a, tw2, T0, T0 + N * TK);
+}
+
 }  // namespace he

@@ -87,6 +87,8 @@ struct he_ctx {
   int tile_x = 16, tile_y = 16, tile_z = 16;  // autotuned tile variants (16 or 8 lines)
   // x pass per mode (XMode): rows per tile and persistent pipelined (true) or one-shot
   int xtile[6] = {16, 16, 16, 16, 16, 16};
+  bool zreg = false;  // z convolution with register line transforms (binary32 chain only)
+  int maxsm = 0;      // opt-in shared memory per block
   bool xpipe[6] = {false, false, false, false, false, false};
   std::string tune_log;                        // the autotuner's trials (he_autotune_report)
   size_t smem_x = 0, smem_y = 0, smem_z = 0;
@@ -627,6 +629,19 @@ static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
 template <int N, int TILE, typename Rt>
 static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
   const int tk = (N > 0) ? TILE : ctx->tkx;
+  if constexpr (N > 0 && sizeof(Rt) == 4) {
+    if (ctx->zreg) {  // register line transforms (fft_reg.cuh), binary32 chain
+      using C = typename Cx<Rt>::T;
+      const size_t rsmem = sizeof(C) * (size_t)N * TILE * (a.k2f ? 2 : 1);
+      CK(cudaFuncSetAttribute(k_zconv_reg<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+      dim3 grid((ctx->nxh + TILE - 1) / TILE, ctx->ny, 1);
+      tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
+      CK(launch_chain(ctx, k_zconv_reg<N, TILE, Rt>, grid, dim3(yreg_threads(N, TILE)), rsmem, a,
+                      (const C*)ctx->plz.tw2f));
+      LAUNCHED();
+      return HE_OK;
+    }
+  }
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
@@ -1144,10 +1159,32 @@ static int autotune_tiles(he_ctx_t* ctx) {
   }
   if (st == HE_OK && yz_fast(ctx->ny))
     st = pick(&ctx->tile_y, [](he_ctx_t* c) -> int { return ypass(c, c->wA, c->wB, true); }, "y");
-  if (st == HE_OK && yz_fast(ctx->nz))
-    st = pick(&ctx->tile_z, [](he_ctx_t* c) -> int {
-      return zconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, nullptr);
-    }, "z");
+  if (st == HE_OK && yz_fast(ctx->nz)) {
+    auto zfn = [](he_ctx_t* c) -> int { return zconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, nullptr); };
+    st = pick(&ctx->tile_z, zfn, "z");
+    if (st == HE_OK && ctx->mixed) {
+      // the binary32 chain also has the register variant: keep it if it beats the best so far
+      const int tile0 = ctx->tile_z;
+      float t0 = 0.0f;
+      st = timed(zfn, &t0);
+      float best = t0;
+      int best_tile = tile0;
+      bool best_reg = false;
+      ctx->zreg = true;
+      for (int tile : {16, 8}) {
+        if (st != HE_OK) break;
+        ctx->tile_z = tile;
+        float ms = 0.0f;
+        st = timed(zfn, &ms);
+        char line[96];
+        snprintf(line, sizeof line, "z register %d: %.2f us\n", tile, 1e3f * ms / 3.0f);
+        ctx->tune_log += line;
+        if (ms < best) { best = ms; best_tile = tile; best_reg = true; }
+      }
+      ctx->zreg = best_reg;
+      ctx->tile_z = best_tile;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st == HE_OK) CK(cudaMemsetAsync(ctx->wA, 0, 16 * ctx->Nk, ctx->stream));
@@ -2109,6 +2146,7 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   int maxsm = 0, dev = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  ctx->maxsm = maxsm;
   if ((int)ctx->smem_x > maxsm || (int)ctx->smem_y > maxsm || (int)ctx->smem_z > maxsm)
     return fail(ctx, HE_ERR_ARG, "grid too large for the shared-memory FFT passes");
 
@@ -2932,6 +2970,33 @@ int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n) {
   *n = (int)agg.size();
   for (int i = 0; i < (int)agg.size() && i < max; ++i) out[i] = agg[i];
   return HE_OK;
+}
+
+int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
+  if (!ctx) return HE_ERR_ARG;
+  if (tile != 8 && tile != 16) return fail(ctx, HE_ERR_ARG, "tile must be 8 or 16");
+  if (variant != 0 && variant != 1) return fail(ctx, HE_ERR_ARG, "variant must be 0 or 1");
+  switch (pass) {
+    case 0:
+      if (!x_fast(ctx, tile)) return fail(ctx, HE_ERR_ARG, "x pass: no compile-time variant for this grid");
+      for (int m = 0; m < 6; ++m) {
+        if (variant && (long)xpipe_smem(ctx, m, tile) > (long)ctx->maxsm)
+          return fail(ctx, HE_ERR_ARG, "pipelined x pass with %d rows does not fit shared memory", tile);
+      }
+      for (int m = 0; m < 6; ++m) { ctx->xpipe[m] = variant != 0; ctx->xtile[m] = tile; }
+      ctx->tile_x = tile;
+      return HE_OK;
+    case 1:
+      if (variant != 1) return fail(ctx, HE_ERR_ARG, "the y pass has the register variant only");
+      ctx->tile_y = tile;
+      return HE_OK;
+    case 2:
+      if (variant && !ctx->mixed) return fail(ctx, HE_ERR_ARG, "the register z pass is built for HE_PREC_MIXED");
+      ctx->zreg = variant != 0;
+      ctx->tile_z = tile;
+      return HE_OK;
+    default: return fail(ctx, HE_ERR_ARG, "pass must be 0 (x), 1 (y) or 2 (z)");
+  }
 }
 
 int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len) {

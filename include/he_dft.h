@@ -289,6 +289,12 @@ int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z);
  * and the x-pass variant chosen), NUL-terminated and truncated to len bytes.  No counterpart in
  * the reference (FFTW plans are fixed by fftini). */
 int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
+/* Overrides the autotuner's choice for one pass family (reproducible runs, tests): pass 0 = x
+ * (variant 0 one-shot, 1 persistent pipelined; every mode), 1 = y (variant 1, the register
+ * transform), 2 = z (variant 0 shared-memory Stockham, 1 register transform, HE_PREC_MIXED only);
+ * tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
+ * counterpart in the reference. */
+int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
 /* ---- energy sums without device allocation ----

@@ -155,3 +155,23 @@ def test_mixed_quantum_field_formats_round_trip():
         assert np.array_equal(ctx.download("upotx"), r.astype(np.float32).astype(np.float64))
         denx = ctx.download("denx")
         assert np.allclose(denx, np.sum(np.abs(z) ** 2, axis=-1), rtol=1e-6)
+
+
+@pytest.mark.parametrize("zvar,tile", [(0, 8), (1, 8), (1, 16)])
+def test_mixed_fft_variants_agree(zvar, tile):
+    """Each z-pass variant of the binary32 chain (shared-memory Stockham, register transform)
+    and the pipelined x pass give the FP64 fields to binary32 accuracy."""
+    w = workload(64)
+    den = C.woods_saxon(w)
+    out = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, precision=prec) as ctx:
+            if prec == "mixed":
+                ctx.set_fft_variant("z", zvar, tile)
+                ctx.set_fft_variant("x", zvar, tile)
+            ctx.upload("den", den)
+            ctx.poten()
+            out[prec] = {k: ctx.download(k) for k in ("pot4", "dencg", "delj4", "fden")}
+    for k, b in {"pot4": 2e-6, "dencg": 2e-6, "delj4": 2e-6, "fden": 2e-6}.items():
+        r = rel(out["mixed"][k], out["f64"][k])
+        assert 1e-12 < r < b, (k, r)
