@@ -282,6 +282,9 @@ def run_ours(args):
     N = w.n
     ctx = Context(w, precision=args.precision)
     mixed_main = args.precision == "mixed"
+    for spec in filter(None, args.fft_pin.split(",")):
+        p_, v_, t_ = spec.split(":")
+        ctx.set_fft_variant(p_, int(v_), int(t_))
     # A dedicated (non-default) stream: the library's kernels and the timing events share it.
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -707,6 +710,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", dest="mixed_compare", action="store_false",
                     help="skip the mixed-precision comparison run")
+    ap.add_argument("--fft-pin", default="",
+                    help="pin FFT pass variants of the timed classical context instead of the "
+                         "autotuner's choice, e.g. 'x0:0:8,x3:1:8,y:1:8,z:0:8' (pass:variant:tile; "
+                         "used to profile the variants a timed run picked: under a profiler the "
+                         "autotuner's trial timings are distorted)")
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
                     help="precision of the timed line (mixed: HE_PREC_MIXED; for the classical "
                          "workload the mixed-vs-FP64 comparison runs only with the default f64)")

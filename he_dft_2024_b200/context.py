@@ -97,9 +97,13 @@ class Context:
         return tuple(x.value for x in v)
 
     def set_fft_variant(self, pass_, variant, tile):
-        """Override the autotuner for one pass family: pass_ 'x', 'y' or 'z'; variant 0/1 (x:
-        one-shot / pipelined, y: register only, z: shared memory / register); tile 8 or 16."""
-        self._ck(self.L.he_set_fft_variant(self.h, {"x": 0, "y": 1, "z": 2}[pass_], variant, tile))
+        """Override the autotuner for one pass family: pass_ 'x' (every mode), 'x0'..'x5' (one
+        x mode), 'y' or 'z'; variant 0/1 (x: one-shot / pipelined, y: register only, z: shared
+        memory / register); tile 8 or 16."""
+        code = {"x": 0, "y": 1, "z": 2}.get(pass_)
+        if code is None:
+            code = 3 + int(pass_[1:])
+        self._ck(self.L.he_set_fft_variant(self.h, code, variant, tile))
 
     def autotune_report(self):
         """The FFT autotuner's trial times, one line per variant, and the x-pass variant chosen."""

@@ -2333,13 +2333,15 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   if (qfield(field)) return q_xfer(ctx, field, const_cast<void*>(host), bytes, true);
   if (field >= HE_F_RIMP && field <= HE_F_QV) {
     if (ctx->mode != HE_MODE_DYNAMICS) return fail(ctx, HE_ERR_STATE, "no impurities in statics");
-    ImpDev h;
-    TRY(imp_pull(ctx, &h));
+    // only the member's bytes go to the device struct (no read-back, no wait): the driver uploads
+    // aimp every iteration
+    ImpDev h{};
+    h.n = ctx->n_imp;
     size_t cnt = 0;
     double* m = imp_member(&h, field, &cnt);
     if (!m || bytes != cnt * 8) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes", field, cnt * 8);
-    std::memcpy(m, host, bytes);
-    TRY(imp_push(ctx, &h));
+    const size_t off = (size_t)((char*)m - (char*)&h);
+    CK(cudaMemcpyAsync((char*)ctx->imp + off, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
     ctx->force_fresh = false;
     return HE_OK;
   }
@@ -2995,7 +2997,17 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
       ctx->zreg = variant != 0;
       ctx->tile_z = tile;
       return HE_OK;
-    default: return fail(ctx, HE_ERR_ARG, "pass must be 0 (x), 1 (y) or 2 (z)");
+    default:
+      if (pass >= 3 && pass < 9) {  // one x mode (XMode pass - 3)
+        const int m = pass - 3;
+        if (!x_fast(ctx, tile)) return fail(ctx, HE_ERR_ARG, "x pass: no compile-time variant for this grid");
+        if (variant && (long)xpipe_smem(ctx, m, tile) > (long)ctx->maxsm)
+          return fail(ctx, HE_ERR_ARG, "pipelined x pass with %d rows does not fit shared memory", tile);
+        ctx->xpipe[m] = variant != 0;
+        ctx->xtile[m] = tile;
+        return HE_OK;
+      }
+      return fail(ctx, HE_ERR_ARG, "pass must be 0 (x), 1 (y), 2 (z) or 3..8 (one x mode)");
   }
 }
 

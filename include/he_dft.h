@@ -206,7 +206,9 @@ int he_compute_kernels(he_ctx_t* ctx);
 int he_set_absorber(he_ctx_t* ctx, const he_absorber_t* abs);
 int he_set_impurities(he_ctx_t* ctx, const he_impurities_t* imp);
 
-/* Module-array transfer.  bytes must equal the field's size (see enum he_field). */
+/* Module-array transfer.  bytes must equal the field's size (see enum he_field).  Both return
+ * once the host buffer may be reused; the copy is ordered before every later call on the context
+ * (field downloads and uploads wait for the device, impurity-array uploads do not). */
 int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes);
 int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes);
 
@@ -291,8 +293,10 @@ int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z);
 int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
 /* Overrides the autotuner's choice for one pass family (reproducible runs, tests): pass 0 = x
  * (variant 0 one-shot, 1 persistent pipelined; every mode), 1 = y (variant 1, the register
- * transform), 2 = z (variant 0 shared-memory Stockham, 1 register transform, HE_PREC_MIXED only);
- * tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
+ * transform), 2 = z (variant 0 shared-memory Stockham, 1 register transform, HE_PREC_MIXED only),
+ * 3 + m = the x pass of one mode m only (0 R2C of den, 1 R2C of the statics correlation source,
+ * 2 C2R of two spectra, 3 the same plus the correlation R2C, 4 C2R + pot4, 5 C2R of one
+ * spectrum); tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
  * counterpart in the reference. */
 int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
