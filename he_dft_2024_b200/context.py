@@ -98,9 +98,10 @@ class Context:
 
     def set_fft_variant(self, pass_, variant, tile):
         """Override the autotuner for one pass family: pass_ 'x' (every mode), 'x0'..'x5' (one
-        x mode), 'y' or 'z'; variant 0/1 (x: one-shot / pipelined, y: register only, z: shared
-        memory / register); tile 8 or 16."""
-        code = {"x": 0, "y": 1, "z": 2}.get(pass_)
+        x mode), 'y', 'z' or 'xy' (fused plane passes of the classical field evaluation);
+        variant 0/1 (x: one-shot / pipelined, y: register only, z: shared memory / register,
+        xy: off / on); tile 8 or 16."""
+        code = {"x": 0, "y": 1, "z": 2, "xy": 9}.get(pass_)
         if code is None:
             code = 3 + int(pass_[1:])
         self._ck(self.L.he_set_fft_variant(self.h, code, variant, tile))

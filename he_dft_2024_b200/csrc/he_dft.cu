@@ -18,6 +18,7 @@
 #include "fft.cuh"
 #include "fft_kernels.cuh"
 #include "fft_reg.cuh"
+#include "fft_xy.cuh"
 #include "ops.cuh"
 #include "setup.cuh"
 #include "quantum.cuh"
@@ -88,6 +89,7 @@ struct he_ctx {
   // x pass per mode (XMode): rows per tile and persistent pipelined (true) or one-shot
   int xtile[6] = {16, 16, 16, 16, 16, 16};
   bool zreg = false;  // z convolution with register line transforms (binary32 chain only)
+  bool xyfuse = false;  // classical field evaluation with fused x-y plane passes (fft_xy.cuh)
   int maxsm = 0;      // opt-in shared memory per block
   bool xpipe[6] = {false, false, false, false, false, false};
   std::string tune_log;                        // the autotuner's trials (he_autotune_report)
@@ -715,6 +717,60 @@ static int correlation_tail(he_ctx_t* ctx, const double* extra = nullptr,
   return xpass<X_C2R_POT>(ctx, a);
 }
 
+// ---- fused x-y plane passes (fft_xy.cuh): binary32 chain, nx = ny in {64, 96, 128} ---------------
+static bool xy_fusable(const he_ctx_t* ctx) {
+  return ctx->mixed && ctx->nx == ctx->ny && (ctx->nx == 64 || ctx->nx == 96 || ctx->nx == 128) &&
+         split_n1(ctx->nx) > 0 && ((long)ctx->nxh * ctx->ny) % 2 == 0;
+}
+static XYArgs xyargs(he_ctx_t* ctx) {
+  XYArgs a{};
+  a.twx = ctx->plx.tw2f; a.twy = ctx->ply.tw2f;
+  a.renor = ctx->renor; a.renor1 = ctx->renor / ctx->cg_scale;
+  a.cp4 = ctx->fn.cp4; a.cpp4 = ctx->fn.cpp4;
+  a.a0 = ctx->fn.cp4 / 2.0; a.a1 = ctx->fn.cpp4 / 3.0;
+  a.lsolid = ctx->fn.lsolid;
+  a.C = ctx->fn.C; a.beta = ctx->fn.beta; a.den_m = ctx->fn.den_m;
+  return a;
+}
+template <int N>
+static int xy_launch(he_ctx_t* ctx, int kind, const XYArgs& a) {
+  static const char* names[3] = {"fft_xy_r2c_den", "fft_xy_c2r_cg_lj_r2c_corr", "fft_xy_c2r_pot4"};
+  void (*k)(XYArgs) = kind == 0 ? k_xy_r2c<N> : kind == 1 ? k_xy_c2r2_corr<N> : k_xy_c2r_pot<N>;
+  const size_t smem = kind == 1 ? xy_smem_corr<N>() : xy_smem_r2c<N>();
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  tname(ctx, names[kind]);
+  CK(launch_chain(ctx, k, dim3(ctx->nz), dim3(kXYThreads), smem, a));
+  LAUNCHED();
+  return HE_OK;
+}
+static int xy_pass(he_ctx_t* ctx, int kind, const XYArgs& a) {
+  switch (ctx->nx) {
+    case 64: return xy_launch<64>(ctx, kind, a);
+    case 96: return xy_launch<96>(ctx, kind, a);
+    case 128: return xy_launch<128>(ctx, kind, a);
+    default: return fail(ctx, HE_ERR_STATE, "fused x-y passes need nx = ny in {64, 96, 128}");
+  }
+}
+// Dynamics_TDDFT/poten.f90:131-218 with fused plane passes: 5 launches instead of 9.
+static int poten_fused(he_ctx_t* ctx, const double* extra, const double* extra2) {
+  XYArgs a = xyargs(ctx);
+  a.den = (const float*)ctx->den;
+  a.specA = (float2*)ctx->wA;
+  TRY(xy_pass(ctx, 0, a));
+  TRY(zconv(ctx, ctx->wA, ctx->wcgk, ctx->wB, ctx->fvlj4, ctx->fden));
+  a.specB = (const float2*)ctx->wB;
+  a.out1 = (float*)ctx->dencg; a.out2 = (float*)ctx->delj4;
+  TRY(xy_pass(ctx, 1, a));
+  TRY(zconv(ctx, ctx->wA, ctx->wcgk, nullptr, nullptr, nullptr));
+  XYArgs b = xyargs(ctx);
+  b.specA = (float2*)ctx->wA;
+  b.den = (const float*)ctx->den; b.dencg_in = (const float*)ctx->dencg;
+  b.delj4_in = (const float*)ctx->delj4;
+  b.extra = (const float*)extra; b.extra2 = (const float*)extra2;
+  b.out1 = (float*)ctx->pot4;
+  return xy_pass(ctx, 2, b);
+}
+
 // ---- module-array access -----------------------------------------------------------------------
 static size_t wf_elem(const he_ctx_t* ctx) {
   return ctx->mode == HE_MODE_STATICS ? sizeof(double) : sizeof(double2);
@@ -1183,6 +1239,28 @@ static int autotune_tiles(he_ctx_t* ctx) {
       }
       ctx->zreg = best_reg;
       ctx->tile_z = best_tile;
+    }
+  }
+  if (st == HE_OK && ctx->mode == HE_MODE_DYNAMICS && !ctx->otc && xy_fusable(ctx)) {
+    // the whole classical field evaluation, plane-fused against the separate passes
+    auto sep = [](he_ctx_t* c) -> int {
+      TRY(spectrum_cg_lj(c));
+      XArgs a = xargs(c);
+      a.specA = c->wA; a.specB = c->wB; a.den = c->den;
+      a.out1 = c->dencg; a.out2 = c->delj4;
+      TRY(xpass<X_C2R2_CORR>(c, a));
+      return correlation_tail(c, nullptr, nullptr);
+    };
+    auto fused = [](he_ctx_t* c) -> int { return poten_fused(c, nullptr, nullptr); };
+    float ts = 0.0f, tf = 0.0f;
+    st = timed(sep, &ts);
+    if (st == HE_OK) st = timed(fused, &tf);
+    if (st == HE_OK) {
+      char line[128];
+      snprintf(line, sizeof line, "field separate passes: %.2f us\nfield x-y fused: %.2f us\n",
+               1e3f * ts / 3.0f, 1e3f * tf / 3.0f);
+      ctx->tune_log += line;
+      ctx->xyfuse = tf < ts;
     }
   }
   cudaEventDestroy(e0);
@@ -2434,6 +2512,7 @@ int he_poten(he_ctx_t* ctx) {
     if (ctx->otc) TRY(term_alfa(ctx));  // He_statics/poten.f90:86-91 (denalf from the refresh)
     return correlation_tail(ctx, nullptr, ctx->otc ? ctx->ualphas : nullptr);
   }
+  if (ctx->xyfuse && !ctx->otc) return poten_fused(ctx, nullptr, nullptr);
   TRY(spectrum_cg_lj(ctx));
   XArgs a = xargs(ctx);
   a.specA = ctx->wA; a.specB = ctx->wB;
@@ -2996,6 +3075,11 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
       if (variant && !ctx->mixed) return fail(ctx, HE_ERR_ARG, "the register z pass is built for HE_PREC_MIXED");
       ctx->zreg = variant != 0;
       ctx->tile_z = tile;
+      return HE_OK;
+    case 9:
+      if (variant && !xy_fusable(ctx))
+        return fail(ctx, HE_ERR_ARG, "fused x-y passes need HE_PREC_MIXED and nx = ny in {64, 96, 128}");
+      ctx->xyfuse = variant != 0;
       return HE_OK;
     default:
       if (pass >= 3 && pass < 9) {  // one x mode (XMode pass - 3)

@@ -296,7 +296,9 @@ int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
  * transform), 2 = z (variant 0 shared-memory Stockham, 1 register transform, HE_PREC_MIXED only),
  * 3 + m = the x pass of one mode m only (0 R2C of den, 1 R2C of the statics correlation source,
  * 2 C2R of two spectra, 3 the same plus the correlation R2C, 4 C2R + pot4, 5 C2R of one
- * spectrum); tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
+ * spectrum), 9 = the classical field evaluation with fused x-y plane passes (variant 1) or
+ * separate passes (0; HE_PREC_MIXED, nx = ny in {64, 96, 128}, tile ignored but checked);
+ * tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
  * counterpart in the reference. */
 int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);

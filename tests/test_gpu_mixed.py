@@ -157,6 +157,27 @@ def test_mixed_quantum_field_formats_round_trip():
         assert np.allclose(denx, np.sum(np.abs(z) ** 2, axis=-1), rtol=1e-6)
 
 
+@pytest.mark.parametrize("n", [64, 96, 128])
+def test_mixed_fused_xy_passes_match_f64(n):
+    """The plane-fused field evaluation (fft_xy.cuh) against the FP64 fields, and a few steps of
+    it against the separate passes."""
+    w = workload(n)
+    den = C.woods_saxon(w)
+    out = {}
+    for prec, fused in (("f64", None), ("mixed", 1), ("mixed", 0)):
+        with Context(w, precision=prec) as ctx:
+            if fused is not None:
+                ctx.set_fft_variant("xy", fused, 8)
+            ctx.upload("den", den)
+            ctx.poten()
+            out[(prec, fused)] = {k: ctx.download(k) for k in ("pot4", "dencg", "delj4", "fden")}
+    for k, b in {"pot4": 2e-6, "dencg": 2e-6, "delj4": 2e-6, "fden": 2e-6}.items():
+        r = rel(out[("mixed", 1)][k], out[("f64", None)][k])
+        assert 1e-12 < r < b, (k, r)
+        r2 = rel(out[("mixed", 1)][k], out[("mixed", 0)][k])
+        assert r2 < b, (k, r2)
+
+
 @pytest.mark.parametrize("zvar,tile", [(0, 8), (1, 8), (1, 16)])
 def test_mixed_fft_variants_agree(zvar, tile):
     """Each z-pass variant of the binary32 chain (shared-memory Stockham, register transform)
