@@ -62,3 +62,30 @@ def test_snapshot_restore_round_trip(tmp_path):
         e_b = b.energy()
     for k in ("etot4", "ekin4", "elj4", "ecor4", "eHeX"):
         assert abs(e_b[k] - e_a[k]) <= 1e-12 * max(abs(e_a[k]), 1.0), k
+
+
+def test_mixed_observables_and_restart(tmp_path):
+    """The mixed path (HE_PREC_MIXED): observables from the binary32 psi plane and den against the
+    FP64 run of the same trajectory, and a snapshot restored into a fresh mixed context (psi
+    travels as binary64 text and is split into the pair again)."""
+    w, psi = moving_droplet()
+    obs = {}
+    p = tmp_path / "psi_mixed.restart"
+    for prec in ("f64", "mixed"):
+        with Context(w, precision=prec) as ctx:
+            D.dynamics_setup(ctx, psi, w.n_imp)
+            for it in range(1, 6):
+                D.dynamics_iteration(ctx, it, w.deltat, w.n_imp)
+            obs[prec] = ctx.observables(w.n4)
+            if prec == "mixed":
+                K.snapshot(ctx, p, w.n4, iteration=5, time_ps=5 * w.deltatps)
+                psi_m, e_m = ctx.download("psi"), ctx.energy()
+    for k, r in obs["f64"].items():
+        assert abs(obs["mixed"][k] - r) <= 1e-5 * max(abs(r), 1.0), (k, obs["mixed"][k], r)
+    with Context(w, precision="mixed") as b:
+        K.restore(b, p)
+        b.potenimp()
+        b.poten()
+        back = b.download("psi")
+        assert np.max(np.abs(back - psi_m)) <= 2.0 ** -44 * np.max(np.abs(psi_m))
+        assert abs(b.energy()["etot"] - e_m["etot"]) <= 1e-6 * abs(e_m["etot"])
