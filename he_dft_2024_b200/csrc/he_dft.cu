@@ -12,6 +12,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <mutex>
+#include <tuple>
 
 #include "../../include/he_dft.h"
 #include "common.cuh"
@@ -147,6 +149,7 @@ struct he_ctx {
   unsigned* counter = nullptr;
   double* sums = nullptr;
   double* hsum = nullptr;  // pinned host mirror of sums
+  ImpDev* himp = nullptr;  // pinned host mirror of the impurity struct
   // optional per-kernel CUDA-event timing (he_timing / he_timing_report)
   struct TRec {
     const char* name;
@@ -193,6 +196,23 @@ static int fail(he_ctx_t* c, int code, const char* fmt, ...) {
     int s_ = (expr);         \
     if (s_ != HE_OK) return s_; \
   } while (0)
+
+// Raises a kernel's dynamic shared-memory limit, once per kernel and device (the attribute
+// persists; asking the driver on every launch costs host time in the gaps after each
+// synchronising call).
+static cudaError_t set_smem_attr(const void* fn, size_t smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::vector<std::tuple<const void*, int, size_t>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto& d : done)
+    if (std::get<0>(d) == fn && std::get<1>(d) == dev && std::get<2>(d) >= smem) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done.emplace_back(fn, dev, smem);
+  return e;
+}
 
 // Launch of an FFT pass (a kernel that starts with pdl_wait_and_trigger) on the context's current
 // stream with programmatic stream serialisation.
@@ -449,8 +469,7 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
   constexpr size_t smem = stencil_smem<Op, kTX, kTY>();
   static int occ = -1;  // resident CTAs per SM of this instantiation
   if (occ < 0) {
-    CK(cudaFuncSetAttribute(k_stencil<Op, kTX, kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem));
+    CK(set_smem_attr((const void*)k_stencil<Op, kTX, kTY>, smem));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<Op, kTX, kTY>, kTX * kTY, smem));
   }
   TRY(join_aux(ctx));  // stencils read uimp / write den / reduce through the shared partials
@@ -462,8 +481,7 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
     TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
     rt = tail(ctx, slot);
   }
-  CK(cudaFuncSetAttribute(k_stencil<Op, kTX, kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)smem));
+  CK(set_smem_attr((const void*)k_stencil<Op, kTX, kTY>, smem));
   tname(ctx, Op::kname());
   k_stencil<Op, kTX, kTY><<<grid, block, smem, ctx->stream>>>(f, g, op, rt);
   LAUNCHED();
@@ -539,7 +557,7 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
                                  "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4", "fft_x_c2r"};
   if (!ctx->xpipe[MODE] || N == 0) {
     const size_t csmem = fft_smem(ctx->plx, rb, 2, sizeof(typename Cx<Rt>::T));
-    CK(cudaFuncSetAttribute(k_xpass_c<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
+    CK(set_smem_attr((const void*)k_xpass_c<MODE, N, TILE, Rt>, csmem));
     tname(ctx, names[MODE]);
     CK(launch_chain(ctx, k_xpass_c<MODE, N, TILE, Rt>, dim3((unsigned)ntiles), dim3(nthr), csmem, a));
     LAUNCHED();
@@ -552,13 +570,13 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   static size_t occ_smem = 0;
   static int occ = 0;
   if (occ_smem != smem) {
-    CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(set_smem_attr((const void*)k_xpass<MODE, N, TILE, Rt>, smem));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xpass<MODE, N, TILE, Rt>, pthr, smem));
     occ_smem = smem;
   }
   if (occ < 1) return fail(ctx, HE_ERR_STATE, "x pass: %zu bytes of shared memory do not fit an SM", smem);
   const unsigned nb = (unsigned)std::min<long>(ntiles, (long)occ * ctx->num_sms);
-  CK(cudaFuncSetAttribute(k_xpass<MODE, N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(set_smem_attr((const void*)k_xpass<MODE, N, TILE, Rt>, smem));
   tname(ctx, names[MODE]);
   CK(launch_chain(ctx, k_xpass<MODE, N, TILE, Rt>, dim3(nb), dim3(pthr), smem, a));
   LAUNCHED();
@@ -596,10 +614,10 @@ static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
     const C* tw2;
     if constexpr (sizeof(Rt) == 4) tw2 = ctx->ply.tw2f;
     else tw2 = ctx->ply.tw2;
-    CK(cudaFuncSetAttribute(k_ypass_reg<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+    CK(set_smem_attr((const void*)k_ypass_reg<N, TILE, Rt>, rsmem));
     CK(launch_chain(ctx, k_ypass_reg<N, TILE, Rt>, grid, dim3(yreg_threads(N, TILE)), rsmem, a, tw2));
   } else {
-    CK(cudaFuncSetAttribute(k_ypass<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(set_smem_attr((const void*)k_ypass<N, TILE, Rt>, smem));
     CK(launch_chain(ctx, k_ypass<N, TILE, Rt>, grid, dim3(nthr), smem, a));
   }
   LAUNCHED();
@@ -635,7 +653,7 @@ static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
     if (ctx->zreg) {  // register line transforms (fft_reg.cuh), binary32 chain
       using C = typename Cx<Rt>::T;
       const size_t rsmem = sizeof(C) * (size_t)N * TILE * (a.k2f ? 2 : 1);
-      CK(cudaFuncSetAttribute(k_zconv_reg<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+      CK(set_smem_attr((const void*)k_zconv_reg<N, TILE, Rt>, rsmem));
       dim3 grid((ctx->nxh + TILE - 1) / TILE, ctx->ny, 1);
       tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
       CK(launch_chain(ctx, k_zconv_reg<N, TILE, Rt>, grid, dim3(yreg_threads(N, TILE)), rsmem, a,
@@ -647,7 +665,7 @@ static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
-  CK(cudaFuncSetAttribute(k_zconv<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(set_smem_attr((const void*)k_zconv<N, TILE, Rt>, smem));
   tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
   CK(launch_chain(ctx, k_zconv<N, TILE, Rt>, grid, dim3(nthr), smem, a));
   LAUNCHED();
@@ -737,7 +755,7 @@ static int xy_launch(he_ctx_t* ctx, int kind, const XYArgs& a) {
   static const char* names[3] = {"fft_xy_r2c_den", "fft_xy_c2r_cg_lj_r2c_corr", "fft_xy_c2r_pot4"};
   void (*k)(XYArgs) = kind == 0 ? k_xy_r2c<N> : kind == 1 ? k_xy_c2r2_corr<N> : k_xy_c2r_pot<N>;
   const size_t smem = kind == 1 ? xy_smem_corr<N>() : xy_smem_r2c<N>();
-  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(set_smem_attr((const void*)k, smem));
   tname(ctx, names[kind]);
   CK(launch_chain(ctx, k, dim3(ctx->nz), dim3(kXYThreads), smem, a));
   LAUNCHED();
@@ -778,8 +796,11 @@ static size_t wf_elem(const he_ctx_t* ctx) {
 
 static int imp_pull(he_ctx_t* ctx, ImpDev* h) {
   TRY(join_aux(ctx));
-  CK(cudaMemcpyAsync(h, ctx->imp, sizeof(ImpDev), cudaMemcpyDeviceToHost, ctx->stream));
+  // through the pinned mirror: an asynchronous copy that the one synchronisation covers
+  ImpDev* m = ctx->himp ? ctx->himp : h;
+  CK(cudaMemcpyAsync(m, ctx->imp, sizeof(ImpDev), cudaMemcpyDeviceToHost, ctx->stream));
   TRY(sync_all(ctx));
+  if (m != h) std::memcpy(h, m, sizeof(ImpDev));
   return HE_OK;
 }
 static int imp_push(he_ctx_t* ctx, const ImpDev* h) {
@@ -1387,7 +1408,7 @@ static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a) {
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
-  CK(cudaFuncSetAttribute(k_zmix<N, TILE, Rt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(set_smem_attr((const void*)k_zmix<N, TILE, Rt>, smem));
   tname(ctx, a.nout == 0 ? "fft_z_fwd" : a.fwd_in ? "fft_z_mix_fwd" : "fft_z_mix");
   k_zmix<N, TILE, Rt><<<grid, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
@@ -2286,6 +2307,7 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   TRY(dalloc_t(ctx, &ctx->counter, 1));
   TRY(dalloc_t(ctx, &ctx->sums, S_COUNT));
   CK(cudaMallocHost(&ctx->hsum, S_COUNT * sizeof(double)));
+  if (mode == HE_MODE_DYNAMICS) CK(cudaMallocHost(&ctx->himp, sizeof(ImpDev)));
   TRY(autotune_tiles(ctx));
   TRY(sync_all(ctx));
   return HE_OK;
@@ -2297,6 +2319,7 @@ void he_ctx_destroy(he_ctx_t* ctx) {
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->hsum) cudaFreeHost(ctx->hsum);
+  if (ctx->himp) cudaFreeHost(ctx->himp);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
