@@ -164,11 +164,13 @@ def dist_env():
 
 
 def reduce_max(t, ws):
+    """Max over ranks of a per-rank time (the job time of a replicas run)."""
     if ws == 1:
         return t
     import torch
     import torch.distributed as dist
-    x = torch.tensor([t], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    x = torch.tensor([t], dtype=torch.float64, device=dev)
     dist.all_reduce(x, op=dist.ReduceOp.MAX)
     return float(x.item())
 
