@@ -146,6 +146,7 @@ def load():
         "he_tuned_tiles": (ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         "he_autotune_report": (ip, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "he_set_fft_variant": (ip, [vp, ip, ip, ip]),
+        "he_state_fingerprint": (ip, [vp, ctypes.POINTER(ctypes.c_ulonglong)]),
         "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
         "he_set_quantum_impurities": (ip, [vp, ctypes.POINTER(HeQImpurities)]),
         "he_qimp_moments": (ip, [vp, dp]),

@@ -106,6 +106,12 @@ class Context:
             code = 3 + int(pass_[1:])
         self._ck(self.L.he_set_fft_variant(self.h, code, variant, tile))
 
+    def state_fingerprint(self):
+        """Hash of the buffer relabelling, ring indices and lazy flags (he_state_fingerprint)."""
+        v = ctypes.c_ulonglong(0)
+        self._ck(self.L.he_state_fingerprint(self.h, ctypes.byref(v)))
+        return int(v.value)
+
     def autotune_report(self):
         """The FFT autotuner's trial times, one line per variant, and the x-pass variant chosen."""
         buf = ctypes.create_string_buffer(4096)

@@ -3118,6 +3118,32 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
   }
 }
 
+int he_state_fingerprint(const he_ctx_t* ctx, unsigned long long* out) {
+  if (!ctx || !out) return HE_ERR_ARG;
+  // FNV-1a over everything a step's launches depend on besides the array contents: the buffer
+  // relabelling (psi, psiold, hpsiold, scratch and the impurity wave functions' counterparts),
+  // the ring indices and the lazy-evaluation flags
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ull; }
+  };
+  const void* bufs[] = {ctx->psi, ctx->scratch, ctx->psiold[0], ctx->psiold[1], ctx->psiold[2],
+                        ctx->hpsiold[0], ctx->hpsiold[1], ctx->xscratch};
+  mix(bufs, sizeof bufs);
+  for (int i = 0; i < kMaxQImp; ++i) {
+    mix(&ctx->psix[i], sizeof(void*));
+    mix(ctx->psixold[i], sizeof ctx->psixold[i]);
+    mix(ctx->hpsixold[i], sizeof ctx->hpsixold[i]);
+  }
+  mix(ctx->ioldp, sizeof ctx->ioldp);
+  mix(ctx->ioldh, sizeof ctx->ioldh);
+  const int flags[2] = {ctx->cglj_pending ? 1 : 0, ctx->force_fresh ? 1 : 0};
+  mix(flags, sizeof flags);
+  *out = h;
+  return HE_OK;
+}
+
 int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len) {
   if (!ctx || !buf || len == 0) return HE_ERR_ARG;
   std::string t = ctx->tune_log;

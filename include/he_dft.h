@@ -301,6 +301,13 @@ int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
  * tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
  * counterpart in the reference. */
 int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
+/* A hash of the host-side state a step's launches depend on besides the arrays' contents: which
+ * buffer currently plays psi, psiold, hpsiold, the scratch (and the impurity wave functions'
+ * counterparts), the ring indices and the lazy-evaluation flags.  Steps issued from states with
+ * equal fingerprints launch the same kernels on the same buffers, so a caller that records steps
+ * into CUDA graphs can replay them once the fingerprint cycles back (the relabelling is
+ * periodic).  No counterpart in the reference. */
+int he_state_fingerprint(const he_ctx_t* ctx, unsigned long long* out);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
 /* ---- energy sums without device allocation ----
