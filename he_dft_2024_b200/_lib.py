@@ -147,6 +147,7 @@ def load():
         "he_autotune_report": (ip, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "he_set_fft_variant": (ip, [vp, ip, ip, ip]),
         "he_state_fingerprint": (ip, [vp, ctypes.POINTER(ctypes.c_ulonglong)]),
+        "he_join": (ip, [vp]),
         "he_timing_report": (ip, [vp, ctypes.POINTER(HeKernelTime), ip, ctypes.POINTER(ip)]),
         "he_set_quantum_impurities": (ip, [vp, ctypes.POINTER(HeQImpurities)]),
         "he_qimp_moments": (ip, [vp, dp]),

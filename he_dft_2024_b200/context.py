@@ -121,6 +121,10 @@ class Context:
     def synchronize(self):
         self._ck(self.L.he_synchronize(self.h))
 
+    def join(self):
+        """Join the side stream's queued work into the context's stream (no host wait)."""
+        self._ck(self.L.he_join(self.h))
+
     def set_stream(self, stream_ptr):
         self._ck(self.L.he_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
 

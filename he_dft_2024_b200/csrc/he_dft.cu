@@ -286,9 +286,15 @@ static int fork_aux(he_ctx_t* ctx) {
   CK(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
   return HE_OK;
 }
-// Stream for an impurity-state kernel (the side stream when overlapping).
+// Stream for an impurity-state kernel (the side stream when overlapping).  A side stream that
+// has been joined is forked from the main stream first, so that its work always hangs off the
+// main stream's order (and a step recorded into a CUDA graph records it).
 static cudaStream_t imp_stream(he_ctx_t* ctx) {
   if (!overlap_on(ctx)) return ctx->stream;
+  if (!ctx->aux_pending && !ctx->on_aux &&
+      (cudaEventRecord(ctx->ev_fork, ctx->stream) != cudaSuccess ||
+       cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0) != cudaSuccess))
+    return ctx->stream;  // fall back to the main stream (ordered, no overlap)
   ctx->aux_pending = true;
   return ctx->aux;
 }
@@ -2343,6 +2349,11 @@ int he_synchronize(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
   TRY(sync_all(ctx));
   return HE_OK;
+}
+
+int he_join(he_ctx_t* ctx) {
+  if (!ctx) return HE_ERR_ARG;
+  return join_aux(ctx);
 }
 
 int he_set_kernels(he_ctx_t* ctx, const double* fvlj4, const double* wcgk, const double* kalfs) {

@@ -195,6 +195,11 @@ size_t he_device_bytes(const he_ctx_t* ctx);
 /* Use an external CUDA stream (cudaStream_t); NULL selects the context's own stream. */
 int he_set_stream(he_ctx_t* ctx, void* stream);
 int he_synchronize(he_ctx_t* ctx);
+/* Orders the work this context has queued on its internal side stream (the impurity field and
+ * integrator kernels of the dynamics mode) before whatever comes next on its stream, without
+ * waiting on the host: the last call of a step recorded into a CUDA graph.  No counterpart in
+ * the reference. */
+int he_join(he_ctx_t* ctx);
 
 /* k-space kernels.  he_set_kernels uploads host arrays computed by the reference's fforma/initcg
  * (fforma.f90:11-61, initcg.f90:32-49); kalfs may be NULL unless core4 = "OTC".

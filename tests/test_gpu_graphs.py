@@ -59,3 +59,50 @@ def test_graph_cycle_replays_eager_steps(precision):
     for c in ctxs:
         c.close()
     torch.cuda.set_stream(torch.cuda.default_stream())
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_graph_cycle_replays_eager_classical_steps(precision):
+    """The classical step (impurity work forked onto the side stream and joined with he_join at
+    the end of each recorded step) replayed from a captured cycle equals the eager steps."""
+    w = C.tddft_1000(n=32)
+    w = C.replace(w, xmax=10.0, ymax=10.0, zmax=10.0, n4=300, rimp0=((0.5, -0.3, 8.0),),
+                  deltatps=2e-4)
+    den = C.woods_saxon(w)
+    psi = D.initial_wavefunction(w, den)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctxs = []
+    for _ in range(2):
+        c = Context(w, precision=precision)
+        c.set_stream(stream.cuda_stream)
+        D.dynamics_setup(c, psi, w.n_imp)
+        for it in range(1, 6):
+            D.dynamics_iteration(c, it, w.deltat, w.n_imp)
+        ctxs.append(c)
+    eager, graphed = ctxs
+    graphed.join()  # pending side-stream work of the eager steps, outside the recording
+    start = graphed.state_fingerprint()
+    graphs = []
+    for _ in range(64):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+            D.dynamics_iteration(graphed, 6, w.deltat, w.n_imp)
+            graphed.join()
+        graphs.append(g)
+        if graphed.state_fingerprint() == start:
+            break
+    assert graphed.state_fingerprint() == start, "no cycle within 64 steps"
+    for rep in range(2):
+        for g in graphs:
+            g.replay()
+    for k in range(2 * len(graphs)):
+        D.dynamics_iteration(eager, 6 + k, w.deltat, w.n_imp)
+    torch.cuda.synchronize()
+    for name in ("psi", "den", "pot4", "rimp", "vimp"):
+        assert np.array_equal(graphed.download(name), eager.download(name)), name
+    assert graphed.energy()["etot"] == eager.energy()["etot"]
+    del graphs
+    for c in ctxs:
+        c.close()
+    torch.cuda.set_stream(torch.cuda.default_stream())
