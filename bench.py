@@ -8,7 +8,9 @@ droplet is a seeded synthetic Woods-Saxon profile (no reference data ships); the
 iterations (RK-Gill start) run before the timed region, as in the reference driver.
 
 value     device time (CUDA events on the context's stream) for K steps with all state resident
-          in HBM; the per-step working set (~0.45 GB) exceeds L2 (126 MB).
+          in HBM; the per-step working set (~0.45 GB) exceeds L2 (126 MB).  The steps are
+          replayed from CUDA graphs (one per step of the ring buffers' relabelling cycle;
+          --no-graph launches them one by one).
 e2e       the same K steps through the C-ABI the way the Fortran driver calls it every iteration:
           steppc returning errHe/errimp/errvimp to the host, forceimp returning F to the host,
           aimp = F/m computed on the host and uploaded, rimp/vimp read back for the per-step
@@ -17,6 +19,13 @@ roofline  the kernel with the largest share of device time, its algorithmic byte
           (every input field read once, every output written once) over its mean CUDA-event time.
 cpu_baseline  the CPU oracle (C++ restatement, OpenMP on all host cores) on the identical
           128^3 state copied from the device, a bounded sample of driver iterations.
+mixed     the same workload in the mixed-precision path (HE_PREC_MIXED), timed the same way, with
+          its per-kernel breakdown and its E/N, rho L2 norm and impurity z compared with the
+          binary64 run after 2000 driver iterations (--no-mixed skips it).
+
+Other lines: --precision mixed (the timed line in the mixed path), --n 256 (4He_5000 on 256^3),
+--workload quantum (16 trajectories with a quantum impurity on 192^3, graph-replayed batch
+steps), --workload serving (a Poisson stream of trajectory requests under continuous batching).
 
 --impl reference times that CPU oracle alone on the same workload (the reference Fortran cannot be
 built in this image: no Fortran compiler, no FFTW).  Multi-GPU (torchrun): independent replicas,
