@@ -25,7 +25,8 @@ mixed     the same workload in the mixed-precision path (HE_PREC_MIXED), timed t
 
 Other lines: --precision mixed (the timed line in the mixed path), --n 256 (4He_5000 on 256^3),
 --workload quantum (16 trajectories with a quantum impurity on 192^3, graph-replayed batch
-steps), --workload serving (a Poisson stream of trajectory requests under continuous batching).
+steps), --workload serving (a Poisson stream of trajectory requests under continuous batching),
+--workload statics (the imaginary-time 4He_500 droplet on 64^3).
 
 --impl reference times that CPU oracle alone on the same workload (the reference Fortran cannot be
 built in this image: no Fortran compiler, no FFTW).  Multi-GPU (torchrun): independent replicas,
@@ -717,6 +718,77 @@ def run_quantum(args):
         print(json.dumps(line), flush=True)
 
 
+METRIC_S = "imaginary-time grid-pt-iterations/s (FP64, 64^3 statics, 4He_500)"
+
+
+def run_statics(args):
+    """The statics workload (He_statics, BCN4HeDFT.f90:1113-1160): 4He_500 on 64^3 (h = 0.7 A),
+    imaginary-time steppcr iterations with derden, fden, dencg and poten after each.  The
+    chemical potential comes back to the host every iteration (steppcr's in/out argument), as
+    in the reference driver, so the time is host-observed: CUDA events bracket the loop
+    including those round trips.  cpu_baseline: the oracle on the host cores, same iterations."""
+    import torch
+    from he_dft_2024_b200 import config as C, driver as D
+    from he_dft_2024_b200.context import Context
+    from oracle import oracle as O
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    w = C.statics_500()
+    N = w.n
+    den0 = C.woods_saxon(w)
+    dt = w.deltat_statics
+    with Context(w, mode="statics") as ctx:
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx.set_stream(stream.cuda_stream)
+        mu = D.statics_setup(ctx, den0, w.n4)
+        it = 1
+        for _ in range(max(args.warmup, 5)):  # the 4 RK iterations and the first PMC ones
+            mu, _ = D.statics_iteration(ctx, it, dt, mu, w.n4)
+            it += 1
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                mu, err = D.statics_iteration(ctx, it, dt, mu, w.n4)
+                it += 1
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        secs = reduce_max(ev0.elapsed_time(ev1) / 1e3, ws)
+        e = ctx.energy()
+    value = N * args.steps * ws / secs
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        o = O.Statics(w.as_dict(), nthreads=threads)
+        muo = D.statics_setup(o, den0, w.n4)
+        for k in range(1, 6):
+            muo, _ = D.statics_iteration(o, k, dt, muo, w.n4)
+        n_cpu = 20
+        t0 = time.perf_counter()
+        for k in range(6, 6 + n_cpu):
+            muo, _ = D.statics_iteration(o, k, dt, muo, w.n4)
+        tc = time.perf_counter() - t0
+        cpu = {"value": N * n_cpu / tc, "unit": "grid-pt-iterations/s", "cores": threads, "kind": "port",
+               "sample": f"{n_cpu} steppcr iterations of the same workload after its 5-iteration start"}
+    line = {
+        "metric": METRIC_S, "value": value, "unit": "grid-pt-iterations/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": max(args.warmup, 5), "ms_per_step": secs * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "h_A": w.h[0], "n4": w.n4,
+                   "deltat_imaginary": dt, "parallelism": f"replicas{ws}",
+                   "l2": "working set smaller than L2: the 64^3 statics state stays L2-resident"},
+        "mu_K": mu, "E_per_N_K": e["etot"] / w.n4, "cpu_baseline": cpu, "clocks": clk.summary(),
+        "e2e": {"value": value, "unit": "grid-pt-iterations/s", "h2d_bytes_per_step": 8,
+                "d2h_bytes_per_step": 8 * 3,
+                "note": "the loop is the driver's own: mu and its errors cross to the host every iteration"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_serving(args):
     """The serving workload: a seeded Poisson stream of trajectory requests (N log-uniform in
     [300, 10000], classical Morse impurity at U(100,500) m/s), each args.req_steps driver
@@ -822,7 +894,8 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
                     help="precision of the timed line (mixed: HE_PREC_MIXED; for the classical "
                          "workload the mixed-vs-FP64 comparison runs only with the default f64)")
-    ap.add_argument("--workload", default="classical", choices=["classical", "quantum", "serving"])
+    ap.add_argument("--workload", default="classical",
+                    choices=["classical", "quantum", "serving", "statics"])
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="quantum workload: launch the batch step's kernels one by one instead "
@@ -837,6 +910,8 @@ def main():
         run_quantum(args)
     elif args.workload == "serving" and args.impl == "ours":
         run_serving(args)
+    elif args.workload == "statics" and args.impl == "ours":
+        run_statics(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
