@@ -196,3 +196,22 @@ def test_mixed_fft_variants_agree(zvar, tile):
     for k, b in {"pot4": 2e-6, "dencg": 2e-6, "delj4": 2e-6, "fden": 2e-6}.items():
         r = rel(out["mixed"][k], out["f64"][k])
         assert 1e-12 < r < b, (k, r)
+
+
+@pytest.mark.parametrize("icon", [8, 18, 24])
+def test_mixed_boundaries_match_f64(icon):
+    """Periodic (8), antiperiodic (18) and reflecting (24) boundaries in the binary32 stencils:
+    a few driver iterations against the FP64 run."""
+    w = C.replace(workload(32), icon=icon, noise=0.05)
+    den = C.woods_saxon(w)
+    psi = D.initial_wavefunction(w, den)
+    res = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, precision=prec) as ctx:
+            D.dynamics_setup(ctx, psi, w.n_imp)
+            for it in range(1, 9):
+                D.dynamics_iteration(ctx, it, w.deltat, w.n_imp)
+            res[prec] = (ctx.download("psi"), ctx.energy()["etot"] / w.n4)
+    r = rel(res["mixed"][0], res["f64"][0])
+    assert 1e-12 < r < 1e-5, r
+    assert abs(res["mixed"][1] - res["f64"][1]) < 1e-5
