@@ -737,7 +737,7 @@ def run_statics(args):
     N = w.n
     den0 = C.woods_saxon(w)
     dt = w.deltat_statics
-    with Context(w, mode="statics") as ctx:
+    with Context(w, mode="statics", precision=args.precision) as ctx:
         stream = torch.cuda.Stream()
         torch.cuda.set_stream(stream)
         ctx.set_stream(stream.cuda_stream)
@@ -773,10 +773,10 @@ def run_statics(args):
         cpu = {"value": N * n_cpu / tc, "unit": "grid-pt-iterations/s", "cores": threads, "kind": "port",
                "sample": f"{n_cpu} steppcr iterations of the same workload after its 5-iteration start"}
     line = {
-        "metric": METRIC_S, "value": value, "unit": "grid-pt-iterations/s", "n_gpus": ws,
+        "metric": METRIC_S if args.precision == "f64" else METRIC_S.replace("FP64", "mixed"), "value": value, "unit": "grid-pt-iterations/s", "n_gpus": ws,
         "steps": args.steps, "warmup": max(args.warmup, 5), "ms_per_step": secs * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f32x2" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "h_A": w.h[0], "n4": w.n4,
                    "deltat_imaginary": dt, "parallelism": f"replicas{ws}",
                    "l2": "working set smaller than L2: the 64^3 statics state stays L2-resident"},

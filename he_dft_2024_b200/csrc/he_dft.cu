@@ -881,6 +881,8 @@ static int field_ref(he_ctx_t* ctx, int field, FieldRef* r) {
 enum FieldFmt { FMT_F64 = 0, FMT_R32 = 1, FMT_C32 = 2, FMT_HL = 3 };
 static FieldFmt field_fmt(const he_ctx_t* ctx, int field) {
   if (!ctx->mixed) return FMT_F64;
+  if (ctx->mode == HE_MODE_STATICS && field == HE_F_PC) return FMT_HL;  // holds sto1 (full size)
+  if (field == HE_F_HPSI) return FMT_R32;
   switch (field) {
     case HE_F_PSI: case HE_F_PSIOLD1: case HE_F_PSIOLD2: case HE_F_PSIOLD3: return FMT_HL;
     case HE_F_PC: case HE_F_Q: case HE_F_HPSIOLD1: case HE_F_HPSIOLD2: case HE_F_FDEN: return FMT_C32;
@@ -1070,6 +1072,124 @@ __global__ void __launch_bounds__(256) k_varmu(const double* hpsi, const double*
   reduce_tail<1>(rt, gridDim.x);
 }
 
+// ---- statics in the mixed path ------------------------------------------------------------------
+// psi, psiold, the corrector's output and pc (which carries the full-size prediction sto1) are
+// compensated binary32 pairs: hi plane [0, N), lo plane [N, 2N) of the 8N-byte buffer; H psi, q,
+// hpsiold, timec, den are binary32.  The pointwise imaginary-time updates below do their few
+// operations per point in binary64 on that storage; the norm, mu and error sums are binary64.
+HE_D double ld_pair(const float* b, long i, long N) { return (double)b[i] + (double)b[N + i]; }
+HE_D void st_pair(float* b, long i, long N, double v) {
+  const float h = (float)v;
+  b[i] = h;
+  b[N + i] = (float)(v - (double)h);
+}
+struct StatPWM {
+  long N;
+  double dxyz, n4, dt, dtmin, sdmu, dmumax;
+  const double* sums;
+  const float* psi;  // pair
+  float* out;        // pair
+  float* po3;        // pair
+  const float* po2;  // pair
+  const float* h1;
+  float* h2;
+  float* pc;         // pair
+  float* q;
+  float* hsave;
+  const float* hpsi;
+  float* timec;
+  double a, b, c;
+  int jr;
+};
+HE_D double local_dt_m(double hp, double ps, const StatPWM& s) {
+  return s.dt / (1.0 + exp((fabs(hp / ps) - s.dmumax) / s.sdmu)) + s.dtmin;
+}
+__global__ void __launch_bounds__(256) k_stat_predict_m(const StatPWM s, const ReduceTail rt) {
+  const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
+  const double hmean = s.sums[S_STAT_H] * s.dxyz / s.n4;
+  double acc[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < s.N; i += (long)gridDim.x * blockDim.x) {
+    const double ps = ld_pair(s.psi, i, s.N), hp = s.hpsi[i];
+    const double tc = local_dt_m(hp, ps, s);
+    s.timec[i] = (float)tc;
+    const double s4 = -(hp - hmean * ps);
+    const double sto1 = ld_pair(s.po3, i, s.N) + c4o3 * tc * (2.0 * s4 - (double)s.h1[i] + 2.0 * (double)s.h2[i]);
+    const double pn = sto1 - c112 * ld_pair(s.pc, i, s.N);
+    st_pair(s.po3, i, s.N, pn);
+    st_pair(s.pc, i, s.N, sto1);
+    s.h2[i] = (float)s4;
+    acc[0] += pn * pn;
+  }
+  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
+  reduce_tail<1>(rt, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_stat_correct_m(const StatPWM s, const ReduceTail rt) {
+  const double c9 = 9.0 / 121.0;
+  const double mu = s.sums[S_STAT_MU] * s.dxyz / s.n4;
+  double acc[2] = {0.0, 0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < s.N; i += (long)gridDim.x * blockDim.x) {
+    const double ps = ld_pair(s.psi, i, s.N);
+    const double s4 = -((double)s.hpsi[i] - mu * ps);
+    const double s5 = 0.125 * (9.0 * ld_pair(s.po3, i, s.N) - ld_pair(s.po2, i, s.N) +
+                               3.0 * (double)s.timec[i] * (s4 + 2.0 * (double)s.h1[i] - (double)s.h2[i]));
+    const double p = ld_pair(s.pc, i, s.N) - s5;
+    st_pair(s.pc, i, s.N, p);
+    const double o = s5 + c9 * p;
+    st_pair(s.out, i, s.N, o);
+    acc[0] += fabs(p);
+    acc[1] += o * o;
+  }
+  block_reduce_store<2>(acc, rt.partials + 2 * blockIdx.x);
+  reduce_tail<2>(rt, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_stat_rk_m(const StatPWM s, const ReduceTail rt) {
+  const double err = s.sums[S_STAT_H] * s.dxyz / s.n4;
+  double acc[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < s.N; i += (long)gridDim.x * blockDim.x) {
+    const double ps = ld_pair(s.psi, i, s.N), hp = s.hpsi[i];
+    if (s.jr == 0) s.timec[i] = (float)local_dt_m(hp, ps, s);
+    const double tc = s.timec[i];
+    const double s4 = -(hp - err * ps);
+    const double qq = s.q[i];
+    const double s1 = s.a * (s4 - s.b * qq);
+    s.q[i] = (float)(qq + 3.0 * s1 - s.c * s4);
+    if (s.hsave) s.hsave[i] = (float)s4;
+    const double o = ps + tc * s1;
+    st_pair(s.out, i, s.N, o);
+    acc[0] += o * o;
+  }
+  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
+  reduce_tail<1>(rt, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_stat_normalize_m(float* psi, float* den, long N,
+                                                          const double* sums, double n4, double dxyz) {
+  const double cnorm = sqrt(n4 / (sums[S_STAT_N] * dxyz));
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double v = fabs(ld_pair(psi, i, N)) * cnorm;
+    st_pair(psi, i, N, v);
+    den[i] = (float)(v * v);
+  }
+}
+__global__ void __launch_bounds__(256) k_sumsq_m(const float* psi, long N, const ReduceTail rt) {
+  double acc[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double v = ld_pair(psi, i, N);
+    acc[0] += v * v;
+  }
+  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
+  reduce_tail<1>(rt, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_varmu_m(const float* hpsi, const float* psi, long N, double mu,
+                                                 const ReduceTail rt) {
+  double acc[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double v = ld_pair(psi, i, N);
+    acc[0] += fabs((double)hpsi[i] - mu * v) * v;
+  }
+  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
+  reduce_tail<1>(rt, gridDim.x);
+}
+
 __global__ void k_copy_slot(double* sums, int dst, int src) {
   if (threadIdx.x == 0 && blockIdx.x == 0) sums[dst] = sums[src];
 }
@@ -1122,7 +1242,25 @@ static StatPW statpw(he_ctx_t* ctx, double dt, int n4) {
   return s;
 }
 
+static StatPWM statpwm(he_ctx_t* ctx, double dt, int n4) {
+  StatPWM s{};
+  s.N = ctx->N;
+  s.dxyz = ctx->dxyz;
+  s.n4 = (double)n4;
+  s.dt = dt;
+  s.dtmin = 1.0e-10; s.sdmu = 1.0e-1; s.dmumax = 1.0e2;  // He_statics/modules.f90:299
+  s.sums = ctx->sums;
+  s.timec = (float*)ctx->timec;
+  return s;
+}
 static int stat_hpsi(he_ctx_t* ctx, double* out, int slot) {
+  if (ctx->mixed) {  // binary32 stencil on psi's hi plane
+    OpHpsiRT<float> op{};
+    op.s8[0] = (const float*)ctx->pot4;
+    op.out = (float*)out;
+    op.h2o2m = (float)ctx->fn.h2o2m4;
+    return run_stencil_red(ctx, ctx->g2, (const float*)ctx->psi, op, slot);
+  }
   OpHpsiR op{};
   op.s8[0] = ctx->pot4;
   op.out = out;
@@ -1132,8 +1270,12 @@ static int stat_hpsi(he_ctx_t* ctx, double* out, int slot) {
 
 static int stat_normalize(he_ctx_t* ctx, int n4) {
   tname(ctx, "statics_normalize");
-  k_stat_normalize<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
-                                                            ctx->sums, (double)n4, ctx->dxyz);
+  if (ctx->mixed)
+    k_stat_normalize_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((float*)ctx->psi, (float*)ctx->den,
+                                                                ctx->N, ctx->sums, (double)n4, ctx->dxyz);
+  else
+    k_stat_normalize<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
+                                                              ctx->sums, (double)n4, ctx->dxyz);
   LAUNCHED();
   return HE_OK;
 }
@@ -2170,8 +2312,6 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS && mode != HE_MODE_QUANTUM)
     bad(HE_ERR_ARG, "unknown mode");
   else if (precision != HE_PREC_F64 && precision != HE_PREC_MIXED) bad(HE_ERR_ARG, "unknown precision");
-  else if (precision == HE_PREC_MIXED && mode == HE_MODE_STATICS)
-    bad(HE_ERR_ARG, "HE_PREC_MIXED is built for the real-time modes");
   else if (precision == HE_PREC_MIXED && std::strncmp(fun->core4, "OTC", 3) == 0)
     bad(HE_ERR_ARG, "HE_PREC_MIXED does not cover core4='OTC'");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
@@ -2827,6 +2967,14 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
     op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
     op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
     TRY(run_stencil_red(ctx, ctx->g1, (const double2*)ctx->psi, op, S_EN));
+  } else if (ctx->mixed) {  // statics, binary32 fields and psi's hi plane
+    OpEnergy<float> op{};
+    op.s8[0] = (const float*)ctx->den; op.s8[1] = (const float*)ctx->dencg;
+    op.s8[2] = (const float*)ctx->delj4; op.s8[3] = (const float*)ctx->den;
+    op.has_u = 0;
+    op.aux1 = 0.5 * ctx->fn.cp4; op.aux2 = (1.0 / 3.0) * ctx->fn.cpp4;
+    op.beta = ctx->fn.beta; op.den_m = ctx->fn.den_m; op.lsolid = ctx->fn.lsolid;
+    TRY(run_stencil_red(ctx, ctx->g1, (const float*)ctx->psi, op, S_EN));
   } else {
     OpEnergy<double> op{};
     op.s8[0] = ctx->den; op.s8[1] = ctx->dencg; op.s8[2] = ctx->delj4; op.s8[3] = ctx->den;
@@ -2906,7 +3054,8 @@ int he_refresh_density(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
   if (!ctx->kernels_ok) return fail(ctx, HE_ERR_STATE, "k-space kernels not set");
-  TRY(he_derden(ctx));
+  // (the gradients feed only the alpha_s term, which the mixed path does not cover)
+  if (!ctx->mixed) TRY(he_derden(ctx));
   TRY(spectrum_cg_lj(ctx));
   XArgs a = xargs(ctx);
   a.specA = ctx->wA; a.specB = ctx->wB;
@@ -2925,7 +3074,10 @@ int he_evolo0(he_ctx_t* ctx, double* mu4, double* mu4err, int n4) {
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
   TRY(stat_hpsi(ctx, ctx->hpsi, S_STAT_H));
   tname(ctx, "statics_sumsq");
-  k_sumsq<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double*)ctx->psi, ctx->N, tail(ctx, S_STAT_N));
+  if (ctx->mixed)
+    k_sumsq_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const float*)ctx->psi, ctx->N, tail(ctx, S_STAT_N));
+  else
+    k_sumsq<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double*)ctx->psi, ctx->N, tail(ctx, S_STAT_N));
   LAUNCHED();
   TRY(stat_normalize(ctx, n4));
   TRY(read_sums(ctx));
@@ -2949,16 +3101,29 @@ int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
       k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H);
       LAUNCHED();
     }
-    StatPW s = statpw(ctx, deltat, n4);
-    s.psi = (double*)ctx->psi;
-    s.hpsi = ctx->hpsi;
-    s.q = (double*)ctx->q;
-    s.out = (double*)(jr == 0 ? ctx->psiold[2] : ctx->scratch);
-    s.hsave = jr == 0 ? (double*)ctx->hpsiold[1] : nullptr;
-    s.a = arun[jr]; s.b = brun[jr]; s.c = crun[jr];
-    s.jr = jr;
-    tname(ctx, "statics_rk_update");
-    k_stat_rk<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+    if (ctx->mixed) {
+      StatPWM s = statpwm(ctx, deltat, n4);
+      s.psi = (const float*)ctx->psi;
+      s.hpsi = (const float*)ctx->hpsi;
+      s.q = (float*)ctx->q;
+      s.out = (float*)(jr == 0 ? ctx->psiold[2] : ctx->scratch);
+      s.hsave = jr == 0 ? (float*)ctx->hpsiold[1] : nullptr;
+      s.a = arun[jr]; s.b = brun[jr]; s.c = crun[jr];
+      s.jr = jr;
+      tname(ctx, "statics_rk_update_f32");
+      k_stat_rk_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+    } else {
+      StatPW s = statpw(ctx, deltat, n4);
+      s.psi = (double*)ctx->psi;
+      s.hpsi = ctx->hpsi;
+      s.q = (double*)ctx->q;
+      s.out = (double*)(jr == 0 ? ctx->psiold[2] : ctx->scratch);
+      s.hsave = jr == 0 ? (double*)ctx->hpsiold[1] : nullptr;
+      s.a = arun[jr]; s.b = brun[jr]; s.c = crun[jr];
+      s.jr = jr;
+      tname(ctx, "statics_rk_update");
+      k_stat_rk<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+    }
     LAUNCHED();
     if (jr == 0) {
       void* o3 = ctx->psiold[2];
@@ -2986,7 +3151,20 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
   if (!ctx || !mu4 || !mu4err) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
   TRY(stat_hpsi(ctx, ctx->hpsi, S_STAT_H));
-  {
+  if (ctx->mixed) {
+    StatPWM s = statpwm(ctx, deltat, n4);
+    s.psi = (const float*)ctx->psi;
+    s.hpsi = (const float*)ctx->hpsi;
+    s.po3 = (float*)ctx->psiold[ctx->ioldp[2] - 1];
+    s.h1 = (const float*)ctx->hpsiold[ctx->ioldh[0] - 1];
+    s.h2 = (float*)ctx->hpsiold[ctx->ioldh[1] - 1];
+    s.pc = (float*)ctx->pc;
+    tname(ctx, "statics_predict_f32");
+    k_stat_predict_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+    LAUNCHED();
+    std::swap(ctx->psi, ctx->psiold[ctx->ioldp[2] - 1]);
+    std::swap(ctx->ioldh[0], ctx->ioldh[1]);
+  } else {
     StatPW s = statpw(ctx, deltat, n4);
     s.psi = (double*)ctx->psi;
     s.hpsi = ctx->hpsi;
@@ -3003,7 +3181,22 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
   TRY(stat_normalize(ctx, n4));
   TRY(he_poten(ctx));
   TRY(stat_hpsi(ctx, ctx->t4, S_STAT_MU));
-  {
+  if (ctx->mixed) {
+    StatPWM s = statpwm(ctx, deltat, n4);
+    s.psi = (const float*)ctx->psi;
+    s.hpsi = (const float*)ctx->t4;
+    s.po3 = (float*)ctx->psiold[ctx->ioldp[2] - 1];
+    s.po2 = (const float*)ctx->psiold[ctx->ioldp[1] - 1];
+    s.h1 = (const float*)ctx->hpsiold[ctx->ioldh[0] - 1];
+    s.h2 = (float*)ctx->hpsiold[ctx->ioldh[1] - 1];
+    s.pc = (float*)ctx->pc;
+    s.out = (float*)ctx->scratch;
+    ReduceTail rt = tail(ctx, S_STAT_PC);
+    tname(ctx, "statics_correct_f32");
+    k_stat_correct_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, rt);
+    LAUNCHED();
+    std::swap(ctx->psi, ctx->scratch);
+  } else {
     StatPW s = statpw(ctx, deltat, n4);
     s.psi = (double*)ctx->psi;
     s.hpsi = ctx->t4;
@@ -3040,8 +3233,12 @@ int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu) {
   if (!ctx || !errmu) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
   tname(ctx, "statics_varmu");
-  k_varmu<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(ctx->hpsi, (const double*)ctx->psi, ctx->N, mu,
-                                                   tail(ctx, S_VARMU));
+  if (ctx->mixed)
+    k_varmu_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const float*)ctx->hpsi, (const float*)ctx->psi,
+                                                       ctx->N, mu, tail(ctx, S_VARMU));
+  else
+    k_varmu<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(ctx->hpsi, (const double*)ctx->psi, ctx->N, mu,
+                                                     tail(ctx, S_VARMU));
   LAUNCHED();
   TRY(read_sums(ctx));
   *errmu = ctx->hsum[S_VARMU] * ctx->dxyz / (double)npart;

@@ -646,20 +646,24 @@ static __global__ void k_imp_correct(ImpDev* g, double dt) {
 
 // ---- statics (real psi) ------------------------------------------------------------------------
 // hpsi = -(d2x+d2y+d2z)*h2o2m4 + pot4*psi; acc = sum psi*hpsi  (steppcr.f90:40-42).
-struct OpHpsiR {
-  static const char* kname() { return "statics_hpsi"; }
-  using T = double;
+// TT = float: the mixed path (binary32 hi plane of psi, binary32 pot4 and H psi; the sum in
+// binary64).
+template <typename TT>
+struct OpHpsiRT {
+  static const char* kname() { return sizeof(TT) == 4 ? "statics_hpsi_f32" : "statics_hpsi"; }
+  using T = TT;
   static constexpr int NV = 1, N8 = 1, N16 = 0;
-  const double* s8[N8];      // pot4
-  const double2* s16[1];
-  double* out;
-  double h2o2m;
-  HE_D void at(int, int, int, long i, double dx, double dy, double dz, double c, const double* v8,
-               const double2*, int, double* acc) const {
-    const double h = -((dx + dy) + dz) * h2o2m + v8[0] * c;
+  const TT* s8[N8];          // pot4
+  const typename RealOf<TT>::Z* s16[1];
+  TT* out;
+  TT h2o2m;
+  HE_D void at(int, int, int, long i, TT dx, TT dy, TT dz, TT c, const TT* v8,
+               const typename RealOf<TT>::Z*, int, double* acc) const {
+    const TT h = -((dx + dy) + dz) * h2o2m + v8[0] * c;
     out[i] = h;
-    acc[0] += c * h;
+    acc[0] += (double)c * (double)h;
   }
 };
+using OpHpsiR = OpHpsiRT<double>;
 
 }  // namespace he

@@ -38,8 +38,10 @@ typedef struct he_ctx he_ctx_t;
 /* HE_MODE_QUANTUM: real-time dynamics with quantum impurities (Dynamics_quantum_impurities):
  * complex psi plus impurity wave functions psix_i (he_set_quantum_impurities). */
 enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1, HE_MODE_QUANTUM = 2 };
-/* HE_PREC_F64: binary64 throughout.  HE_PREC_MIXED (HE_MODE_DYNAMICS and HE_MODE_QUANTUM, OT/OP
- * cores; in the quantum mode psix and psixold are pairs too, upotx / potx4 / denx binary32): the FFT chain
+/* HE_PREC_F64: binary64 throughout.  HE_PREC_MIXED (every mode, OT/OP cores; in the quantum mode
+ * psix and psixold are pairs too, upotx / potx4 / denx binary32; in the statics mode the real
+ * psi, psiold and pc are pairs, H psi binary32, and the imaginary-time updates and the norm, mu
+ * and error sums binary64): the FFT chain
  * of the mean field, the 13-point stencils and H psi run in binary32; den, pot4, dencg, delj4,
  * uimp, fden, pc, q and hpsiold are held in binary32; psi and psiold are held as compensated
  * binary32 pairs (about 48 significant bits) and updated with error-free transformations; the

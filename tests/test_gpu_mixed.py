@@ -71,8 +71,6 @@ def test_mixed_rejects_unsupported_modes():
         with pytest.raises(HeError):
             ctx.derden()
     with pytest.raises(HeError):
-        Context(w, mode="statics", precision="mixed")
-    with pytest.raises(HeError):
         Context(C.replace(w, core="OTC", lsolid=0), precision="mixed")
 
 
@@ -215,3 +213,26 @@ def test_mixed_boundaries_match_f64(icon):
     r = rel(res["mixed"][0], res["f64"][0])
     assert 1e-12 < r < 1e-5, r
     assert abs(res["mixed"][1] - res["f64"][1]) < 1e-5
+
+
+
+def test_mixed_statics_matches_f64():
+    """Imaginary time (He_statics) in the mixed path: psi, psiold and pc as compensated pairs,
+    H psi and the FFT chain in binary32, norm / mu / energy sums in binary64; 30 iterations of a
+    40^3 droplet against the FP64 run."""
+    w = C.replace(C.statics_500(), nx=40, ny=40, nz=40, xmax=14.0, ymax=14.0, zmax=14.0)
+    den0 = C.woods_saxon(w)
+    res = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, mode="statics", precision=prec) as ctx:
+            mu = D.statics_setup(ctx, den0, w.n4)
+            for it in range(1, 31):
+                mu, err = D.statics_iteration(ctx, it, w.deltat_statics, mu, w.n4)
+            den = ctx.download("den")
+            res[prec] = (mu, ctx.energy()["etot"] / w.n4, np.sqrt(np.sum(den * den)),
+                         ctx.varmu(w.n4, mu), ctx.download("psi"))
+    m, f = res["mixed"], res["f64"]
+    assert abs(m[0] - f[0]) < 1e-5 * abs(f[0]), (m[0], f[0])       # mu
+    assert abs(m[1] - f[1]) < 1e-5, (m[1], f[1])                  # E/N, K
+    assert abs(m[2] - f[2]) < 1e-6 * f[2]                         # rho L2
+    assert 1e-12 < rel(m[4], f[4]) < 1e-5
