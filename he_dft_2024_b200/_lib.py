@@ -141,6 +141,7 @@ def load():
         "he_evolo0": (ip, [vp, dp, dp, ip]),
         "he_steprkr": (ip, [vp, d, dp, dp, ip]),
         "he_steppcr": (ip, [vp, d, dp, dp, ip, dp]),
+        "he_statics_iterations": (ip, [vp, ip, d, dp, dp, ip, dp]),
         "he_varmu": (ip, [vp, ip, d, dp]),
         "he_timing": (ip, [vp, ip]),
         "he_tuned_tiles": (ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),

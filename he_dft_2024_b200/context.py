@@ -297,6 +297,15 @@ class Context:
         self.errpc = p.value
         return m.value, e.value
 
+    def statics_iterations(self, niter, deltat, mu4, n4):
+        """niter passes of steppcr + refresh_density + poten with one host read at the end
+        (he_statics_iterations); returns (mu4, mu4err) of the last pass, errpc in self.errpc."""
+        m, e, p = ctypes.c_double(mu4), ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._ck(self.L.he_statics_iterations(self.h, niter, deltat, ctypes.byref(m),
+                                              ctypes.byref(e), n4, ctypes.byref(p)))
+        self.errpc = p.value
+        return m.value, e.value
+
     def varmu(self, npart, mu):
         e = ctypes.c_double(0.0)
         self._ck(self.L.he_varmu(self.h, npart, mu, ctypes.byref(e)))

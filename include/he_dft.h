@@ -278,6 +278,17 @@ int he_evolo0(he_ctx_t* ctx, double* mu4, double* mu4err, int n4);
 /* steprkr / steppcr (He_statics/steprkr.f90:1-96, steppcr.f90:1-108). errpc may be NULL. */
 int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4);
 int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4, double* errpc);
+/* niter passes of the statics loop body with Lrkpc and ppot = 1 (BCN4HeDFT.f90:1120-1160):
+ * steppcr, derden, fftfw(den,fden), dencg, poten -- what he_steppcr, he_refresh_density and
+ * he_poten called niter times do, with the host reading the sums once at the end instead of
+ * after every pass (the reference reads mu4 only where it prints, every pener iterations).
+ * mu4, mu4err and errpc (may be NULL) are those of the last pass.  The passes run as CUDA
+ * graphs, one per buffer relabelling (the ring repeats after 30 passes), captured on first use
+ * after one eager pass and dropped when the k-space kernels or FFT variants change; with
+ * he_timing on they run eagerly.  No counterpart call in the reference: it replaces the loop
+ * body between two energy evaluations. */
+int he_statics_iterations(he_ctx_t* ctx, int niter, double deltat, double* mu4, double* mu4err, int n4,
+                          double* errpc);
 /* varmu(npart,mu,errmu): He_statics/varmu.f90:31. */
 int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu);
 

@@ -106,3 +106,45 @@ def test_graph_cycle_replays_eager_classical_steps(precision):
     for c in ctxs:
         c.close()
     torch.cuda.set_stream(torch.cuda.default_stream())
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_statics_iterations_match_per_iteration_calls(precision):
+    """he_statics_iterations (passes replayed from per-relabelling graphs, one host read at the
+    end) against the driver's own per-iteration steppcr + refresh + poten calls: identical
+    mu, mu4err, errpc and fields after 46 passes, i.e. past one 30-pass relabelling cycle."""
+    w = C.statics_500()  # 64^3
+    den0 = C.woods_saxon(w)
+    dt = w.deltat_statics
+    out = []
+    for batched in (False, True):
+        with Context(w, mode="statics", precision=precision) as ctx:
+            ctx.set_fft_variant("x", 0, 8)  # both contexts on the same kernels
+            ctx.set_fft_variant("y", 1, 8)
+            ctx.set_fft_variant("z", 0, 8)
+            mu = D.statics_setup(ctx, den0, w.n4)
+            it = 1
+            for _ in range(5):  # the 4 RK iterations and the first predictor-corrector one
+                mu, _ = D.statics_iteration(ctx, it, dt, mu, w.n4)
+                it += 1
+            l0 = ctx.launches
+            if batched:
+                mu, err = ctx.statics_iterations(1, dt, mu, w.n4)    # the eager first pass
+                mid = ctx.statics_iterations(44, dt, mu, w.n4)       # captures the cycle, replays
+                mu, err = ctx.statics_iterations(1, dt, mid[0], w.n4)
+            else:
+                for k in range(46):
+                    mu, err = D.statics_iteration(ctx, it, dt, mu, w.n4)
+                    it += 1
+                    if k == 44:
+                        mid = (mu, err)
+            out.append((mu, err, ctx.errpc, ctx.download("psi"), ctx.download("den"),
+                        ctx.download("pot4"), ctx.launches - l0, mid))
+    (mu_e, err_e, pc_e, psi_e, den_e, pot_e, l_e, mid_e) = out[0]
+    (mu_b, err_b, pc_b, psi_b, den_b, pot_b, l_b, mid_b) = out[1]
+    assert mid_b == mid_e  # mu4err of a batch from the pass before its last, kept on the device
+    assert mu_b == mu_e and err_b == err_e and pc_b == pc_e
+    assert np.array_equal(psi_b, psi_e)
+    assert np.array_equal(den_b, den_e)
+    assert np.array_equal(pot_b, pot_e)
+    assert l_b == l_e + 46  # plus the one slot copy per pass
