@@ -3292,7 +3292,22 @@ static int statics_pass_graphed(he_ctx_t* ctx, double deltat, int n4) {
     return HE_OK;
   }
   if (ctx->stat_graphs.size() >= kMaxStatGraphs) return statics_pass(ctx, deltat, n4);
+  // The capture records kernels without running them, while the pass relabels the ring on the
+  // host as it goes.  Keep the relabelling from before the capture so that a capture or an
+  // instantiation that fails leaves the context describing the buffers as they are.
+  he_ctx::StatGraph before{};
+  before.psi = ctx->psi;
+  before.scratch = ctx->scratch;
+  for (int i = 0; i < 3; ++i) { before.psiold[i] = ctx->psiold[i]; before.ioldp[i] = ctx->ioldp[i]; }
+  for (int i = 0; i < 2; ++i) { before.hpsiold[i] = ctx->hpsiold[i]; before.ioldh[i] = ctx->ioldh[i]; }
   const long long l0 = ctx->launches;
+  auto restore = [&]() {
+    ctx->psi = before.psi;
+    ctx->scratch = before.scratch;
+    for (int i = 0; i < 3; ++i) { ctx->psiold[i] = before.psiold[i]; ctx->ioldp[i] = before.ioldp[i]; }
+    for (int i = 0; i < 2; ++i) { ctx->hpsiold[i] = before.hpsiold[i]; ctx->ioldh[i] = before.ioldh[i]; }
+    ctx->launches = l0;
+  };
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
   const int rc = statics_pass(ctx, deltat, n4);
   cudaGraph_t graph = nullptr;
@@ -3300,6 +3315,7 @@ static int statics_pass_graphed(he_ctx_t* ctx, double deltat, int n4) {
   if (rc != HE_OK || ec != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
     cudaGetLastError();
+    restore();
     if (rc != HE_OK) return rc;
     return fail(ctx, HE_ERR_CUDA, "statics pass capture failed: %s", cudaGetErrorString(ec));
   }
@@ -3307,14 +3323,21 @@ static int statics_pass_graphed(he_ctx_t* ctx, double deltat, int n4) {
   g.key = key;
   const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
   cudaGraphDestroy(graph);
-  if (ei != cudaSuccess) return fail(ctx, HE_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
+  if (ei != cudaSuccess) {
+    restore();
+    return fail(ctx, HE_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
+  }
   g.psi = ctx->psi;
   g.scratch = ctx->scratch;
   for (int i = 0; i < 3; ++i) { g.psiold[i] = ctx->psiold[i]; g.ioldp[i] = ctx->ioldp[i]; }
   for (int i = 0; i < 2; ++i) { g.hpsiold[i] = ctx->hpsiold[i]; g.ioldh[i] = ctx->ioldh[i]; }
   g.launches = ctx->launches - l0;
   ctx->stat_graphs.push_back(g);
-  CK(cudaGraphLaunch(g.exec, ctx->stream));
+  const cudaError_t el = cudaGraphLaunch(g.exec, ctx->stream);
+  if (el != cudaSuccess) {
+    restore();
+    return fail(ctx, HE_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(el));
+  }
   return HE_OK;
 }
 

@@ -10,15 +10,19 @@
 //
 // The only device memory this entry point uses besides the caller's arrays is the file-scope
 // array below: per-CTA partial sums of the reduction, the completion counter and the five final
-// sums.  Its size is fixed: room for kNoAllocMaxBlocks reduction blocks of the stencil grid,
-// i.e. grids up to 256^3 (4096 blocks at 256^3); larger grids are rejected with HE_ERR_ARG.
-// Every GPU that loads the library holds these 328,000 bytes until the process exits.
+// sums.  Its size is fixed: room for kNoAllocMaxBlocks = 8192 reduction blocks of the stencil
+// grid (32 x 8 points x 16 planes each).  A 256^3 grid needs 4096 of them; grids needing more
+// than 8192 are rejected with HE_ERR_ARG.  Every GPU that loads the library holds these 328,000
+// bytes until the process exits.
+//
+// Only the OT and OP cores are accepted: for core4 = 'OTC' the reference adds the alpha_s energy
+// (Dynamics_TDDFT/energy.f90:131-135) to etot4, which needs the alpha_s fields this entry point
+// does not have, so it returns HE_ERR_ARG instead of a total without that term.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/he_dft.h"
 #include "ops.cuh"
@@ -36,35 +40,27 @@ constexpr int kScratchDoubles = kSumsSlot + 32;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// Device address of g_noalloc_scratch, resolved once per device (with that device current).
-constexpr int kMaxDevices = 64;
-double* g_scratch_addr[kMaxDevices] = {};
-std::mutex g_scratch_mutex;
-
+// Device address of g_noalloc_scratch on the current device.  In host code the array's name is
+// only a host-side stand-in, so the address is looked up with the device current.  The lookup
+// is repeated on every call (it is cheap): an address kept across calls would go stale when the
+// caller resets the device (cudaDeviceReset) and the module is loaded again.  The first call on
+// a device may load the library's device code, which is why it should come before any stream
+// capture.
 int scratch_for_current_device(double** out, char* err, size_t errlen) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    if (err && errlen) snprintf(err, errlen, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  double* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    if (err && errlen)
+      snprintf(err, errlen, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
     return HE_ERR_CUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    if (err && errlen) snprintf(err, errlen, "device index %d out of range", dev);
-    return HE_ERR_ARG;
-  }
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
-    double* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      if (err && errlen)
-        snprintf(err, errlen, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-      return HE_ERR_CUDA;
-    }
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+  *out = p;
   return HE_OK;
+}
+
+// core4 as the functional gives it: "OT " and "OP " (a trailing blank or NUL) are accepted.
+bool core_ot_or_op(const char c[4]) {
+  return c[0] == 'O' && (c[1] == 'T' || c[1] == 'P') && (c[2] == ' ' || c[2] == '\0');
 }
 
 void bickley13_rows(double w1[13]) {  // first-derivative row (newder.f:99-130, M=13, K=1)
@@ -116,6 +112,9 @@ extern "C" int he_energy_noalloc(const he_grid_t* grid, const he_functional_t* f
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return bad("grid sizes must be positive");
   if (grid->xmax == 0.0 || grid->ymax == 0.0 || grid->zmax == 0.0)
     return bad("xmax, ymax, zmax must be non-zero");
+  if (!core_ot_or_op(fun->core4))
+    return bad("core4 must be 'OT ' or 'OP ': the 'OTC' total needs the alpha_s energy, which "
+               "he_energy_noalloc does not compute (use he_energy)");
   StencilGeom g{};
   g.nx = grid->nx; g.ny = grid->ny; g.nz = grid->nz;
   g.icon = grid->icon;

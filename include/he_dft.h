@@ -336,10 +336,12 @@ int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
  * given) from the caller's device arrays psi (complex in HE_MODE_DYNAMICS, real in
  * HE_MODE_STATICS), den, dencg, delj4 and uimp (may be NULL), in the reference layout.  Calls no
  * cudaMalloc/cudaFree: the reduction scratch is a fixed 328,000-byte device array inside the
- * library (room for grids up to 256^3; larger grids return HE_ERR_ARG), held on every GPU that
- * loads the library until exit.  The first call on a device looks up that array's address (set-up
- * once per device); make the first call before any stream capture.  All calls share the array:
- * calls whose work overlaps on the GPU race.  Synchronises `stream` (cudaStream_t, NULL = default);
+ * library (room for 8192 reduction blocks of 32x8x16 points: grids up to 256^3, which need 4096;
+ * larger grids return HE_ERR_ARG), held on every GPU that loads the library until exit.  Each
+ * call looks up that array's address on the current device; the first call on a device may load
+ * the library's device code, so make it before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU race.  core4 must be "OT " or "OP " (HE_ERR_ARG for "OTC",
+ * whose etot4 includes the alpha_s energy, and for anything else).  Synchronises `stream` (cudaStream_t, NULL = default);
  * fills *out (impurity fields other than eHeX/eimpu are zero); on error writes a message to
  * err[errlen] when given. */
 int he_energy_noalloc(const he_grid_t* grid, const he_functional_t* fun, int mode,

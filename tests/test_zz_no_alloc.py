@@ -20,9 +20,9 @@ RTOL = 1e-12
 HE_KEYS = ("ekin4", "elj4", "ecor4", "esolid", "etot4")
 
 
-def _grid_fun(w):
+def _grid_fun(w, core=b"OT "):
     g = _lib.HeGrid(w.nx, w.ny, w.nz, w.xmax, w.ymax, w.zmax, w.npd, w.icon)
-    f = _lib.HeFunctional(b"OT ", w.h4, w.eps4, w.sigma4, w.cp4, w.cpp4, w.den4c, w.alphas, w.l,
+    f = _lib.HeFunctional(core, w.h4, w.eps4, w.sigma4, w.cp4, w.cpp4, w.den4c, w.alphas, w.l,
                           w.den0s, w.h2o2m4, w.lsolid, w.C, w.beta, w.den_m)
     return g, f
 
@@ -52,15 +52,31 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     assert b"256^3" in err.value
 
 
+@pytest.mark.parametrize("core", [b"OTC", b"XX "])
+def test_noalloc_refuses_cores_it_cannot_total(core):
+    """core4='OTC' adds the alpha_s energy to etot4, which this entry point does not compute; it
+    and unknown cores are refused on the host, before any device work (no GPU needed)."""
+    L = _lib.load()
+    w = C.tddft_1000(n=32)
+    g, f = _grid_fun(w, core)
+    out = _lib.HeEnergies()
+    err = ctypes.create_string_buffer(256)
+    dummy = ctypes.c_void_p(16)
+    st = L.he_energy_noalloc(ctypes.byref(g), ctypes.byref(f), _lib.HE_MODE_DYNAMICS, dummy, dummy,
+                             dummy, dummy, None, None, ctypes.byref(out), err, 256)
+    assert st == _lib.HE_ERR_ARG
+    assert b"core4" in err.value
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["dynamics", "statics"])
-def test_energy_noalloc_matches_he_energy_twice(mode):
+@pytest.mark.parametrize("mode,icon", [("dynamics", 13), ("dynamics", 18), ("statics", 13)])
+def test_energy_noalloc_matches_he_energy_twice(mode, icon):
     import torch
     from he_dft_2024_b200.context import Context
 
     if mode == "dynamics":
         w = C.replace(C.tddft_1000(n=32), xmax=20.0, ymax=20.0, zmax=20.0, n4=300,
-                      rimp0=((0.5, -0.3, 8.0),), deltatps=5e-4)
+                      rimp0=((0.5, -0.3, 8.0),), deltatps=5e-4, icon=icon)
     else:
         w = C.replace(C.statics_500(), nx=32, ny=32, nz=32, xmax=11.2, ymax=11.2, zmax=11.2)
     with Context(w, mode=mode) as ctx:
