@@ -105,3 +105,27 @@ def quantum_iteration(s, iteraux, deltat, lrk=False, errors=False):
     s.potenimp()
     s.poten()
     return err
+
+
+def statics_relax(s, den, n4, deltat, iterations, chunk=50):
+    """The statics recipe as a start state for real time: psi = sqrt(den), then `iterations`
+    imaginary-time passes (four steprkr, then steppcr; BCN4HeDFT.f90:1086-1160), after which the
+    driver writes den (printout.f90:52-69) and the dynamics reads it back (readenc.f90:90-110,
+    psi = sqrt(den)).  A device context runs the steppcr passes through he_statics_iterations,
+    `chunk` at a time.  Returns (den, mu4, mu4err)."""
+    mu = statics_setup(s, den, n4)
+    err = 0.0
+    it = 1
+    while it <= min(4, iterations):
+        mu, err = statics_iteration(s, it, deltat, mu, n4)
+        it += 1
+    while it <= iterations:
+        k = min(chunk, iterations - it + 1)
+        if hasattr(s, "statics_iterations"):
+            mu, err = s.statics_iterations(k, deltat, mu, n4)
+        else:
+            for j in range(k):
+                mu, err = statics_iteration(s, it + j, deltat, mu, n4)
+        it += k
+    out = s.download("den") if hasattr(s, "download") else s.get("den")
+    return np.asfortranarray(np.asarray(out).reshape(np.shape(den), order="F")), mu, err

@@ -49,3 +49,21 @@ def test_two_ranks_take_the_max_time():
     for rank, w, r, l, t in res:
         assert (w, r, l) == (2, rank, rank)
         assert t == pytest.approx(1.5)  # both ranks see the slowest rank's time
+
+
+def test_bench_gpus_flag_launches_that_many_ranks():
+    """`bench.py --gpus 2` started without a launcher starts itself again as two ranks with the
+    environment torchrun would give them; the reference arm (CPU only) then prints one line, from
+    rank 0, with n_gpus = 2."""
+    import json
+    import subprocess
+    env = dict(os.environ)
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--gpus", "2", "--steps", "1", "--warmup", "0", "--n", "32"],
+                       capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    assert lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
