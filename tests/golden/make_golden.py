@@ -13,7 +13,7 @@ The table values are read as text (never compiled or run), expanded to the full 
 way newder.f:99-130 does (ICON=1: the first (M*M+1)/2 entries are stored, the rest follow by the
 parity sign (-1)**K), and written with their exact binary64 value as hex.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py <path to the reference checkout>
 """
 import json
 import os
@@ -77,7 +77,9 @@ def tstgrid_sizes(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference checkout>")
+    ref = sys.argv[1]
     dyn = os.path.join(ref, "Dynamics_TDDFT")
     linked = parse_block_data(os.path.join(dyn, "mates.f"))
     copy = parse_block_data(os.path.join(dyn, "blockds.f"))
