@@ -1224,7 +1224,7 @@ static int launch_impfield_t(he_ctx_t* ctx) {
   OpImpField<NI, TT> op{};
   op.tab = ctx->pot_tab; op.imp = ctx->imp; op.uimp = (TT*)ctx->uimp;
   op.n = ctx->n_imp; op.npot = ctx->npot;
-  op.delinter = ctx->delinter; op.rmax = ctx->rmaxinterpol;
+  op.delinter = ctx->delinter; op.rmax = ctx->rmaxinterpol; op.inv_delinter = 1.0 / ctx->delinter;
   op.xmax = ctx->xmax; op.ymax = ctx->ymax; op.zmax = ctx->zmax;
   op.hx = ctx->hx; op.hy = ctx->hy; op.hz = ctx->hz;
   return run_stencil_red(ctx, ctx->g1, (const TT*)ctx->den, op, S_FORCE);

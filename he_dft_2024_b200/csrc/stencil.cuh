@@ -14,11 +14,16 @@
 // (the x and y derivatives).  While plane z is being consumed, the next plane is already in
 // flight: its halo and the consumer's pointwise operands by cp.async into the other half of
 // double-buffered shared-memory stages (the halo zero-filled outside the grid for icon=13), and
-// its z+7 column value by register prefetch.  Every field value is read from HBM once per chunk;
-// halo re-reads hit L2.
+// its z+7 column value by register prefetch.  One barrier per plane: the next plane's copies are
+// issued right after it, into the buffers every thread finished reading before reaching it.
+// Binary64 complex fields are further prefetched into L2 (stencil_l2_ahead planes beyond the
+// copies: the operand rows, and the psi rows whose column values the register prefetch reads).
+// Every field value is read from HBM once per chunk; halo re-reads hit L2.
 // The consumer ('Op') receives the three derivatives, the centre value and its staged operands
 // and does the fused pointwise work (H psi, predictor/corrector, reductions).
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace he {
@@ -123,11 +128,23 @@ __device__ void reduce_tail(const ReduceTail& rt, long nb) {
 // Minimum resident CTAs per SM for a stencil instantiation (caps registers at 64K/(256*m)).
 // (binary32 complex fields without reductions: 4, i.e. 64 registers; with binary64 reductions
 // the consumers would spill at 64, and the corrector measured faster at 3 on 256^3 grids)
+// An Op may set its own count with a static constexpr int kMinBlocks.
+template <class O, class = void>
+struct OpMinBlocks { static constexpr int v = 0; };
+template <class O>
+struct OpMinBlocks<O, std::void_t<decltype(O::kMinBlocks)>> { static constexpr int v = O::kMinBlocks; };
 template <class Op>
 constexpr int stencil_min_blocks() {
   using T = typename Op::T;
+  if constexpr (OpMinBlocks<Op>::v > 0) return OpMinBlocks<Op>::v;
   return sizeof(T) == 16 ? 2 : (sizeof(T) == 8 ? (Op::NV > 0 ? 3 : 4) : 3);
 }
+
+// Planes of L2 prefetch ahead of the shared-memory copies (0 = none): binary64 complex fields
+// only (128^3 FP64 step: corrector 106 -> 95 us, predictor 96 -> 85 us with 2; the binary32
+// stencils measured no gain).
+template <typename T>
+constexpr int stencil_l2_ahead() { return sizeof(T) == 16 ? 2 : 0; }
 
 // Dynamic shared memory of one stencil CTA: the double-buffered halo tile and the
 // double-buffered operand stages.
@@ -247,12 +264,48 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
 
+  // L2 prefetch (prefetch.global.L2, one 128-byte line per instruction, addresses inside the
+  // arrays only): the operand rows of plane iz, and the TY + 12 psi rows (x halo included) of
+  // plane iz.
+  constexpr int PF = stencil_l2_ahead<T>();
+  auto l2_lines = [](const void* base, long bytes) {
+    const char* end = static_cast<const char*>(base) + bytes;
+    for (const char* p = (const char*)((uintptr_t)base & ~(uintptr_t)127); p < end; p += 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  };
+  auto prefetch_ops = [&](int iz) {
+    if (iz >= z1) return;
+    const int nxr = min(TX, g.nx - x0);
+    for (int r = tid; r < (Op::N16 + Op::N8) * TY; r += NT) {
+      const int k = r / TY, yy = y0 + (r - k * TY);
+      if (yy >= g.ny) continue;
+      const long off = (long)x0 + (long)g.nx * (yy + (long)g.ny * iz);
+      if (k < Op::N16) l2_lines(op.s16[k] + off, (long)nxr * sizeof(Z));
+      else l2_lines(op.s8[k - Op::N16] + off, (long)nxr * sizeof(R));
+    }
+  };
+  auto prefetch_psi = [&](int iz) {
+    if (iz >= g.nz) return;
+    const int xa = max(x0 - 6, 0), xb = min(x0 + TX + 6, g.nx);
+    for (int r = tid; r < TY + 12; r += NT) {
+      const int yy = y0 - 6 + r;
+      if (yy < 0 || yy >= g.ny) continue;
+      l2_lines(f + (long)xa + (long)g.nx * (yy + (long)g.ny * iz), (long)(xb - xa) * sizeof(T));
+    }
+  };
+
   // Prologue: z-queue f(z0-6 .. z0+5), the next column value f(z0+6) and plane z0's stage.
   T q[13];
 #pragma unroll
   for (int m = 0; m < 12; ++m) q[m + 1] = column(z0 - 6 + m);
   T qn = column(z0 + 6);
   issue_plane(0, z0);
+  if (PF > 0) {
+    for (int d = 1; d <= PF; ++d) {
+      prefetch_ops(z0 + d);
+      prefetch_psi(z0 + 6 + d);
+    }
+  }
 
   for (int iz = z0; iz < z1; ++iz) {
     const int b = (iz - z0) & 1;
@@ -261,16 +314,21 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
     for (int m = 0; m < 12; ++m) q[m] = q[m + 1];
     q[12] = qn;
     // Centre of plane iz: from the queue (threads past the grid edge stage the boundary value).
+    // Buffer b was last read for plane iz-2, before the previous barrier.
     tb[(ty + 6) * (TX + 12) + tx + 6] = inside ? q[6] : load_bc(f, g, ix, iy, iz);
+    cp_async_wait<0>();
+    fix_halo_sign(b, iz);
+    __syncthreads();
+    // Plane iz+1 into buffer b^1, which every thread finished reading (plane iz-1) before the
+    // barrier above.
     if (iz + 1 < z1) {
       issue_plane(b ^ 1, iz + 1);
       qn = column(iz + 7);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
     }
-    fix_halo_sign(b, iz);
-    __syncthreads();
+    if (PF > 0) {
+      prefetch_ops(iz + 1 + PF);
+      prefetch_psi(iz + 7 + PF);
+    }
     if (inside) {
       const auto& W = stencil_w<T>(g);
       T dx = zero_of(T()), dy = zero_of(T()), dz = zero_of(T());
@@ -289,7 +347,6 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
       op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
             st16 + b * Op::N16 * NT + tid, NT, acc);
     }
-    __syncthreads();
   }
   if constexpr (Op::NV > 0) {
     const long nb = (long)gridDim.x * gridDim.y * gridDim.z;
