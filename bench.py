@@ -88,6 +88,8 @@ def kernel_bytes_per_point(nx, mixed=False):
             "fft_y": 2 * c * hk,
             "fft_z_conv1": 2 * c * hk + r * hk,
             "fft_z_conv2": c * hk + 3 * c * hk + 2 * r * hk,
+            "fft_yz_conv1": 2 * c * hk + r * hk,
+            "fft_yz_conv2": c * hk + 3 * c * hk + 2 * r * hk,
         }
     c, r = 16.0, 8.0
     return {
@@ -109,6 +111,9 @@ def kernel_bytes_per_point(nx, mixed=False):
         "fft_y": 2 * c * hk,
         "fft_z_conv1": 2 * c * hk + r * hk,
         "fft_z_conv2": c * hk + 3 * c * hk + 2 * r * hk,
+        # fused y-z convolutions (64^3): spectrum and kernel(s) in, result(s) (and fden) out
+        "fft_yz_conv1": 2 * c * hk + r * hk,
+        "fft_yz_conv2": c * hk + 3 * c * hk + 2 * r * hk,
     }
 
 
@@ -907,6 +912,66 @@ METRIC_S = "imaginary-time grid-pt-iterations/s (FP64, 64^3 statics, 4He_500)"
 PENER = 50  # statics passes between energy evaluations (BCN4HeDFT.f90:67, pener)
 
 
+def run_statics_group(args):
+    """--workload statics --droplets B: B 4He_500 droplets on 64^3 with different seeded noise,
+    grouped (he_ctx_group) so that one launch per kernel advances all of them; value: the
+    aggregate grid-pt-iterations/s of he_statics_iterations_members, PENER passes per call."""
+    import torch
+    from he_dft_2024_b200 import config as C, driver as D
+    from he_dft_2024_b200.context import Context
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    base = C.statics_500()
+    B = args.droplets
+    wl = [C.replace(base, seed=base.seed + 7 * k) for k in range(B)]
+    N, dt, n4 = base.n, base.deltat_statics, base.n4
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctxs = [Context(w, mode="statics") for w in wl]
+    lead = ctxs[0]
+    lead.set_stream(stream.cuda_stream)
+    lead.group(ctxs[1:])
+    try:
+        mu = D.statics_setup_group(lead, [C.woods_saxon(w) for w in wl], n4)
+        for it in range(1, max(args.warmup, 5) + 1):
+            mu = D.statics_iteration_group(lead, it, dt, n4)
+        mu, _, _ = lead.statics_iterations_members(1, dt, mu, n4)
+        mu, _, _ = lead.statics_iterations_members(2 * PENER, dt, mu, n4)  # graphs of the cycle
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = lead.launches
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            left = args.steps
+            while left > 0:
+                mu, err, _ = lead.statics_iterations_members(min(PENER, left), dt, mu, n4)
+                left -= PENER
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        launches = lead.launches - l0
+        secs = reduce_max(ev0.elapsed_time(ev1) / 1e3, ws)
+        es = lead.energy_members()
+    finally:
+        lead.close()
+    value = N * args.steps * B * ws / secs
+    line = {
+        "metric": METRIC_S.replace("4He_500", f"{B} x 4He_500 grouped"), "value": value,
+        "unit": "grid-pt-iterations/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 5), "ms_per_step": secs * 1e3 / args.steps,
+        "ms_per_droplet_iteration": secs * 1e3 / args.steps / B,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": base.name, "grid": [base.nx, base.ny, base.nz], "h_A": base.h[0],
+                   "n4": n4, "droplets": B, "deltat_imaginary": dt, "parallelism": f"replicas{ws}",
+                   "l2": "working set smaller than L2: the 64^3 statics states stay L2-resident"},
+        "mu_K": [float(m) for m in mu], "E_per_N_K": [e["etot"] / n4 for e in es],
+        "clocks": clk.summary(), "gpu_launches": launches, "passes_per_call": PENER,
+        "note": "one launch per kernel advances every droplet (device pointer map per member)",
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_statics(args):
     """The statics workload (He_statics, BCN4HeDFT.f90:1113-1160): 4He_500 on 64^3 (h = 0.7 A),
     imaginary-time steppcr iterations with derden, fden, dencg and poten after each.  value:
@@ -1125,6 +1190,8 @@ def main():
     ap.add_argument("--workload", default="classical",
                     choices=["classical", "quantum", "serving", "statics"])
     ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--droplets", type=int, default=1,
+                    help="statics workload: droplets advanced together as one group (he_ctx_group)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="quantum workload: launch the batch step's kernels one by one instead "
                          "of replaying captured CUDA graphs")
@@ -1147,6 +1214,8 @@ def main():
         run_quantum(args)
     elif args.workload == "serving" and args.impl == "ours":
         run_serving(args)
+    elif args.workload == "statics" and args.impl == "ours" and args.droplets > 1:
+        run_statics_group(args)
     elif args.workload == "statics" and args.impl == "ours":
         run_statics(args)
     elif args.impl == "reference":

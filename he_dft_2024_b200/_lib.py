@@ -155,6 +155,13 @@ def load():
         "he_observables": (ip, [vp, ip, dp]),
         "he_ft_v_spline_table": (ip, [ctypes.POINTER(HePairPot), d, d, ip, ip, dp, ip,
                                       ctypes.c_char_p, ctypes.c_size_t]),
+        "he_ctx_group": (ip, [ctypes.POINTER(vp), ip]),
+        "he_group_size": (ip, [vp]),
+        "he_upload_member": (ip, [vp, ip, ip, vp, ctypes.c_size_t]),
+        "he_download_member": (ip, [vp, ip, ip, vp, ctypes.c_size_t]),
+        "he_member_mu": (ip, [vp, ip, ip, dp]),
+        "he_statics_iterations_members": (ip, [vp, ip, d, ip, dp, dp, dp]),
+        "he_energy_members": (ip, [vp, ctypes.POINTER(HeEnergies)]),
         "he_energy_noalloc": (ip, [ctypes.POINTER(HeGrid), ctypes.POINTER(HeFunctional), ip, vp,
                                    vp, vp, vp, vp, vp, ctypes.POINTER(HeEnergies),
                                    ctypes.c_char_p, ctypes.c_size_t]),

@@ -58,6 +58,55 @@ class Context:
         if getattr(self, "h", None):
             self.L.he_ctx_destroy(self.h)
             self.h = None
+        for m in getattr(self, "_members", ()):
+            m.close()
+        self._members = []
+
+    # ---- groups (he_ctx_group): several statics droplets per launch ----------------------------
+    def group(self, members):
+        """Make this context the leader of itself plus `members` (contexts created alike and set
+        up on their own, in the same ring state).  The leader takes the members over: it closes
+        them when it closes, and they must not be called directly any more."""
+        hs = (ctypes.c_void_p * (1 + len(members)))(self.h, *[m.h for m in members])
+        self._ck(self.L.he_ctx_group(hs, 1 + len(members)))
+        self._members = list(members)
+
+    @property
+    def members(self):
+        return self.L.he_group_size(self.h)
+
+    def upload_member(self, m, name, arr):
+        dt = np.complex128 if self._is_complex(name) else np.float64
+        a = np.asarray(arr, dtype=dt).reshape(self._shape(name), order="F")
+        buf = np.ascontiguousarray(a.ravel(order="F"))
+        self._ck(self.L.he_upload_member(self.h, m, FIELDS[name], buf.ctypes.data_as(ctypes.c_void_p),
+                                         buf.nbytes))
+
+    def download_member(self, m, name):
+        dt = np.complex128 if self._is_complex(name) else np.float64
+        shape = self._shape(name)
+        buf = np.empty(int(np.prod(shape)), dtype=dt)
+        self._ck(self.L.he_download_member(self.h, m, FIELDS[name], buf.ctypes.data_as(ctypes.c_void_p),
+                                           buf.nbytes))
+        return buf.reshape(shape, order="F")
+
+    def member_mu(self, n4, after_rk=False):
+        out = np.zeros(self.members)
+        self._ck(self.L.he_member_mu(self.h, n4, 1 if after_rk else 0, dptr(out)))
+        return out
+
+    def statics_iterations_members(self, niter, deltat, mu4, n4):
+        """he_statics_iterations_members: (mu4, mu4err, errpc) arrays over the members."""
+        mu = np.ascontiguousarray(np.asarray(mu4, np.float64).copy())
+        err, pc = np.zeros(self.members), np.zeros(self.members)
+        self._ck(self.L.he_statics_iterations_members(self.h, niter, deltat, n4, dptr(mu), dptr(err),
+                                                      dptr(pc)))
+        return mu, err, pc
+
+    def energy_members(self):
+        out = (_lib.HeEnergies * self.members)()
+        self._ck(self.L.he_energy_members(self.h, out))
+        return [{k: getattr(e, k) for k, _ in _lib.HeEnergies._fields_} for e in out]
 
     def __del__(self):
         try:
@@ -98,10 +147,11 @@ class Context:
 
     def set_fft_variant(self, pass_, variant, tile):
         """Override the autotuner for one pass family: pass_ 'x' (every mode), 'x0'..'x5' (one
-        x mode), 'y', 'z' or 'xy' (fused plane passes of the classical field evaluation);
+        x mode), 'y', 'z', 'xy' (fused plane passes of the classical field evaluation) or 'yz'
+        (64^3: convolutions with fused y-z passes over a thread-block cluster);
         variant 0/1 (x: one-shot / pipelined, y: register only, z: shared memory / register,
         xy: off / on); tile 8 or 16."""
-        code = {"x": 0, "y": 1, "z": 2, "xy": 9}.get(pass_)
+        code = {"x": 0, "y": 1, "z": 2, "xy": 9, "yz": 10}.get(pass_)
         if code is None:
             code = 3 + int(pass_[1:])
         self._ck(self.L.he_set_fft_variant(self.h, code, variant, tile))

@@ -165,6 +165,33 @@ HE_D void pdl_wait_and_trigger() {
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
+// ---- members of a context group ----------------------------------------------------------------
+// A group (he_ctx_group) advances several contexts of identical geometry with one launch per
+// kernel: the leader's launches carry a grid dimension over the members, and every CTA of member
+// m maps each device pointer of its arguments -- all of them the leader's buffers -- to member
+// m's corresponding buffer through this table: the leader's buffer starts (ascending) and sizes,
+// then per member the starts of its buffers in the same order.  A pointer inside no leader buffer
+// is returned unchanged, and so is every pointer of member 0 (the leader itself, and every
+// context that is not in a group: nmem = 1, no table).
+struct MemberMap {
+  const unsigned long long* tab;  // [nbuf] leader starts, [nbuf] sizes, [nmem][nbuf] member starts
+  int nbuf, nmem;
+  template <class T>
+  HE_D T* operator()(T* p, int m) const {
+    if (m == 0 || p == nullptr || nbuf == 0) return p;
+    const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+    int lo = 0, hi = nbuf - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(tab + mid) <= a) lo = mid;
+      else hi = mid - 1;
+    }
+    const unsigned long long b = __ldg(tab + lo);
+    if (a < b || a >= b + __ldg(tab + nbuf + lo)) return p;
+    return reinterpret_cast<T*>(__ldg(tab + 2 * nbuf + (size_t)m * nbuf + lo) + (a - b));
+  }
+};
+
 // ---- block reduction of NV doubles (fixed order => deterministic) ------------------------------
 template <int NV>
 __device__ void block_reduce_store(double (&v)[NV], double* __restrict__ out) {

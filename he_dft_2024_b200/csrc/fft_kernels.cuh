@@ -56,6 +56,13 @@ struct XArgs {
                              // that made specA (the mixed chain scales its wcgk copy)
   int lsolid;
   double C, beta, den_m;
+  MemberMap mm;              // group members (blockIdx.y is the member)
+  HE_D void remap(int m) {
+    den = mm(den, m); dencg_in = mm(dencg_in, m); delj4_in = mm(delj4_in, m);
+    specA = mm(specA, m); specB = mm(specB, m);
+    out1 = mm(out1, m); out2 = mm(out2, m);
+    extra = mm(extra, m); extra2 = mm(extra2, m);
+  }
 };
 
 HE_D double corr_source(double den, double dcg, double cp4, double cpp4) {
@@ -128,8 +135,10 @@ HE_HD size_t xpass_smem(int stw_len, int rb, int n) {
 // load-transform-store CTA is hidden behind the transform.
 constexpr int kXPipeThreads = 256;  // threads of a pipelined x-pass CTA, whatever its rows
 template <int MODE, int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a) {
+__global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a_in) {
   pdl_wait_and_trigger();
+  XArgs a = a_in;
+  a.remap(blockIdx.y);
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
   using ST = XStage<MODE>;
@@ -271,8 +280,10 @@ __global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a) {
 // One-shot variant of k_xpass: one CTA per row tile, loading its inputs straight from global
 // memory (no staging buffers, so less shared memory per CTA; the autotuner picks between the two).
 template <int MODE, int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a) {
+__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a_in) {
   pdl_wait_and_trigger();
+  XArgs a = a_in;
+  a.remap(blockIdx.y);
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
   const Rs* den = reinterpret_cast<const Rs*>(a.den);
@@ -392,11 +403,22 @@ struct YZArgs {
   const double* k2;          // null: single kernel
   const float* k1f;          // binary32 copies of k1, k2 (the mixed chain)
   const float* k2f;
+  int narr;                  // k_ypass: arrays per member (blockIdx.z = member x narr + array)
+  MemberMap mm;              // group members (k_zconv: blockIdx.z is the member)
+  HE_D void remap(int m) {
+    arr[0] = mm(arr[0], m); arr[1] = mm(arr[1], m);
+    io = mm(io, m); out2 = mm(out2, m); fden_out = mm(fden_out, m);
+    k1 = mm(k1, m); k2 = mm(k2, m); k1f = mm(k1f, m); k2f = mm(k2f, m);
+  }
 };
 
 template <int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
+__global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a_in) {
   pdl_wait_and_trigger();
+  const int narr = a_in.narr > 0 ? a_in.narr : (int)gridDim.z;
+  YZArgs a = a_in;
+  a.remap((int)blockIdx.z / narr);
+  const int ai = (int)blockIdx.z % narr;
   using C = typename Cx<Rt>::T;
   C* smem = smem_as<C>();
   const int n = (N > 0) ? N : a.ny;
@@ -406,7 +428,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int z = blockIdx.y;
-  C* arr = reinterpret_cast<C*>(a.arr[blockIdx.z]);
+  C* arr = reinterpret_cast<C*>(a.arr[ai]);
   C* tw = smem;
   C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
   C* P1 = P0 + TK * ls;
@@ -427,8 +449,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a) {
 }
 
 template <int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a) {
+__global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a_in) {
   pdl_wait_and_trigger();
+  YZArgs a = a_in;
+  a.remap(blockIdx.z);
   using C = typename Cx<Rt>::T;
   using X = Cx<Rt>;
   constexpr bool F32 = sizeof(Rt) == 4;

@@ -215,7 +215,8 @@ HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
   const int tid = threadIdx.x;
   const int nxh = a.nxh;
   const int kx0 = blockIdx.x * TK;
-  C* arr = reinterpret_cast<C*>(a.arr[blockIdx.z]);
+  const int narr = a.narr > 0 ? a.narr : (int)gridDim.z;
+  C* arr = reinterpret_cast<C*>(a.mm(a.arr[blockIdx.z % narr], (int)blockIdx.z / narr));
   const long base = (long)nxh * N * blockIdx.y;
   {
     const int c = tid % TK, am = tid / TK;  // phase A: column c, a = am
@@ -364,9 +365,11 @@ HE_D void zconv_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T0, C* T
 }
 
 template <int N, int TK, typename Rt = double>
-__global__ void __launch_bounds__(yreg_threads(N, TK)) k_zconv_reg(const YZArgs a,
+__global__ void __launch_bounds__(yreg_threads(N, TK)) k_zconv_reg(const YZArgs a_in,
                                                                    const typename Cx<Rt>::T* tw2) {
   pdl_wait_and_trigger();
+  YZArgs a = a_in;
+  a.remap(blockIdx.z);
   using C = typename Cx<Rt>::T;
   C* T0 = smem_as<C>();
   zconv_reg_body<N, TK>(a, tw2, T0, T0 + N * TK);

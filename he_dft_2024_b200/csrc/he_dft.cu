@@ -21,6 +21,7 @@
 #include "fft_kernels.cuh"
 #include "fft_reg.cuh"
 #include "fft_xy.cuh"
+#include "fft_yz.cuh"
 #include "ops.cuh"
 #include "setup.cuh"
 #include "quantum.cuh"
@@ -84,6 +85,12 @@ struct he_ctx {
   long long launches = 0;
   size_t bytes = 0;
   std::vector<void*> allocs;
+  std::vector<size_t> alloc_bytes;  // sizes of allocs, in the same order
+  // group (he_ctx_group): this context as the leader of nmem members whose buffers the member
+  // map pairs with this context's; every launch covers all members
+  int nmem = 1;
+  MemberMap mm{};
+  std::vector<unsigned long long> mmhost;  // host copy of the map table
   // FFT
   LinePlan plx{}, ply{}, plz{};
   int x_rb = 16, tkx = 16;
@@ -93,6 +100,7 @@ struct he_ctx {
   int xtile[6] = {16, 16, 16, 16, 16, 16};
   bool zreg = false;  // z convolution with register line transforms (binary32 chain only)
   bool xyfuse = false;  // classical field evaluation with fused x-y plane passes (fft_xy.cuh)
+  bool yzfuse = false;  // convolutions with the y and z passes fused over a cluster (fft_yz.cuh)
   int maxsm = 0;      // opt-in shared memory per block
   bool xpipe[6] = {false, false, false, false, false, false};
   std::string tune_log;                        // the autotuner's trials (he_autotune_report)
@@ -278,6 +286,7 @@ static int dalloc(he_ctx_t* ctx, void** p, size_t bytes) {
     return fail(ctx, HE_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
   }
   ctx->allocs.push_back(*p);
+  ctx->alloc_bytes.push_back(bytes);
   ctx->bytes += bytes;
   CK(cudaMemsetAsync(*p, 0, bytes, ctx->stream));
   return HE_OK;
@@ -497,6 +506,8 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<Op, kTX, kTY>, kTX * kTY, smem));
   }
   TRY(join_aux(ctx));  // stencils read uimp / write den / reduce through the shared partials
+  if (ctx->nmem > 1 && !HasRemap<Op>::value)
+    return fail(ctx, HE_ERR_STATE, "%s does not run over the members of a group", Op::kname());
   StencilGeom g = g0;
   g.zc = choose_zc(ctx, occ);
   dim3 grid = stencil_grid(ctx, g), block(kTX, kTY);
@@ -505,6 +516,9 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
     TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
     rt = tail(ctx, slot);
   }
+  g.nzc = (int)grid.z;  // blockIdx.z = member x nzc + chunk
+  g.mm = ctx->mm;
+  grid.z *= ctx->nmem;
   CK(set_smem_attr((const void*)k_stencil<Op, kTX, kTY>, smem));
   tname(ctx, Op::kname());
   k_stencil<Op, kTX, kTY><<<grid, block, smem, ctx->stream>>>(f, g, op, rt);
@@ -541,6 +555,7 @@ static XArgs xargs(he_ctx_t* ctx) {
   a.a0 = ctx->fn.cp4 / 2.0; a.a1 = ctx->fn.cpp4 / 3.0;
   a.lsolid = ctx->fn.lsolid;
   a.C = ctx->fn.C; a.beta = ctx->fn.beta; a.den_m = ctx->fn.den_m;
+  a.mm = ctx->mm;
   return a;
 }
 // Line lengths with a compile-time FFT instantiation; other admissible lengths run the same
@@ -583,7 +598,7 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
     const size_t csmem = fft_smem(ctx->plx, rb, 2, sizeof(typename Cx<Rt>::T));
     CK(set_smem_attr((const void*)k_xpass_c<MODE, N, TILE, Rt>, csmem));
     tname(ctx, names[MODE]);
-    CK(launch_chain(ctx, k_xpass_c<MODE, N, TILE, Rt>, dim3((unsigned)ntiles), dim3(nthr), csmem, a));
+    CK(launch_chain(ctx, k_xpass_c<MODE, N, TILE, Rt>, dim3((unsigned)ntiles, ctx->nmem), dim3(nthr), csmem, a));
     LAUNCHED();
     return HE_OK;
   }
@@ -602,7 +617,7 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   const unsigned nb = (unsigned)std::min<long>(ntiles, (long)occ * ctx->num_sms);
   CK(set_smem_attr((const void*)k_xpass<MODE, N, TILE, Rt>, smem));
   tname(ctx, names[MODE]);
-  CK(launch_chain(ctx, k_xpass<MODE, N, TILE, Rt>, dim3(nb), dim3(pthr), smem, a));
+  CK(launch_chain(ctx, k_xpass<MODE, N, TILE, Rt>, dim3(nb, ctx->nmem), dim3(pthr), smem, a));
   LAUNCHED();
   return HE_OK;
 }
@@ -630,7 +645,7 @@ static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
   const int tk = (N > 0) ? TILE : ctx->tkx;
   const size_t smem = fft_smem(ctx->ply, tk, 2, sizeof(C));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
-  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->nz, narr);
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->nz, narr * ctx->nmem);  // z: member x narr + array
   tname(ctx, "fft_y");
   if constexpr (N > 0) {
     // register line transform (fft_reg.cuh): TK columns x N2 threads, T[k1][a][c] in shared memory
@@ -667,6 +682,8 @@ static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
   a.arr[0] = a0; a.arr[1] = a1 ? a1 : a0;
   a.inv = inv;
   const int narr = a1 ? 2 : 1;
+  a.narr = narr;
+  a.mm = ctx->mm;
   return ctx->mixed ? ypass_t<float>(ctx, a, narr) : ypass_t<double>(ctx, a, narr);
 }
 
@@ -678,7 +695,7 @@ static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
       using C = typename Cx<Rt>::T;
       const size_t rsmem = sizeof(C) * (size_t)N * TILE * (a.k2f ? 2 : 1);
       CK(set_smem_attr((const void*)k_zconv_reg<N, TILE, Rt>, rsmem));
-      dim3 grid((ctx->nxh + TILE - 1) / TILE, ctx->ny, 1);
+      dim3 grid((ctx->nxh + TILE - 1) / TILE, ctx->ny, ctx->nmem);
       tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
       CK(launch_chain(ctx, k_zconv_reg<N, TILE, Rt>, grid, dim3(yreg_threads(N, TILE)), rsmem, a,
                       (const C*)ctx->plz.tw2f));
@@ -688,7 +705,7 @@ static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
   }
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
-  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, ctx->nmem);
   CK(set_smem_attr((const void*)k_zconv<N, TILE, Rt>, smem));
   tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
   CK(launch_chain(ctx, k_zconv<N, TILE, Rt>, grid, dim3(nthr), smem, a));
@@ -725,11 +742,56 @@ static int zconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, co
   a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
   a.pl = ctx->plz;
   a.io = io; a.out2 = out2; a.fden_out = fden_out; a.k1 = k1; a.k2 = k2;
+  a.mm = ctx->mm;
   if (!ctx->mixed) return zconv_t<double>(ctx, a);
   a.k1f = kernel_f32(ctx, k1);
   a.k2f = kernel_f32(ctx, k2);
   if (!a.k1f || (k2 && !a.k2f)) return fail(ctx, HE_ERR_STATE, "no binary32 copy of a k-space kernel");
   return zconv_t<float>(ctx, a);
+}
+
+// ---- fused y-z convolutions (fft_yz.cuh): 64^3-sized y-z planes ----
+static bool yz_fusable(const he_ctx_t* ctx) { return ctx->ny == 64 && ctx->nz == 64; }
+template <int N, int CS, bool TWO, typename Rt>
+static int yzconv_n(he_ctx_t* ctx, const YZConvArgs& a) {
+  constexpr size_t smem = yz_smem<N, CS, Rt>();
+  void (*k)(YZConvArgs) = k_yzconv<N, CS, TWO, Rt>;
+  CK(set_smem_attr((const void*)k, smem));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(((ctx->nxh + 1) / 2) * CS), ctx->nmem);
+  cfg.blockDim = dim3(kYZThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  tname(ctx, TWO ? "fft_yz_conv2" : "fft_yz_conv1");
+  CK(cudaLaunchKernelEx(&cfg, k, a));
+  LAUNCHED();
+  return HE_OK;
+}
+// io <- y^-1 z^-1 (K1 . z y io) [and out2 <- y^-1 z^-1 (K2 . z y io), fden_out <- z y io]
+static int yzconv(he_ctx_t* ctx, double2* io, const double* k1, double2* out2, const double* k2,
+                  double2* fden_out) {
+  if (!yz_fusable(ctx)) return fail(ctx, HE_ERR_STATE, "no fused y-z convolution for this grid");
+  YZConvArgs a{};
+  a.nxh = ctx->nxh;
+  a.io = io; a.out2 = out2; a.fden_out = fden_out; a.k1 = k1; a.k2 = k2;
+  a.tw2 = ctx->ply.tw2; a.tw2f = ctx->ply.tw2f;
+  a.mm = ctx->mm;
+  const bool two = k2 != nullptr;
+  if (two && (!out2 || !fden_out)) return fail(ctx, HE_ERR_STATE, "two-kernel convolution needs out2 and fden");
+  if (ctx->mixed) {
+    a.k1f = kernel_f32(ctx, k1);
+    a.k2f = kernel_f32(ctx, k2);
+    if (!a.k1f || (two && !a.k2f)) return fail(ctx, HE_ERR_STATE, "no binary32 copy of a k-space kernel");
+    return two ? yzconv_n<64, 4, true, float>(ctx, a) : yzconv_n<64, 4, false, float>(ctx, a);
+  }
+  return two ? yzconv_n<64, 4, true, double>(ctx, a) : yzconv_n<64, 4, false, double>(ctx, a);
 }
 
 // fden = R2C(den); wA <- fden*wcgk and wB <- fden*fvlj4 back in (x-transformed) row space.
@@ -738,6 +800,7 @@ static int spectrum_cg_lj(he_ctx_t* ctx) {
   a.den = ctx->den;
   a.specA = ctx->wA;
   TRY(xpass<X_R2C_DEN>(ctx, a));
+  if (ctx->yzfuse) return yzconv(ctx, ctx->wA, ctx->wcgk, ctx->wB, ctx->fvlj4, ctx->fden);
   TRY(ypass(ctx, ctx->wA, nullptr, false));
   TRY(zconv(ctx, ctx->wA, ctx->wcgk, ctx->wB, ctx->fvlj4, ctx->fden));
   TRY(ypass(ctx, ctx->wA, ctx->wB, true));
@@ -747,9 +810,13 @@ static int spectrum_cg_lj(he_ctx_t* ctx) {
 // (extra: potx4 of the quantum impurities, or null).
 static int correlation_tail(he_ctx_t* ctx, const double* extra = nullptr,
                             const double* extra2 = nullptr) {
-  TRY(ypass(ctx, ctx->wA, nullptr, false));
-  TRY(zconv(ctx, ctx->wA, ctx->wcgk, nullptr, nullptr, nullptr));
-  TRY(ypass(ctx, ctx->wA, nullptr, true));
+  if (ctx->yzfuse) {
+    TRY(yzconv(ctx, ctx->wA, ctx->wcgk, nullptr, nullptr, nullptr));
+  } else {
+    TRY(ypass(ctx, ctx->wA, nullptr, false));
+    TRY(zconv(ctx, ctx->wA, ctx->wcgk, nullptr, nullptr, nullptr));
+    TRY(ypass(ctx, ctx->wA, nullptr, true));
+  }
   XArgs a = xargs(ctx);
   a.specA = ctx->wA;
   a.den = ctx->den; a.dencg_in = ctx->dencg; a.delj4_in = ctx->delj4;
@@ -986,6 +1053,12 @@ struct StatPW {
   double* den;
   double a, b, c;
   int jr;
+  MemberMap mm;       // group members (blockIdx.y is the member)
+  HE_D void remap(int m) {
+    sums = mm(sums, m); psi = mm(psi, m); out = mm(out, m); po3 = mm(po3, m); po2 = mm(po2, m);
+    h1 = mm(h1, m); h2 = mm(h2, m); pc = mm(pc, m); q = mm(q, m); hsave = mm(hsave, m);
+    hpsi = mm(hpsi, m); timec = mm(timec, m); den = mm(den, m);
+  }
 };
 
 __device__ __forceinline__ double local_dt(double hp, double ps, const StatPW& s) {
@@ -993,7 +1066,10 @@ __device__ __forceinline__ double local_dt(double hp, double ps, const StatPW& s
 }
 
 // steppcr predictor + modifier (steppcr.f90:40-61); acc = sum psi_new^2.
-__global__ void __launch_bounds__(256) k_stat_predict(const StatPW s, const ReduceTail rt) {
+__global__ void __launch_bounds__(256) k_stat_predict(const StatPW s_in, const ReduceTail rt_in) {
+  StatPW s = s_in;
+  s.remap(blockIdx.y);
+  const ReduceTail rt = remap(rt_in, s.mm, blockIdx.y);
   const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
   const double hmean = s.sums[S_STAT_H] * s.dxyz / s.n4;
   double acc[1] = {0.0};
@@ -1015,7 +1091,10 @@ __global__ void __launch_bounds__(256) k_stat_predict(const StatPW s, const Redu
 }
 
 // steppcr corrector + final value (steppcr.f90:78-90); acc = {sum |pc|, sum psi_new^2}.
-__global__ void __launch_bounds__(256) k_stat_correct(const StatPW s, const ReduceTail rt) {
+__global__ void __launch_bounds__(256) k_stat_correct(const StatPW s_in, const ReduceTail rt_in) {
+  StatPW s = s_in;
+  s.remap(blockIdx.y);
+  const ReduceTail rt = remap(rt_in, s.mm, blockIdx.y);
   const double c9 = 9.0 / 121.0;
   const double mu = s.sums[S_STAT_MU] * s.dxyz / s.n4;
   double acc[2] = {0.0, 0.0};
@@ -1037,7 +1116,10 @@ __global__ void __launch_bounds__(256) k_stat_correct(const StatPW s, const Redu
 }
 
 // steprkr stage update (steprkr.f90:160-179); acc = sum psi_new^2.
-__global__ void __launch_bounds__(256) k_stat_rk(const StatPW s, const ReduceTail rt) {
+__global__ void __launch_bounds__(256) k_stat_rk(const StatPW s_in, const ReduceTail rt_in) {
+  StatPW s = s_in;
+  s.remap(blockIdx.y);
+  const ReduceTail rt = remap(rt_in, s.mm, blockIdx.y);
   const double err = s.sums[S_STAT_H] * s.dxyz / s.n4;
   double acc[1] = {0.0};
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < s.N;
@@ -1060,7 +1142,10 @@ __global__ void __launch_bounds__(256) k_stat_rk(const StatPW s, const ReduceTai
 // psi = |psi| * sqrt(n4/(sum psi^2 dxyz)); den = psi^2.
 __global__ void __launch_bounds__(256) k_stat_normalize(double* psi, double* den, long N,
                                                         const double* sums, double n4,
-                                                        double dxyz) {
+                                                        double dxyz, const MemberMap mm) {
+  psi = mm(psi, blockIdx.y);
+  den = mm(den, blockIdx.y);
+  sums = mm(sums, blockIdx.y);
   const double cnorm = sqrt(n4 / (sums[S_STAT_N] * dxyz));
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N;
        i += (long)gridDim.x * blockDim.x) {
@@ -1070,7 +1155,10 @@ __global__ void __launch_bounds__(256) k_stat_normalize(double* psi, double* den
   }
 }
 
-__global__ void __launch_bounds__(256) k_sumsq(const double* psi, long N, const ReduceTail rt) {
+__global__ void __launch_bounds__(256) k_sumsq(const double* psi, long N, const ReduceTail rt_in,
+                                               const MemberMap mm) {
+  psi = mm(psi, blockIdx.y);
+  const ReduceTail rt = remap(rt_in, mm, blockIdx.y);
   double acc[1] = {0.0};
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N;
        i += (long)gridDim.x * blockDim.x)
@@ -1081,7 +1169,10 @@ __global__ void __launch_bounds__(256) k_sumsq(const double* psi, long N, const 
 
 // varmu: sum |hpsi - mu psi| * psi (varmu.f90:31).
 __global__ void __launch_bounds__(256) k_varmu(const double* hpsi, const double* psi, long N,
-                                               double mu, const ReduceTail rt) {
+                                               double mu, const ReduceTail rt_in, const MemberMap mm) {
+  hpsi = mm(hpsi, blockIdx.y);
+  psi = mm(psi, blockIdx.y);
+  const ReduceTail rt = remap(rt_in, mm, blockIdx.y);
   double acc[1] = {0.0};
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N;
        i += (long)gridDim.x * blockDim.x)
@@ -1208,7 +1299,8 @@ __global__ void __launch_bounds__(256) k_varmu_m(const float* hpsi, const float*
   reduce_tail<1>(rt, gridDim.x);
 }
 
-__global__ void k_copy_slot(double* sums, int dst, int src) {
+__global__ void k_copy_slot(double* sums, int dst, int src, const MemberMap mm) {
+  sums = mm(sums, blockIdx.y);
   if (threadIdx.x == 0 && blockIdx.x == 0) sums[dst] = sums[src];
 }
 
@@ -1218,6 +1310,8 @@ static int pw_blocks(const he_ctx_t* ctx) {
   long b = (ctx->N + 255) / 256;
   return (int)(b < kPwBlocks ? b : kPwBlocks);
 }
+// Grid of a pointwise kernel: blockIdx.y is the member of a group.
+static dim3 pw_grid(const he_ctx_t* ctx) { return dim3(pw_blocks(ctx), ctx->nmem); }
 
 template <int NI, typename TT>
 static int launch_impfield_t(he_ctx_t* ctx) {
@@ -1257,6 +1351,7 @@ static StatPW statpw(he_ctx_t* ctx, double dt, int n4) {
   s.sums = ctx->sums;
   s.timec = ctx->timec;
   s.den = ctx->den;
+  s.mm = ctx->mm;
   return s;
 }
 
@@ -1292,8 +1387,8 @@ static int stat_normalize(he_ctx_t* ctx, int n4) {
     k_stat_normalize_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((float*)ctx->psi, (float*)ctx->den,
                                                                 ctx->N, ctx->sums, (double)n4, ctx->dxyz);
   else
-    k_stat_normalize<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
-                                                              ctx->sums, (double)n4, ctx->dxyz);
+    k_stat_normalize<<<pw_grid(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
+                                                            ctx->sums, (double)n4, ctx->dxyz, ctx->mm);
   LAUNCHED();
   return HE_OK;
 }
@@ -1426,6 +1521,32 @@ static int autotune_tiles(he_ctx_t* ctx) {
       }
       ctx->zreg = best_reg;
       ctx->tile_z = best_tile;
+    }
+  }
+  if (st == HE_OK && yz_fusable(ctx)) {
+    // the two-kernel convolution (fden*wcgk, fden*fvlj4) with separate y / z passes against the
+    // fused y-z kernel
+    auto conv = [](he_ctx_t* c) -> int {
+      if (c->yzfuse) return yzconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, c->fden);
+      TRY(ypass(c, c->wA, nullptr, false));
+      TRY(zconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, c->fden));
+      return ypass(c, c->wA, c->wB, true);
+    };
+    float ts = 0.0f, tf = 0.0f;
+    ctx->yzfuse = false;
+    st = timed(conv, &ts);
+    if (st == HE_OK) {
+      ctx->yzfuse = true;
+      st = timed(conv, &tf);
+    }
+    if (st == HE_OK) {
+      char line[128];
+      snprintf(line, sizeof line, "yz convolution separate passes: %.2f us\nyz convolution fused: %.2f us\n",
+               1e3f * ts / 3.0f, 1e3f * tf / 3.0f);
+      ctx->tune_log += line;
+      ctx->yzfuse = tf < ts;
+    } else {
+      ctx->yzfuse = false;
     }
   }
   if (st == HE_OK && ctx->mode == HE_MODE_DYNAMICS && !ctx->otc && xy_fusable(ctx)) {
@@ -2643,6 +2764,167 @@ int he_upload(he_ctx_t* ctx, int field, const void* host, size_t bytes) {
   return HE_OK;
 }
 
+// ---- groups ------------------------------------------------------------------------------------
+// Member m's counterpart of one of the leader's device pointers (the host copy of the map).
+static void* member_ptr(const he_ctx_t* L, const void* p, int m) {
+  if (m == 0 || L->nmem <= 1 || !p) return const_cast<void*>(p);
+  const int nb = (int)(L->mmhost.size() / (2 + L->nmem));
+  const unsigned long long a = (unsigned long long)p;
+  const unsigned long long* t = L->mmhost.data();
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (t[mid] <= a) lo = mid;
+    else hi = mid - 1;
+  }
+  if (a < t[lo] || a >= t[lo] + t[nb + lo]) return const_cast<void*>(p);
+  return (void*)(t[2 * nb + (size_t)m * nb + lo] + (a - t[lo]));
+}
+
+int he_ctx_group(he_ctx_t* const* ctxs, int n) {
+  if (!ctxs || n < 1 || !ctxs[0]) return HE_ERR_ARG;
+  he_ctx_t* L = ctxs[0];
+  if (L->nmem != 1) return fail(L, HE_ERR_STATE, "the context already leads a group");
+  if (n == 1) return HE_OK;
+  if (L->mode != HE_MODE_STATICS || L->mixed || L->otc)
+    return fail(L, HE_ERR_ARG, "groups run the binary64 statics mode with the OT or OP core");
+  for (int m = 0; m < n; ++m) {
+    he_ctx_t* c = ctxs[m];
+    if (!c) return fail(L, HE_ERR_ARG, "null member %d", m);
+    for (int j = 0; j < m; ++j)
+      if (ctxs[j] == c) return fail(L, HE_ERR_ARG, "member %d repeats member %d", m, j);
+    if (c->nmem != 1 || c->mode != L->mode || c->prec != L->prec || c->otc != L->otc ||
+        c->nx != L->nx || c->ny != L->ny || c->nz != L->nz || c->xmax != L->xmax ||
+        c->ymax != L->ymax || c->zmax != L->zmax || c->icon != L->icon)
+      return fail(L, HE_ERR_ARG, "member %d differs from the leader (mode, precision, grid or core)", m);
+    if (!c->kernels_ok) return fail(L, HE_ERR_STATE, "member %d has no k-space kernels", m);
+    // derden's gradients are allocated on first use; every member holds them before pairing
+    if (!c->dxden) {
+      TRY(dalloc_t(c, &c->dxden, c->N));
+      TRY(dalloc_t(c, &c->dyden, c->N));
+      TRY(dalloc_t(c, &c->dzden, c->N));
+    }
+    TRY(join_aux(c));
+    TRY(sync_all(c));
+  }
+  const size_t nb = L->allocs.size();
+  for (int m = 1; m < n; ++m) {
+    const he_ctx_t* c = ctxs[m];
+    if (c->allocs.size() != nb || c->alloc_bytes != L->alloc_bytes)
+      return fail(L, HE_ERR_STATE, "member %d does not hold the leader's set of buffers", m);
+  }
+  std::vector<size_t> order(nb);
+  for (size_t i = 0; i < nb; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    return (unsigned long long)L->allocs[a] < (unsigned long long)L->allocs[b];
+  });
+  std::vector<unsigned long long> t((2 + (size_t)n) * nb);
+  for (size_t k = 0; k < nb; ++k) {
+    const size_t i = order[k];
+    t[k] = (unsigned long long)L->allocs[i];
+    t[nb + k] = L->alloc_bytes[i];
+    for (int m = 0; m < n; ++m) t[2 * nb + (size_t)m * nb + k] = (unsigned long long)ctxs[m]->allocs[i];
+  }
+  // the members' relabelled buffers (psi, psiold, hpsiold, scratch) must pair with the leader's
+  auto index_of = [&](const he_ctx_t* c, const void* p) -> long {
+    for (size_t i = 0; i < nb; ++i)
+      if (c->allocs[i] == p) return (long)i;
+    return -1;
+  };
+  for (int m = 1; m < n; ++m) {
+    const he_ctx_t* c = ctxs[m];
+    const void* lp[6] = {L->psi, L->scratch, L->psiold[0], L->psiold[1], L->psiold[2], L->hpsiold[0]};
+    const void* cp[6] = {c->psi, c->scratch, c->psiold[0], c->psiold[1], c->psiold[2], c->hpsiold[0]};
+    for (int k = 0; k < 6; ++k)
+      if (index_of(L, lp[k]) != index_of(c, cp[k]))
+        return fail(L, HE_ERR_STATE, "member %d's ring buffers are relabelled differently from the leader's", m);
+    if (index_of(L, L->hpsiold[1]) != index_of(c, c->hpsiold[1]))
+      return fail(L, HE_ERR_STATE, "member %d's ring buffers are relabelled differently from the leader's", m);
+  }
+  unsigned long long* dt = nullptr;
+  TRY(dalloc_t(L, &dt, t.size()));
+  {
+    const cudaError_t e = cudaMemcpyAsync(dt, t.data(), t.size() * sizeof(unsigned long long),
+                                          cudaMemcpyHostToDevice, L->stream);
+    if (e != cudaSuccess) return fail(L, HE_ERR_CUDA, "map table upload failed: %s", cudaGetErrorString(e));
+  }
+  TRY(sync_all(L));
+  L->mmhost = t;
+  L->mm.tab = dt;
+  L->mm.nbuf = (int)nb;
+  L->mm.nmem = n;
+  L->nmem = n;
+  stat_graphs_clear(L);  // graphs recorded before launched the leader alone
+  return HE_OK;
+}
+
+int he_group_size(const he_ctx_t* ctx) { return ctx ? ctx->nmem : 0; }
+
+static int member_xfer(he_ctx_t* ctx, int member, int field, void* host, size_t bytes, bool up) {
+  if (!ctx || !host) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (member < 0 || member >= ctx->nmem) return fail(ctx, HE_ERR_ARG, "member %d of %d", member, ctx->nmem);
+  if (member == 0) return up ? he_upload(ctx, field, host, bytes) : he_download(ctx, field, host, bytes);
+  if (field == HE_F_RING || qfield(field) || (field >= HE_F_RIMP && field <= HE_F_QV))
+    return fail(ctx, HE_ERR_ARG, "field %d has no per-member copy in a statics group", field);
+  TRY(join_aux(ctx));
+  FieldRef r;
+  TRY(field_ref(ctx, field, &r));
+  if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
+  void* d = member_ptr(ctx, r.ptr, member);
+  if (d == r.ptr) return fail(ctx, HE_ERR_STATE, "field %d is not a per-member buffer", field);
+  if (up) CK(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  else CK(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_all(ctx);
+}
+int he_upload_member(he_ctx_t* ctx, int member, int field, const void* host, size_t bytes) {
+  return member_xfer(ctx, member, field, const_cast<void*>(host), bytes, true);
+}
+int he_download_member(he_ctx_t* ctx, int member, int field, void* host, size_t bytes) {
+  return member_xfer(ctx, member, field, host, bytes, false);
+}
+
+// The reduction slots (sums) of every member, nmem x S_COUNT values from the last launches.
+static int member_sums(he_ctx_t* ctx, std::vector<double>& out) {
+  TRY(join_aux(ctx));
+  out.assign((size_t)ctx->nmem * S_COUNT, 0.0);
+  for (int m = 0; m < ctx->nmem; ++m)
+    CK(cudaMemcpyAsync(out.data() + (size_t)m * S_COUNT, member_ptr(ctx, ctx->sums, m),
+                       S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_all(ctx);
+}
+
+int he_member_mu(he_ctx_t* ctx, int n4, int after_rk, double* mu4) {
+  if (!ctx || !mu4) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
+  std::vector<double> s;
+  TRY(member_sums(ctx, s));
+  const int slot = after_rk ? S_HMEAN0 : S_STAT_H;
+  for (int m = 0; m < ctx->nmem; ++m) mu4[m] = s[(size_t)m * S_COUNT + slot] * ctx->dxyz / (double)n4;
+  return HE_OK;
+}
+
+int he_energy_members(he_ctx_t* ctx, he_energies_t* out) {
+  if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (ctx->mode != HE_MODE_STATICS || ctx->mixed) return fail(ctx, HE_ERR_STATE, "binary64 statics groups only");
+  TRY(he_energy(ctx, &out[0]));
+  std::vector<double> all;
+  TRY(member_sums(ctx, all));
+  const double dxyz = ctx->dxyz;
+  for (int m = 1; m < ctx->nmem; ++m) {
+    const double* s = all.data() + (size_t)m * S_COUNT + S_EN;
+    he_energies_t e{};
+    e.esolid = ctx->fn.lsolid ? ctx->fn.C * s[3] * dxyz : 0.0;
+    e.ekin4 = ctx->fn.h2o2m4 * s[0] * dxyz;
+    e.elj4 = 0.5 * s[1] * dxyz;
+    e.ecor4 = s[2] * dxyz;
+    e.etot4 = e.ekin4 + e.elj4 + e.ecor4 + e.esolid;
+    e.eimpu = 0.0;
+    e.etot = e.etot4;
+    out[m] = e;
+  }
+  return HE_OK;
+}
+
 int he_download(he_ctx_t* ctx, int field, void* host, size_t bytes) {
   if (!ctx || !host) return fail(ctx, HE_ERR_ARG, "null argument");
   TRY(join_aux(ctx));
@@ -3097,7 +3379,8 @@ int he_evolo0(he_ctx_t* ctx, double* mu4, double* mu4err, int n4) {
   if (ctx->mixed)
     k_sumsq_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const float*)ctx->psi, ctx->N, tail(ctx, S_STAT_N));
   else
-    k_sumsq<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double*)ctx->psi, ctx->N, tail(ctx, S_STAT_N));
+    k_sumsq<<<pw_grid(ctx), 256, 0, ctx->stream>>>((const double*)ctx->psi, ctx->N, tail(ctx, S_STAT_N),
+                                                   ctx->mm);
   LAUNCHED();
   TRY(stat_normalize(ctx, n4));
   TRY(read_sums(ctx));
@@ -3118,7 +3401,7 @@ int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
     TRY(stat_hpsi(ctx, ctx->hpsi, S_STAT_H));
     if (jr == 0) {
       tname(ctx, "copy_slot");
-      k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H);
+      k_copy_slot<<<dim3(1, ctx->nmem), 32, 0, ctx->stream>>>(ctx->sums, S_HMEAN0, S_STAT_H, ctx->mm);
       LAUNCHED();
     }
     if (ctx->mixed) {
@@ -3142,7 +3425,7 @@ int he_steprkr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
       s.a = arun[jr]; s.b = brun[jr]; s.c = crun[jr];
       s.jr = jr;
       tname(ctx, "statics_rk_update");
-      k_stat_rk<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+      k_stat_rk<<<pw_grid(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
     }
     LAUNCHED();
     if (jr == 0) {
@@ -3192,7 +3475,7 @@ static int steppcr_launch(he_ctx_t* ctx, double deltat, int n4) {
     s.h2 = (double*)ctx->hpsiold[ctx->ioldh[1] - 1];
     s.pc = (double*)ctx->pc;
     tname(ctx, "statics_predict");
-    k_stat_predict<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+    k_stat_predict<<<pw_grid(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
     LAUNCHED();
     std::swap(ctx->psi, ctx->psiold[ctx->ioldp[2] - 1]);
     std::swap(ctx->ioldh[0], ctx->ioldh[1]);
@@ -3227,13 +3510,13 @@ static int steppcr_launch(he_ctx_t* ctx, double deltat, int n4) {
     s.out = (double*)ctx->scratch;
     ReduceTail rt = tail(ctx, S_STAT_PC);
     tname(ctx, "statics_correct");
-    k_stat_correct<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(s, rt);
+    k_stat_correct<<<pw_grid(ctx), 256, 0, ctx->stream>>>(s, rt);
     LAUNCHED();
     std::swap(ctx->psi, ctx->scratch);
   }
   // k_stat_correct leaves sum psi^2 in S_STAT_PC+1; the normalisation reads S_STAT_N.
   tname(ctx, "copy_slot");
-  k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_STAT_N, S_STAT_PC + 1);
+  k_copy_slot<<<dim3(1, ctx->nmem), 32, 0, ctx->stream>>>(ctx->sums, S_STAT_N, S_STAT_PC + 1, ctx->mm);
   LAUNCHED();
   TRY(stat_normalize(ctx, n4));
   const int a = ctx->ioldp[2];
@@ -3259,7 +3542,7 @@ int he_steppcr(he_ctx_t* ctx, double deltat, double* mu4, double* mu4err, int n4
 // derden, fden, dencg, poten; first S_STAT_H (the previous pass's hmean) is kept in S_STAT_PREV.
 static int statics_pass(he_ctx_t* ctx, double deltat, int n4) {
   tname(ctx, "copy_slot");
-  k_copy_slot<<<1, 32, 0, ctx->stream>>>(ctx->sums, S_STAT_PREV, S_STAT_H);
+  k_copy_slot<<<dim3(1, ctx->nmem), 32, 0, ctx->stream>>>(ctx->sums, S_STAT_PREV, S_STAT_H, ctx->mm);
   LAUNCHED();
   TRY(steppcr_launch(ctx, deltat, n4));
   TRY(he_refresh_density(ctx));
@@ -3358,6 +3641,27 @@ int he_statics_iterations(he_ctx_t* ctx, int niter, double deltat, double* mu4, 
   return HE_OK;
 }
 
+int he_statics_iterations_members(he_ctx_t* ctx, int niter, double deltat, int n4, double* mu4,
+                                  double* mu4err, double* errpc) {
+  if (!ctx || !mu4 || !mu4err) return fail(ctx, HE_ERR_ARG, "null argument");
+  if (niter < 1) return fail(ctx, HE_ERR_ARG, "niter must be positive");
+  if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
+  if (!ctx->kernels_ok) return fail(ctx, HE_ERR_STATE, "k-space kernels not set");
+  TRY(join_aux(ctx));
+  for (int k = 0; k < niter; ++k) TRY(statics_pass_graphed(ctx, deltat, n4));
+  std::vector<double> all;
+  TRY(member_sums(ctx, all));
+  for (int m = 0; m < ctx->nmem; ++m) {
+    const double* h = all.data() + (size_t)m * S_COUNT;
+    const double hmean = h[S_STAT_H] * ctx->dxyz / (double)n4;
+    const double prev = niter > 1 ? h[S_STAT_PREV] * ctx->dxyz / (double)n4 : mu4[m];
+    if (errpc) errpc[m] = (9.0 / 121.0) * h[S_STAT_PC] / (double)ctx->N;
+    mu4err[m] = std::fabs(1.0 - prev / hmean);
+    mu4[m] = hmean;
+  }
+  return HE_OK;
+}
+
 int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu) {
   if (!ctx || !errmu) return fail(ctx, HE_ERR_ARG, "null argument");
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
@@ -3366,8 +3670,8 @@ int he_varmu(he_ctx_t* ctx, int npart, double mu, double* errmu) {
     k_varmu_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const float*)ctx->hpsi, (const float*)ctx->psi,
                                                        ctx->N, mu, tail(ctx, S_VARMU));
   else
-    k_varmu<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(ctx->hpsi, (const double*)ctx->psi, ctx->N, mu,
-                                                     tail(ctx, S_VARMU));
+    k_varmu<<<pw_grid(ctx), 256, 0, ctx->stream>>>(ctx->hpsi, (const double*)ctx->psi, ctx->N, mu,
+                                                   tail(ctx, S_VARMU), ctx->mm);
   LAUNCHED();
   TRY(read_sums(ctx));
   *errmu = ctx->hsum[S_VARMU] * ctx->dxyz / (double)npart;
@@ -3437,6 +3741,11 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
       ctx->zreg = variant != 0;
       ctx->tile_z = tile;
       return HE_OK;
+    case 10:
+      if (variant && !yz_fusable(ctx))
+        return fail(ctx, HE_ERR_ARG, "fused y-z convolutions need ny = nz = 64");
+      ctx->yzfuse = variant != 0;
+      return HE_OK;
     case 9:
       if (variant && !xy_fusable(ctx))
         return fail(ctx, HE_ERR_ARG, "fused x-y passes need HE_PREC_MIXED and nx = ny in {64, 96, 128}");
@@ -3452,7 +3761,7 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
         ctx->xtile[m] = tile;
         return HE_OK;
       }
-      return fail(ctx, HE_ERR_ARG, "pass must be 0 (x), 1 (y), 2 (z) or 3..8 (one x mode)");
+      return fail(ctx, HE_ERR_ARG, "pass must be 0 (x), 1 (y), 2 (z), 3..8 (one x mode), 9 (x-y) or 10 (y-z)");
   }
 }
 

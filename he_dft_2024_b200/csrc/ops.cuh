@@ -308,6 +308,9 @@ struct OpEnergy {
   const Z* s16[1];
   double aux1, aux2, beta, den_m;
   int lsolid, has_u;
+  HE_D void remap(const MemberMap& mm, int m) {
+    for (int k = 0; k < N8; ++k) s8[k] = mm(s8[k], m);
+  }
   HE_D static double n2(double v) { return v * v; }
   HE_D static double n2(double2 v) { return v.x * v.x + v.y * v.y; }
   HE_D static double n2(float v) { return (double)v * (double)v; }
@@ -378,6 +381,11 @@ struct OpDerden {
   double* gx;
   double* gy;
   double* gz;
+  HE_D void remap(const MemberMap& mm, int m) {
+    gx = mm(gx, m);
+    gy = mm(gy, m);
+    gz = mm(gz, m);
+  }
   HE_D void at(int, int, int, long i, double dx, double dy, double dz, double, const double*,
                const double2*, int, double*) const {
     gx[i] = dx;
@@ -673,6 +681,10 @@ struct OpHpsiRT {
   const typename RealOf<TT>::Z* s16[1];
   TT* out;
   TT h2o2m;
+  HE_D void remap(const MemberMap& mm, int m) {
+    s8[0] = mm(s8[0], m);
+    out = mm(out, m);
+  }
   HE_D void at(int, int, int, long i, TT dx, TT dy, TT dz, TT c, const TT* v8,
                const typename RealOf<TT>::Z*, int, double* acc) const {
     const TT h = -((dx + dy) + dz) * h2o2m + v8[0] * c;

@@ -33,6 +33,8 @@ struct StencilGeom {
   int zc;            // z-chunk per CTA
   int icon;          // 13, 8, 18 or 24
   int axis_on[3];    // 0 when n(axis) < npd
+  int nzc;           // z-chunks per member: grid.z = nzc x members (0: grid.z, one member)
+  MemberMap mm;      // group members' buffers (nmem = 1 outside a group)
   double w[3][13];   // scaled weights per axis
   float wf[3][13];   // the same in binary32 (stencils over binary32 fields)
 };
@@ -91,6 +93,21 @@ struct ReduceTail {
   unsigned* counter;
   double* out;
 };
+HE_D ReduceTail remap(const ReduceTail& r, const MemberMap& mm, int m) {
+  return ReduceTail{mm(r.partials, m), mm(r.counter, m), mm(r.out, m)};
+}
+
+// Ops (and other argument structs) of kernels that run over the members of a group carry
+// remap(mm, m), which maps their device pointers to member m's buffers.
+template <class O, class = void>
+struct HasRemap : std::false_type {};
+template <class O>
+struct HasRemap<O, std::void_t<decltype(std::declval<O&>().remap(std::declval<const MemberMap&>(), 0))>>
+    : std::true_type {};
+template <class O>
+HE_D void remap_op(O& o, const MemberMap& mm, int m) {
+  if constexpr (HasRemap<O>::value) o.remap(mm, m);
+}
 
 template <int NV>
 __device__ void reduce_tail(const ReduceTail& rt, long nb) {
@@ -158,9 +175,17 @@ HE_HD constexpr size_t stencil_smem() {
 
 template <class Op, int TX, int TY>
 __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
-    k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
-              const ReduceTail rt) {
+    k_stencil(const typename Op::T* __restrict__ f_in, const StencilGeom g, const Op op_in,
+              const ReduceTail rt_in) {
   using T = typename Op::T;
+  // member of a group (blockIdx.z = member x nzc + chunk) and its buffers
+  const int nzc = g.nzc > 0 ? g.nzc : (int)gridDim.z;
+  const int mem = (int)blockIdx.z / nzc;
+  const int bz = (int)blockIdx.z - mem * nzc;
+  const T* __restrict__ f = g.mm(f_in, mem);
+  Op op = op_in;
+  remap_op(op, g.mm, mem);
+  const ReduceTail rt = remap(rt_in, g.mm, mem);
   using R = typename RealOf<T>::R;
   using Z = typename RealOf<T>::Z;
   constexpr int NT = TX * TY;
@@ -176,7 +201,7 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
   const int tid = tx + TX * ty;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int ix = x0 + tx, iy = y0 + ty;
-  const int z0 = blockIdx.z * g.zc;
+  const int z0 = bz * g.zc;
   const int z1 = min(z0 + g.zc, g.nz);
   const bool inside = (ix < g.nx) && (iy < g.ny);
   const long plane = (long)g.nx * g.ny;
@@ -349,8 +374,8 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
     }
   }
   if constexpr (Op::NV > 0) {
-    const long nb = (long)gridDim.x * gridDim.y * gridDim.z;
-    const long blk = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
+    const long nb = (long)gridDim.x * gridDim.y * nzc;
+    const long blk = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * bz);
     block_reduce_store<NV>(acc, rt.partials + blk * NV);
     reduce_tail<NV>(rt, nb);
   }

@@ -129,3 +129,27 @@ def statics_relax(s, den, n4, deltat, iterations, chunk=50):
         it += k
     out = s.download("den") if hasattr(s, "download") else s.get("den")
     return np.asfortranarray(np.asarray(out).reshape(np.shape(den), order="F")), mu, err
+
+
+def statics_setup_group(leader, dens, n4):
+    """statics_setup for every member of a group (he_ctx_group): member m starts from dens[m];
+    one launch per kernel covers all members.  Returns the members' mu4."""
+    for m, den in enumerate(dens):
+        leader.upload_member(m, "den", den)
+        leader.upload_member(m, "psi", np.sqrt(den))
+    leader.refresh_density()
+    leader.poten()
+    leader.evolo0(0.0, n4)
+    return leader.member_mu(n4)
+
+
+def statics_iteration_group(leader, iterrk, deltat, n4):
+    """statics_iteration for every member of a group; returns the members' mu4."""
+    if iterrk <= 4:
+        leader.steprkr(deltat, 0.0, n4)
+    else:
+        leader.steppcr(deltat, 0.0, n4)
+    mu = leader.member_mu(n4, after_rk=iterrk <= 4)
+    leader.refresh_density()
+    leader.poten()
+    return mu

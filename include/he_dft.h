@@ -315,7 +315,10 @@ int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
  * 3 + m = the x pass of one mode m only (0 R2C of den, 1 R2C of the statics correlation source,
  * 2 C2R of two spectra, 3 the same plus the correlation R2C, 4 C2R + pot4, 5 C2R of one
  * spectrum), 9 = the classical field evaluation with fused x-y plane passes (variant 1) or
- * separate passes (0; HE_PREC_MIXED, nx = ny in {64, 96, 128}, tile ignored but checked);
+ * separate passes (0; HE_PREC_MIXED, nx = ny in {64, 96, 128}, tile ignored but checked),
+ * 10 = the convolutions with the y and z passes fused in one launch per convolution over a
+ * thread-block cluster (variant 1) or as separate passes (0; ny = nz = 64, tile ignored but
+ * checked);
  * tile = 8 or 16 lines.  HE_ERR_ARG for a variant this grid or precision does not have.  No
  * counterpart in the reference. */
 int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
@@ -327,6 +330,33 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
  * periodic).  No counterpart in the reference. */
 int he_state_fingerprint(const he_ctx_t* ctx, unsigned long long* out);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
+
+/* ---- groups: several statics droplets advanced by one launch per kernel ----
+ * No counterpart in the reference (its drivers run one droplet per process).  he_ctx_group makes
+ * ctxs[0] the leader of n contexts created alike (same mode, precision, grid and functional;
+ * binary64 statics mode, OT or OP core), each set up on its own (uploads, he_set_kernels or
+ * he_compute_kernels) and in the same ring state.  From then on every routine called on the
+ * leader launches each kernel once with a grid dimension over the members, and every member's
+ * CTAs work on that member's buffers; the members' contexts must stay alive and must not be
+ * called directly until the leader is destroyed.  Scalars the leader's routines return are
+ * member 0's; the *_members calls below return every member's, and he_upload_member /
+ * he_download_member move member m's module arrays (m = 0 is the leader).  Routines outside the
+ * statics loop of BCN4HeDFT.f90:1113-1160 (and energy, varmu) return HE_ERR_STATE in a group. */
+int he_ctx_group(he_ctx_t* const* ctxs, int n);
+/* Number of members the context leads (1 outside a group). */
+int he_group_size(const he_ctx_t* ctx);
+int he_upload_member(he_ctx_t* ctx, int member, int field, const void* host, size_t bytes);
+int he_download_member(he_ctx_t* ctx, int member, int field, void* host, size_t bytes);
+/* mu4[m] of each member as the last statics routine returns it for member 0: after he_steppcr or
+ * he_evolo0 (after_rk = 0) sum(psi H psi) dxyz / n4 of the last H psi reduction, after
+ * he_steprkr (after_rk = 1) that of its first stage. */
+int he_member_mu(he_ctx_t* ctx, int n4, int after_rk, double* mu4);
+/* he_statics_iterations for every member: mu4, mu4err (and errpc) are arrays of he_group_size
+ * values; mu4 carries each member's previous value in (used when niter = 1). */
+int he_statics_iterations_members(he_ctx_t* ctx, int niter, double deltat, int n4, double* mu4,
+                                  double* mu4err, double* errpc);
+/* energy() of every member into out[he_group_size(ctx)]. */
+int he_energy_members(he_ctx_t* ctx, he_energies_t* out);
 
 /* ---- energy sums without device allocation ----
  * No counterpart in the reference.  For callers that cannot let a library allocate device
