@@ -774,12 +774,18 @@ def run_quantum(args):
         ctxs.append(c)
     setup_s = time.perf_counter() - t0
     w = batch[0]
-    for c in ctxs:
+    # --group: the trajectories become one group (he_ctx_group) whose leader launches every
+    # kernel once for all of them; otherwise each context launches its own kernels
+    active = ctxs
+    if args.group and len(ctxs) > 1:
+        ctxs[0].group(ctxs[1:])
+        active = ctxs[:1]
+    for c in active:
         for it in range(1, 4):
             D.quantum_iteration(c, it, w.deltat)
     it = 4
     for _ in range(args.warmup):
-        for c in ctxs:
+        for c in active:
             D.quantum_iteration(c, it, w.deltat)
         it += 1
     torch.cuda.synchronize()
@@ -790,25 +796,25 @@ def run_quantum(args):
     graphs = []
     per_step = None
     if args.graph:
-        start = tuple(c.state_fingerprint() for c in ctxs)
-        lc0 = sum(c.launches for c in ctxs)
+        start = tuple(c.state_fingerprint() for c in active)
+        lc0 = sum(c.launches for c in active)
         for _ in range(GRAPH_MAX_PERIOD):
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
-                for c in ctxs:
+                for c in active:
                     D.quantum_iteration(c, it, w.deltat)  # it >= 4: steppc, as replayed
             graphs.append(g)
-            if tuple(c.state_fingerprint() for c in ctxs) == start:
+            if tuple(c.state_fingerprint() for c in active) == start:
                 break
         else:
             raise RuntimeError("the step's buffer relabelling did not repeat within "
                                f"{GRAPH_MAX_PERIOD} steps")
-        per_step = (sum(c.launches for c in ctxs) - lc0) // len(graphs)  # recorded kernels
+        per_step = (sum(c.launches for c in active) - lc0) // len(graphs)  # recorded kernels
         for g in graphs:  # one untimed pass over the cycle (device state follows the host's)
             g.replay()
         it += len(graphs)
         torch.cuda.synchronize()
-    l0 = sum(c.launches for c in ctxs)
+    l0 = sum(c.launches for c in active)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
@@ -817,13 +823,13 @@ def run_quantum(args):
                 graphs[k % len(graphs)].replay()
         else:
             for _ in range(args.steps):
-                for c in ctxs:
+                for c in active:
                     D.quantum_iteration(c, it, w.deltat)
         ev1.record(stream)
         torch.cuda.synchronize()
     it += args.steps
     secs = ev0.elapsed_time(ev1) / 1e3
-    launches = sum(c.launches for c in ctxs) - l0
+    launches = sum(c.launches for c in active) - l0
     if graphs:
         # complete the cycle so that the device state matches the host's relabelling again
         for k in range(args.steps, args.steps + (-args.steps) % len(graphs)):
@@ -837,9 +843,12 @@ def run_quantum(args):
     # every trajectory, as the driver writes them per step.
     t1 = time.perf_counter()
     for _ in range(args.steps):
-        for c in ctxs:
+        for c in active:
             D.quantum_iteration(c, it, w.deltat, errors=True)
-            c.qimp_moments()
+            if c.members > 1:
+                c.qimp_moments_members()
+            else:
+                c.qimp_moments()
         it += 1
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t1
@@ -870,11 +879,12 @@ def run_quantum(args):
     tot = sum(v[1] for v in rep.values())
     bpp = quantum_bytes_per_point(w.nx, mixed=args.precision == "mixed")
     peak, peak_kind = measured_peak()
+    nm = ctxs[0].members  # a grouped launch covers every trajectory of the batch
     breakdown = {k: {"launches": v[0], "ms_per_launch": v[1] / v[0], "share": v[1] / tot,
-                     "GB/s": (bpp[k] * N / (v[1] / v[0] / 1e3) / 1e9) if k in bpp else None}
+                     "GB/s": (bpp[k] * N * nm / (v[1] / v[0] / 1e3) / 1e9) if k in bpp else None}
                  for k, v in sorted(rep.items(), key=lambda kv: -kv[1][1])}
     name, (nl, kms) = max(rep.items(), key=lambda kv: kv[1][1])
-    achieved = bpp.get(name, 0.0) * N / (kms / nl / 1e3) / 1e9
+    achieved = bpp.get(name, 0.0) * N * nm / (kms / nl / 1e3) / 1e9
     line = {
         "metric": METRIC_Q.replace("FP64", "mixed") if args.precision == "mixed" else METRIC_Q, "value": value, "unit": UNIT, "n_gpus": ws_, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
@@ -882,6 +892,7 @@ def run_quantum(args):
         "config": {"workload": w.name, "trajectories": len(ctxs), "grid": [w.nx, w.ny, w.nz],
                    "cuda_graphs": ({"graphs_per_cycle": len(graphs), "kernels_per_batch_step": per_step}
                                    if graphs else None),
+                   "grouped": len(active) == 1 and len(ctxs) > 1,
                    "n4": w.n4, "impurity": "23 u quantum, Morse He-X via FT_V_spline",
                    "deltat_ps": w.deltatps, "parallelism": f"replicas{ws_}",
                    "device_gb": sum(c.device_bytes for c in ctxs) / 1e9},
@@ -891,7 +902,7 @@ def run_quantum(args):
         "setup_s": setup_s,
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "alg_bytes_per_launch": bpp.get(name, 0.0) * N,
+                     "traffic": None, "alg_bytes_per_launch": bpp.get(name, 0.0) * N * nm,
                      "ms_per_launch": kms / nl},
         "step_alg_bytes_per_point": QSTEP_BYTES_PER_POINT[args.precision],
         "step_roofline_frac": QSTEP_BYTES_PER_POINT[args.precision] * N * args.steps * len(ctxs)
@@ -1192,6 +1203,9 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--droplets", type=int, default=1,
                     help="statics workload: droplets advanced together as one group (he_ctx_group)")
+    ap.add_argument("--no-group", dest="group", action="store_false",
+                    help="quantum workload: every trajectory's context launches its own kernels "
+                         "instead of one group launching each kernel once for the whole batch")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="quantum workload: launch the batch step's kernels one by one instead "
                          "of replaying captured CUDA graphs")

@@ -162,6 +162,7 @@ def load():
         "he_member_mu": (ip, [vp, ip, ip, dp]),
         "he_statics_iterations_members": (ip, [vp, ip, d, ip, dp, dp, dp]),
         "he_energy_members": (ip, [vp, ctypes.POINTER(HeEnergies)]),
+        "he_qimp_moments_members": (ip, [vp, dp]),
         "he_energy_noalloc": (ip, [ctypes.POINTER(HeGrid), ctypes.POINTER(HeFunctional), ip, vp,
                                    vp, vp, vp, vp, vp, ctypes.POINTER(HeEnergies),
                                    ctypes.c_char_p, ctypes.c_size_t]),

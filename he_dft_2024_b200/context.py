@@ -103,6 +103,13 @@ class Context:
                                                       dptr(pc)))
         return mu, err, pc
 
+    def qimp_moments_members(self):
+        """(members, nq, 4) array of norm, <x>, <y>, <z> per member and impurity."""
+        nq = self.w.nq_imp
+        out = np.zeros(self.members * nq * 4)
+        self._ck(self.L.he_qimp_moments_members(self.h, dptr(out)))
+        return out.reshape(self.members, nq, 4)
+
     def energy_members(self):
         out = (_lib.HeEnergies * self.members)()
         self._ck(self.L.he_energy_members(self.h, out))

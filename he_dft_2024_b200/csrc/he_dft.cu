@@ -1694,7 +1694,7 @@ static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a) {
   const int tk = (N > 0) ? TILE : ctx->tkx;
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
-  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, 1);
+  dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, ctx->nmem);
   CK(set_smem_attr((const void*)k_zmix<N, TILE, Rt>, smem));
   tname(ctx, a.nout == 0 ? "fft_z_fwd" : a.fwd_in ? "fft_z_mix_fwd" : "fft_z_mix");
   k_zmix<N, TILE, Rt><<<grid, nthr, smem, ctx->stream>>>(a);
@@ -1717,6 +1717,7 @@ static int zmix_t(he_ctx_t* ctx, const ZMixArgs& a) {
 static int zmix(he_ctx_t* ctx, ZMixArgs a) {
   a.nxh = ctx->nxh; a.ny = ctx->ny; a.nz = ctx->nz; a.tkx = ctx->tkx;
   a.pl = ctx->plz;
+  a.mm = ctx->mm;
   if (!ctx->mixed) return zmix_t<double>(ctx, a);
   // the binary32 chain reads the kernels' binary32 copies (passed through the same slots)
   for (int o = 0; o < a.nout; ++o)
@@ -1864,10 +1865,12 @@ static int q_field(he_ctx_t* ctx) {
 static int q_cnorm2(he_ctx_t* ctx, int i) {
   tname(ctx, "impurity_density");
   if (ctx->mixed)
-    k_cnorm2_pair<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
-        (const float2*)ctx->psix[i], (const float2*)ctx->psix[i] + ctx->N, (float*)ctx->denx[i], ctx->N);
+    k_cnorm2_pair<<<pw_grid(ctx), 256, 0, ctx->stream>>>(
+        (const float2*)ctx->psix[i], (const float2*)ctx->psix[i] + ctx->N, (float*)ctx->denx[i], ctx->N,
+        ctx->mm);
   else
-    k_cnorm2<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const double2*)ctx->psix[i], ctx->denx[i], ctx->N);
+    k_cnorm2<<<pw_grid(ctx), 256, 0, ctx->stream>>>((const double2*)ctx->psix[i], ctx->denx[i], ctx->N,
+                                                    ctx->mm);
   LAUNCHED();
   return HE_OK;
 }
@@ -2056,16 +2059,16 @@ static int q_steppc(he_ctx_t* ctx, double deltat, double* errHe, double* errpsix
 static int q_dot(he_ctx_t* ctx, const double* x, const double* y, int slot) {
   tname(ctx, "dot_reduce");
   if (ctx->mixed)
-    k_dot_f32<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((const float*)x, (const float*)y, ctx->N,
-                                                        tail(ctx, slot));
+    k_dot_f32<<<pw_grid(ctx), 256, 0, ctx->stream>>>((const float*)x, (const float*)y, ctx->N,
+                                                      tail(ctx, slot), ctx->mm);
   else
-    k_dot<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(x, y, ctx->N, tail(ctx, slot));
+    k_dot<<<pw_grid(ctx), 256, 0, ctx->stream>>>(x, y, ctx->N, tail(ctx, slot), ctx->mm);
   LAUNCHED();
   return HE_OK;
 }
 
 // energy (Dynamics_quantum_impurities/energy.f90:12-139).  sto2 of the reference lands in t4.
-static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
+static int q_energy_launch(he_ctx_t* ctx) {
   const int n = ctx->nq;
   if (ctx->mixed) {
     OpEnergy<float2> op{};
@@ -2109,8 +2112,13 @@ static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
       TRY(q_dot(ctx, ctx->t4, ctx->denx[m], S_QII + pair));
     }
   if (ctx->otc) TRY(alfa_energy_sum(ctx));
-  TRY(read_sums(ctx));
-  const double* s = ctx->hsum + S_EN;
+  return HE_OK;
+}
+// The quantum energies from one member's reduction slots h (S_COUNT values).
+static void q_energy_from(const he_ctx_t* ctx, const double* h, const double* ealphas,
+                          he_energies_t* out) {
+  const int n = ctx->nq;
+  const double* s = h + S_EN;
   const double dxyz = ctx->dxyz;
   he_energies_t e{};
   e.esolid = ctx->fn.lsolid ? ctx->fn.C * s[3] * dxyz : 0.0;
@@ -2118,21 +2126,28 @@ static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
   e.elj4 = 0.5 * s[1] * dxyz;
   e.ecor4 = s[2] * dxyz;
   e.etot4 = e.ekin4 + e.elj4 + e.ecor4 + e.esolid;
-  if (ctx->otc) {
-    e.ealphas = alfa_energy(ctx);
+  if (ealphas) {
+    e.ealphas = *ealphas;
     e.etot4 = e.etot4 + e.ealphas;
   }
-  for (int k = 0; k < n; ++k) e.ekinx = e.ekinx + ctx->h2o2mx[k] * ctx->hsum[S_QEK + k];
+  for (int k = 0; k < n; ++k) e.ekinx = e.ekinx + ctx->h2o2mx[k] * h[S_QEK + k];
   e.ekinx = e.ekinx * dxyz;
-  e.eHeX = ctx->hsum[S_QHEX] * dxyz;
-  pair = 0;
+  e.eHeX = h[S_QHEX] * dxyz;
+  int pair = 0;
   for (int k = 0; k < n; ++k)
     for (int m = k + 1; m < n; ++m, ++pair)
-      if (ctx->uimpkk[k + kMaxQImp * m]) e.eimpu_impu = e.eimpu_impu + ctx->hsum[S_QII + pair];
+      if (ctx->uimpkk[k + kMaxQImp * m]) e.eimpu_impu = e.eimpu_impu + h[S_QII + pair];
   e.eimpu_impu = e.eimpu_impu * dxyz;
   e.eimpu = e.ekinx + e.eHeX + e.eimpu_impu;
   e.etot = e.etot4 + e.eimpu;
   *out = e;
+}
+static int q_energy(he_ctx_t* ctx, he_energies_t* out) {
+  TRY(q_energy_launch(ctx));
+  TRY(read_sums(ctx));
+  double ea = 0.0;
+  if (ctx->otc) ea = alfa_energy(ctx);
+  q_energy_from(ctx, ctx->hsum, ctx->otc ? &ea : nullptr, out);
   return HE_OK;
 }
 
@@ -2786,8 +2801,9 @@ int he_ctx_group(he_ctx_t* const* ctxs, int n) {
   he_ctx_t* L = ctxs[0];
   if (L->nmem != 1) return fail(L, HE_ERR_STATE, "the context already leads a group");
   if (n == 1) return HE_OK;
-  if (L->mode != HE_MODE_STATICS || L->mixed || L->otc)
-    return fail(L, HE_ERR_ARG, "groups run the binary64 statics mode with the OT or OP core");
+  if (L->otc || !((L->mode == HE_MODE_STATICS && !L->mixed) || L->mode == HE_MODE_QUANTUM))
+    return fail(L, HE_ERR_ARG, "groups run the binary64 statics mode or the quantum-impurity mode "
+                               "(either precision) with the OT or OP core");
   for (int m = 0; m < n; ++m) {
     he_ctx_t* c = ctxs[m];
     if (!c) return fail(L, HE_ERR_ARG, "null member %d", m);
@@ -2795,11 +2811,14 @@ int he_ctx_group(he_ctx_t* const* ctxs, int n) {
       if (ctxs[j] == c) return fail(L, HE_ERR_ARG, "member %d repeats member %d", m, j);
     if (c->nmem != 1 || c->mode != L->mode || c->prec != L->prec || c->otc != L->otc ||
         c->nx != L->nx || c->ny != L->ny || c->nz != L->nz || c->xmax != L->xmax ||
-        c->ymax != L->ymax || c->zmax != L->zmax || c->icon != L->icon)
+        c->ymax != L->ymax || c->zmax != L->zmax || c->icon != L->icon || c->nq != L->nq ||
+        c->cglj_pending != L->cglj_pending)
       return fail(L, HE_ERR_ARG, "member %d differs from the leader (mode, precision, grid or core)", m);
     if (!c->kernels_ok) return fail(L, HE_ERR_STATE, "member %d has no k-space kernels", m);
+    for (int i = 0; i < L->nq; ++i)
+      if (c->h2o2mx[i] != L->h2o2mx[i]) return fail(L, HE_ERR_ARG, "member %d's impurity masses differ", m);
     // derden's gradients are allocated on first use; every member holds them before pairing
-    if (!c->dxden) {
+    if (L->mode == HE_MODE_STATICS && !c->dxden) {
       TRY(dalloc_t(c, &c->dxden, c->N));
       TRY(dalloc_t(c, &c->dyden, c->N));
       TRY(dalloc_t(c, &c->dzden, c->N));
@@ -2831,14 +2850,23 @@ int he_ctx_group(he_ctx_t* const* ctxs, int n) {
       if (c->allocs[i] == p) return (long)i;
     return -1;
   };
+  auto ring = [](const he_ctx_t* c) {
+    std::vector<const void*> v = {c->psi, c->scratch, c->psiold[0], c->psiold[1], c->psiold[2],
+                                  c->hpsiold[0], c->hpsiold[1], c->xscratch};
+    for (int i = 0; i < c->nq; ++i) {
+      v.push_back(c->psix[i]);
+      for (int k = 0; k < 3; ++k) v.push_back(c->psixold[i][k]);
+      for (int k = 0; k < 2; ++k) v.push_back(c->hpsixold[i][k]);
+    }
+    return v;
+  };
+  const std::vector<const void*> lr = ring(L);
   for (int m = 1; m < n; ++m) {
     const he_ctx_t* c = ctxs[m];
-    const void* lp[6] = {L->psi, L->scratch, L->psiold[0], L->psiold[1], L->psiold[2], L->hpsiold[0]};
-    const void* cp[6] = {c->psi, c->scratch, c->psiold[0], c->psiold[1], c->psiold[2], c->hpsiold[0]};
-    for (int k = 0; k < 6; ++k)
-      if (index_of(L, lp[k]) != index_of(c, cp[k]))
-        return fail(L, HE_ERR_STATE, "member %d's ring buffers are relabelled differently from the leader's", m);
-    if (index_of(L, L->hpsiold[1]) != index_of(c, c->hpsiold[1]))
+    const std::vector<const void*> cr = ring(c);
+    bool same = std::equal(c->ioldp, c->ioldp + 3, L->ioldp) && std::equal(c->ioldh, c->ioldh + 2, L->ioldh);
+    for (size_t k = 0; k < lr.size() && same; ++k) same = index_of(L, lr[k]) == index_of(c, cr[k]);
+    if (!same)
       return fail(L, HE_ERR_STATE, "member %d's ring buffers are relabelled differently from the leader's", m);
   }
   unsigned long long* dt = nullptr;
@@ -2872,9 +2900,23 @@ static int member_xfer(he_ctx_t* ctx, int member, int field, void* host, size_t 
   if (bytes != r.bytes) return fail(ctx, HE_ERR_ARG, "field %d: expected %zu bytes, got %zu", field, r.bytes, bytes);
   void* d = member_ptr(ctx, r.ptr, member);
   if (d == r.ptr) return fail(ctx, HE_ERR_STATE, "field %d is not a per-member buffer", field);
-  if (up) CK(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  else CK(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  return sync_all(ctx);
+  const FieldFmt fmt = field_fmt(ctx, field);  // binary32 storage of the mixed path converts
+  if (fmt == FMT_F64) {
+    if (up) CK(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    else CK(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_all(ctx);
+  }
+  std::vector<unsigned char> dev;
+  if (up) {
+    to_device_fmt(fmt, host, bytes, dev);
+    CK(cudaMemcpyAsync(d, dev.data(), dev.size(), cudaMemcpyHostToDevice, ctx->stream));
+    return sync_all(ctx);
+  }
+  dev.resize(device_fmt_bytes(fmt, bytes));
+  CK(cudaMemcpyAsync(dev.data(), d, dev.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  TRY(sync_all(ctx));
+  from_device_fmt(fmt, dev, host, bytes);
+  return HE_OK;
 }
 int he_upload_member(he_ctx_t* ctx, int member, int field, const void* host, size_t bytes) {
   return member_xfer(ctx, member, field, const_cast<void*>(host), bytes, true);
@@ -2905,7 +2947,16 @@ int he_member_mu(he_ctx_t* ctx, int n4, int after_rk, double* mu4) {
 
 int he_energy_members(he_ctx_t* ctx, he_energies_t* out) {
   if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
-  if (ctx->mode != HE_MODE_STATICS || ctx->mixed) return fail(ctx, HE_ERR_STATE, "binary64 statics groups only");
+  if (ctx->mode == HE_MODE_QUANTUM && !ctx->otc) {
+    if (ctx->nq == 0) return fail(ctx, HE_ERR_STATE, "he_set_quantum_impurities first");
+    TRY(q_energy_launch(ctx));
+    std::vector<double> all;
+    TRY(member_sums(ctx, all));
+    for (int m = 0; m < ctx->nmem; ++m) q_energy_from(ctx, all.data() + (size_t)m * S_COUNT, nullptr, &out[m]);
+    return HE_OK;
+  }
+  if (ctx->mode != HE_MODE_STATICS || ctx->mixed || ctx->otc)
+    return fail(ctx, HE_ERR_STATE, "members' energies: binary64 statics or quantum groups (OT/OP cores)");
   TRY(he_energy(ctx, &out[0]));
   std::vector<double> all;
   TRY(member_sums(ctx, all));
@@ -3878,13 +3929,13 @@ int he_qimp_moments(he_ctx_t* ctx, double* out) {
   for (int i = 0; i < ctx->nq; ++i) {
     tname(ctx, "impurity_moments");
     if (ctx->mixed)
-      k_moments<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
+      k_moments<<<pw_grid(ctx), 256, 0, ctx->stream>>>(
           (const float2*)ctx->psix[i], ctx->nx, ctx->ny, ctx->N, -ctx->xmax, -ctx->ymax, -ctx->zmax,
-          ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i));
+          ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i), ctx->mm);
     else
-      k_moments<<<pw_blocks(ctx), 256, 0, ctx->stream>>>(
+      k_moments<<<pw_grid(ctx), 256, 0, ctx->stream>>>(
           (const double2*)ctx->psix[i], ctx->nx, ctx->ny, ctx->N, -ctx->xmax, -ctx->ymax, -ctx->zmax,
-          ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i));
+          ctx->hx, ctx->hy, ctx->hz, tail(ctx, S_QMOM + 4 * i), ctx->mm);
     LAUNCHED();
   }
   TRY(read_sums(ctx));
@@ -3896,6 +3947,25 @@ int he_qimp_moments(he_ctx_t* ctx, double* out) {
     out[4 * i + 2] = m[2] * ctx->dxyz / a;
     out[4 * i + 3] = m[3] * ctx->dxyz / a;
   }
+  return HE_OK;
+}
+
+int he_qimp_moments_members(he_ctx_t* ctx, double* out) {
+  if (!ctx || !out) return fail(ctx, HE_ERR_ARG, "null argument");
+  std::vector<double> m0(4 * (size_t)std::max(ctx->nq, 1));
+  TRY(he_qimp_moments(ctx, m0.data()));
+  std::vector<double> all;
+  TRY(member_sums(ctx, all));
+  for (int mb = 0; mb < ctx->nmem; ++mb)
+    for (int i = 0; i < ctx->nq; ++i) {
+      const double* m = all.data() + (size_t)mb * S_COUNT + S_QMOM + 4 * i;
+      double* o = out + 4 * ((size_t)mb * ctx->nq + i);
+      const double a = m[0] * ctx->dxyz;
+      o[0] = a;
+      o[1] = m[1] * ctx->dxyz / a;
+      o[2] = m[2] * ctx->dxyz / a;
+      o[3] = m[3] * ctx->dxyz / a;
+    }
   return HE_OK;
 }
 

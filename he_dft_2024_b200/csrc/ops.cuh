@@ -11,6 +11,11 @@ struct Timec {
   const double* ay;
   const double* az;
   double lambdah;
+  HE_D void remap(const MemberMap& mm, int m) {
+    ax = mm(ax, m);
+    ay = mm(ay, m);
+    az = mm(az, m);
+  }
   HE_D double re(int ix, int iy, int iz) const {
     double s = 1.0 + ax[ix];
     s = s + 1.0 + ay[iy];
@@ -18,6 +23,13 @@ struct Timec {
     return lambdah * s;
   }
 };
+
+
+// remap helpers for the Ops' operand arrays
+template <class P, int K>
+HE_D void remap_all(P* (&a)[K], const MemberMap& mm, int m) {
+  for (int k = 0; k < K; ++k) a[k] = mm(a[k], m);
+}
 
 // H psi of the real-time classical path (steprk.f90:67, steppc.f90:51,118):
 //   timec*((d2x+d2y+d2z)*h2o2m4 - pot4*psi) - i*uimp*psi,  timec = (tr, 1).
@@ -65,6 +77,10 @@ struct OpPredictT {
   double* den;
   Timec tm;
   double h2o2m, s43, c112, mu;
+  HE_D void remap(const MemberMap& mm, int m) {
+    remap_all(s8, mm, m); remap_all(s16, mm, m);
+    po3 = mm(po3, m); h2 = mm(h2, m); pc = mm(pc, m); den = mm(den, m); tm.remap(mm, m);
+  }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
                const double* v8, const double2* v16, int vs, double*) const {
     const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
@@ -93,6 +109,10 @@ struct OpCorrectT {
   double* den;
   Timec tm;
   double h2o2m, s3, c9, mu;
+  HE_D void remap(const MemberMap& mm, int m) {
+    remap_all(s8, mm, m); remap_all(s16, mm, m);
+    pc = mm(pc, m); out = mm(out, m); den = mm(den, m); tm.remap(mm, m);
+  }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
                const double* v8, const double2* v16, int vs, double* acc) const {
     const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
@@ -124,6 +144,10 @@ struct OpRKT {
   double* den;
   Timec tm;
   double h2o2m, a, b, cc, dt, mu;
+  HE_D void remap(const MemberMap& mm, int m) {
+    remap_all(s8, mm, m); remap_all(s16, mm, m);
+    q = mm(q, m); out = mm(out, m); hsave = mm(hsave, m); den = mm(den, m); tm.remap(mm, m);
+  }
   HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
                const double* v8, const double2* v16, int vs, double*) const {
     const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
@@ -204,6 +228,11 @@ struct OpRKMT {
   float* den;
   Timec tm;
   float h2o2m, a, b, cc, dt, mu;
+  HE_D void remap(const MemberMap& mm, int m) {
+    remap_all(s8, mm, m); remap_all(s16, mm, m);
+    q = mm(q, m); out_hi = mm(out_hi, m); out_lo = mm(out_lo, m); hsave = mm(hsave, m);
+    den = mm(den, m); tm.remap(mm, m);
+  }
   HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
                const float* v8, const float2* v16, int vs, double*) const {
     const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
@@ -234,6 +263,11 @@ struct OpPredictMT {
   float* den;
   Timec tm;
   float h2o2m, s43, c112, mu;
+  HE_D void remap(const MemberMap& mm, int m) {
+    remap_all(s8, mm, m); remap_all(s16, mm, m);
+    po3_hi = mm(po3_hi, m); po3_lo = mm(po3_lo, m); h2 = mm(h2, m); den = mm(den, m);
+    tm.remap(mm, m);
+  }
   HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
                const float* v8, const float2* v16, int vs, double*) const {
     const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
@@ -265,6 +299,11 @@ struct OpCorrectMT {
   float* den;
   Timec tm;
   float h2o2m, s3, c9, c112, mu;
+  HE_D void remap(const MemberMap& mm, int m) {
+    remap_all(s8, mm, m); remap_all(s16, mm, m);
+    pc = mm(pc, m); out_hi = mm(out_hi, m); out_lo = mm(out_lo, m); den = mm(den, m);
+    tm.remap(mm, m);
+  }
   HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
                const float* v8, const float2* v16, int vs, double* acc) const {
     const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);

@@ -36,6 +36,7 @@ struct OpGrad2T {
   static constexpr int NV = 1, N8 = 0, N16 = 0;
   const R* s8[1];
   const Z* s16[1];
+  HE_D void remap(const MemberMap&, int) {}  // no pointers besides the stencil's field
   HE_D static double n2(TT v) { return (double)v.x * (double)v.x + (double)v.y * (double)v.y; }
   HE_D void at(int, int, int, long, TT dx, TT dy, TT dz, TT, const R*, const Z*, int,
                double* acc) const {
@@ -54,11 +55,25 @@ struct ZMixArgs {
   int nterm[2];
   const double2* src[2][kMaxTerms];  // full spectra; null = the forward spectrum of fwd_in
   const double* ker[2][kMaxTerms];   // real kernels over the half spectrum
+  MemberMap mm;                      // group members (blockIdx.z is the member)
+  HE_D void remap(int m) {
+    fwd_in = mm(fwd_in, m);
+    fwd_store = mm(fwd_store, m);
+    for (int o = 0; o < 2; ++o) {
+      out[o] = mm(out[o], m);
+      for (int t = 0; t < kMaxTerms; ++t) {
+        src[o][t] = mm(src[o][t], m);
+        ker[o][t] = mm(ker[o][t], m);
+      }
+    }
+  }
 };
 
 // Rt = float: the mixed path (binary32 spectra, kernels given as their binary32 copies).
 template <int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
+__global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a_in) {
+  ZMixArgs a = a_in;
+  a.remap(blockIdx.z);
   using C = typename Cx<Rt>::T;
   C* smem = smem_as<C>();
   const C* fwd_in = reinterpret_cast<const C*>(a.fwd_in);
@@ -138,13 +153,18 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a) {
 
 // ---- pointwise passes (grid-stride, deterministic two-level reductions) -----------------------
 __global__ void __launch_bounds__(256) k_cnorm2(const double2* __restrict__ f, double* __restrict__ out,
-                                                long N) {
+                                                long N, const MemberMap mm) {
+  f = mm(f, blockIdx.y);
+  out = mm(out, blockIdx.y);
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
     out[i] = cnorm2(f[i]);
 }
 
 __global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const double* __restrict__ b,
-                                             long N, const ReduceTail rt) {
+                                             long N, const ReduceTail rt_in, const MemberMap mm) {
+  a = mm(a, blockIdx.y);
+  b = mm(b, blockIdx.y);
+  const ReduceTail rt = remap(rt_in, mm, blockIdx.y);
   double acc[1] = {0.0};
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
     acc[0] += a[i] * b[i];
@@ -155,7 +175,11 @@ __global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const
 // The mixed path: |psix|^2 of the compensated pair (hi and lo planes), rounded once to binary32.
 __global__ void __launch_bounds__(256) k_cnorm2_pair(const float2* __restrict__ hi,
                                                      const float2* __restrict__ lo,
-                                                     float* __restrict__ out, long N) {
+                                                     float* __restrict__ out, long N,
+                                                     const MemberMap mm) {
+  hi = mm(hi, blockIdx.y);
+  lo = mm(lo, blockIdx.y);
+  out = mm(out, blockIdx.y);
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
     const double re = (double)hi[i].x + (double)lo[i].x, im = (double)hi[i].y + (double)lo[i].y;
     out[i] = (float)(re * re + im * im);
@@ -164,7 +188,10 @@ __global__ void __launch_bounds__(256) k_cnorm2_pair(const float2* __restrict__ 
 
 // sum a*b of binary32 fields, summed in binary64 (the mixed path's energy sums).
 __global__ void __launch_bounds__(256) k_dot_f32(const float* __restrict__ a, const float* __restrict__ b,
-                                                 long N, const ReduceTail rt) {
+                                                 long N, const ReduceTail rt_in, const MemberMap mm) {
+  a = mm(a, blockIdx.y);
+  b = mm(b, blockIdx.y);
+  const ReduceTail rt = remap(rt_in, mm, blockIdx.y);
   double acc[1] = {0.0};
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
     acc[0] += (double)a[i] * (double)b[i];
@@ -177,7 +204,10 @@ __global__ void __launch_bounds__(256) k_dot_f32(const float* __restrict__ a, co
 template <typename C>
 __global__ void __launch_bounds__(256) k_moments(const C* __restrict__ f, int nx, int ny, long N,
                                                  double x0, double y0, double z0, double hx,
-                                                 double hy, double hz, const ReduceTail rt) {
+                                                 double hy, double hz, const ReduceTail rt_in,
+                                                 const MemberMap mm) {
+  f = mm(f, blockIdx.y);
+  const ReduceTail rt = remap(rt_in, mm, blockIdx.y);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
     const long r = i / nx;

@@ -333,11 +333,12 @@ int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
 /* ---- groups: several statics droplets advanced by one launch per kernel ----
  * No counterpart in the reference (its drivers run one droplet per process).  he_ctx_group makes
- * ctxs[0] the leader of n contexts created alike (same mode, precision, grid and functional;
- * binary64 statics mode, OT or OP core), each set up on its own (uploads, he_set_kernels or
+ * ctxs[0] the leader of n contexts created alike (same mode, precision, grid, functional and
+ * impurity masses; binary64 statics or quantum-impurity mode, OT or OP core), each set up on its own (uploads, he_set_kernels or
  * he_compute_kernels) and in the same ring state.  From then on every routine called on the
  * leader launches each kernel once with a grid dimension over the members, and every member's
- * CTAs work on that member's buffers; the members' contexts must stay alive and must not be
+ * CTAs work on that member's buffers (the quantum-impurity mode groups too, in either precision:
+ * the members there are trajectories, e.g. with different impurity kicks); the members' contexts must stay alive and must not be
  * called directly until the leader is destroyed.  Scalars the leader's routines return are
  * member 0's; the *_members calls below return every member's, and he_upload_member /
  * he_download_member move member m's module arrays (m = 0 is the leader).  Routines outside the
@@ -355,8 +356,11 @@ int he_member_mu(he_ctx_t* ctx, int n4, int after_rk, double* mu4);
  * values; mu4 carries each member's previous value in (used when niter = 1). */
 int he_statics_iterations_members(he_ctx_t* ctx, int niter, double deltat, int n4, double* mu4,
                                   double* mu4err, double* errpc);
-/* energy() of every member into out[he_group_size(ctx)]. */
+/* energy() of every member into out[he_group_size(ctx)] (statics and quantum groups). */
 int he_energy_members(he_ctx_t* ctx, he_energies_t* out);
+/* he_qimp_moments of every member: out[4 (m nq + i) + 0..3] = norm, <x>, <y>, <z> of member m's
+ * impurity i. */
+int he_qimp_moments_members(he_ctx_t* ctx, double* out);
 
 /* ---- energy sums without device allocation ----
  * No counterpart in the reference.  For callers that cannot let a library allocate device

@@ -82,3 +82,48 @@ def test_groups_outside_their_scope_are_refused():
     finally:
         for c in (a, b, d):
             c.close()
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_quantum_group_members_equal_trajectories_run_alone(precision):
+    """Three quantum-impurity trajectories with different kicks on 32^3 (one 23 u impurity each):
+    set up on their own, then grouped; RK-Gill start and predictor-corrector steps with one launch
+    per kernel must leave every member exactly as the trajectory run alone (psi, psix, energies,
+    impurity moments)."""
+    ws = [C.replace(C.quantum_2000(n=32, speed_ms=s, direction=d), n4=300, xmax=12.0, ymax=12.0,
+                    zmax=12.0, deltatps=5e-4)
+          for s, d in ((100.0, (0, 0, 1)), (250.0, (1, 0, 0)), (400.0, (0, 1, 1)))]
+    steps = 6
+
+    def make(w):
+        c = Context(w, mode="quantum", precision=precision)
+        c.set_fft_variant("x", 0, 8)
+        c.set_fft_variant("y", 1, 8)
+        c.set_fft_variant("z", 0, 8)
+        den = C.woods_saxon(w)
+        D.quantum_setup(c, D.initial_wavefunction(w, den), [C.psix_initial(w, 0)])
+        return c
+
+    ref = []
+    for w in ws:
+        with make(w) as c:
+            for it in range(1, steps + 1):
+                D.quantum_iteration(c, it, w.deltat)
+            ref.append(dict(psi=c.download("psi"), psix=c.download("psix"), e=c.energy(),
+                            mom=c.qimp_moments()))
+    ctxs = [make(w) for w in ws]
+    lead = ctxs[0]
+    try:
+        lead.group(ctxs[1:])
+        for it in range(1, steps + 1):
+            D.quantum_iteration(lead, it, ws[0].deltat)
+        es = lead.energy_members()
+        mom = lead.qimp_moments_members()
+        got = [dict(psi=lead.download_member(m, "psi")) for m in range(3)]
+    finally:
+        lead.close()
+    for m in range(3):
+        assert np.array_equal(got[m]["psi"], ref[m]["psi"]), m
+        for k in ("etot", "ekin4", "ekinx", "eHeX"):
+            assert es[m][k] == ref[m]["e"][k], (m, k, es[m][k], ref[m]["e"][k])
+        assert np.array_equal(mom[m], ref[m]["mom"]), m
