@@ -13,6 +13,7 @@
 namespace he {
 
 // falfs and the three sources falfs * d{x,y,z}den (term_alfa.f90:28-36).
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_alf_src(const double* __restrict__ denalf,
                                                  const double* __restrict__ dx, const double* __restrict__ dy,
                                                  const double* __restrict__ dz, double den0s, long N,
@@ -26,8 +27,10 @@ __global__ void __launch_bounds__(256) k_alf_src(const double* __restrict__ dena
     s3[i] = f * dz[i];
   }
 }
+#endif
 
 // grad den . int alf (term_alfa.f90:65-69).
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_alf_dot(const double* __restrict__ dx, const double* __restrict__ dy,
                                                  const double* __restrict__ dz, const double* __restrict__ ix,
                                                  const double* __restrict__ iy, const double* __restrict__ iz,
@@ -35,8 +38,10 @@ __global__ void __launch_bounds__(256) k_alf_dot(const double* __restrict__ dx, 
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
     out[i] = dx[i] * ix[i] + dy[i] * iy[i] + dz[i] * iz[i];
 }
+#endif
 
 // falfs * int{x,y,z}alf (term_alfa.f90:87-92).
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_alf_fi(const double* __restrict__ falfs, const double* __restrict__ ix,
                                                 const double* __restrict__ iy, const double* __restrict__ iz,
                                                 long N, double* __restrict__ s1, double* __restrict__ s2,
@@ -48,6 +53,7 @@ __global__ void __launch_bounds__(256) k_alf_fi(const double* __restrict__ falfs
     s3[i] = f * iz[i];
   }
 }
+#endif
 
 // One component of the divergence: out = d f / d axis (derivnD(1,...) of term_alfa.f90:106-108).
 template <int AX>
@@ -82,6 +88,7 @@ struct OpAlfFinal {
 };
 
 // sum falfs (dxden intxalf + dyden intyalf + dzden intzalf) (energy.f90:131-135).
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_alf_energy(const double* __restrict__ falfs,
                                                     const double* __restrict__ dx, const double* __restrict__ dy,
                                                     const double* __restrict__ dz, const double* __restrict__ ix,
@@ -93,5 +100,6 @@ __global__ void __launch_bounds__(256) k_alf_energy(const double* __restrict__ f
   block_reduce_store<1>(acc, rt.partials + blockIdx.x);
   reduce_tail<1>(rt, gridDim.x);
 }
+#endif
 
 }  // namespace he

@@ -192,6 +192,18 @@ struct MemberMap {
   }
 };
 
+// Pointer p of member m: mapped through mm in the group instantiation (G) of a kernel, returned
+// unchanged otherwise.
+template <bool G, class T>
+HE_D T* on_member(const MemberMap& mm, T* p, int m) {
+  if constexpr (G) return mm(p, m);
+  else return p;
+}
+
+// The heavy kernel templates (stencils, FFT passes) are compiled in their own translation units,
+// which define HE_KERNEL_TU and instantiate the kernels the host code launches; the host
+// translation unit sees their declarations only.
+
 // ---- block reduction of NV doubles (fixed order => deterministic) ------------------------------
 template <int NV>
 __device__ void block_reduce_store(double (&v)[NV], double* __restrict__ out) {

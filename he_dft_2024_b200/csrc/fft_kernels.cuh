@@ -57,12 +57,6 @@ struct XArgs {
   int lsolid;
   double C, beta, den_m;
   MemberMap mm;              // group members (blockIdx.y is the member)
-  HE_D void remap(int m) {
-    den = mm(den, m); dencg_in = mm(dencg_in, m); delj4_in = mm(delj4_in, m);
-    specA = mm(specA, m); specB = mm(specB, m);
-    out1 = mm(out1, m); out2 = mm(out2, m);
-    extra = mm(extra, m); extra2 = mm(extra2, m);
-  }
 };
 
 HE_D double corr_source(double den, double dcg, double cp4, double cpp4) {
@@ -134,21 +128,22 @@ HE_HD size_t xpass_smem(int stw_len, int rb, int n) {
 // tile's contiguous row ranges into the other stage buffer), so the load latency that bounds a
 // load-transform-store CTA is hidden behind the transform.
 constexpr int kXPipeThreads = 256;  // threads of a pipelined x-pass CTA, whatever its rows
-template <int MODE, int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a_in) {
+template <int MODE, int N, int TILE, typename Rt, bool G>
+__global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
-  XArgs a = a_in;
-  a.remap(blockIdx.y);
+  const int mem = G ? (int)blockIdx.y : 0;  // G: blockIdx.y is the group member
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
   using ST = XStage<MODE>;
-  const Rs* extra = reinterpret_cast<const Rs*>(a.extra);
-  const Rs* extra2 = reinterpret_cast<const Rs*>(a.extra2);
-  Rs* out1 = reinterpret_cast<Rs*>(a.out1);
-  Rs* out2 = reinterpret_cast<Rs*>(a.out2);
+  const Rs* extra = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.extra, mem));
+  const Rs* extra2 = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.extra2, mem));
+  Rs* out1 = reinterpret_cast<Rs*>(on_member<G>(a.mm, a.out1, mem));
+  Rs* out2 = reinterpret_cast<Rs*>(on_member<G>(a.mm, a.out2, mem));
   C* smem = smem_as<C>();
-  C* specA = reinterpret_cast<C*>(a.specA);
-  const C* specB = reinterpret_cast<const C*>(a.specB);
+  C* specA = reinterpret_cast<C*>(on_member<G>(a.mm, a.specA, mem));
+  const C* specB = reinterpret_cast<const C*>(on_member<G>(a.mm, a.specB, mem));
   const int n = (N > 0) ? N : a.nx;
   const int nxh = n / 2 + 1;
   const int ls = line_stride(n);
@@ -163,9 +158,9 @@ __global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a_in) {
   const size_t spec_bytes = (size_t)RB * nxh * sizeof(C), real_bytes = (size_t)RB * n * sizeof(Rs);
   // real arrays staged per mode (prologue or epilogue inputs)
   const void* rsrc[3] = {nullptr, nullptr, nullptr};
-  if constexpr (MODE == X_R2C_DEN || MODE == X_C2R2_CORR) rsrc[0] = a.den;
-  if constexpr (MODE == X_R2C_CORR) { rsrc[0] = a.den; rsrc[1] = a.dencg_in; }
-  if constexpr (MODE == X_C2R_POT) { rsrc[0] = a.dencg_in; rsrc[1] = a.delj4_in; rsrc[2] = a.den; }
+  if constexpr (MODE == X_R2C_DEN || MODE == X_C2R2_CORR) rsrc[0] = on_member<G>(a.mm, a.den, mem);
+  if constexpr (MODE == X_R2C_CORR) { rsrc[0] = on_member<G>(a.mm, a.den, mem); rsrc[1] = on_member<G>(a.mm, a.dencg_in, mem); }
+  if constexpr (MODE == X_C2R_POT) { rsrc[0] = on_member<G>(a.mm, a.dencg_in, mem); rsrc[1] = on_member<G>(a.mm, a.delj4_in, mem); rsrc[2] = on_member<G>(a.mm, a.den, mem); }
   const int nreal = (MODE == X_C2R_POT && !a.lsolid) ? 2 : ST::nreal;  // den: penalty only
   auto issue = [&](int buf, long t) {
     unsigned char* st = stage0 + buf * sbytes;
@@ -276,26 +271,30 @@ __global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a_in) {
   }
   cp_async_wait<0>();
 }
+#else
+;
+#endif
 
 // One-shot variant of k_xpass: one CTA per row tile, loading its inputs straight from global
 // memory (no staging buffers, so less shared memory per CTA; the autotuner picks between the two).
-template <int MODE, int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a_in) {
+template <int MODE, int N, int TILE, typename Rt, bool G>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
-  XArgs a = a_in;
-  a.remap(blockIdx.y);
+  const int mem = G ? (int)blockIdx.y : 0;  // G: blockIdx.y is the group member
   using C = typename Cx<Rt>::T;
   using Rs = Rt;  // real-space fields: binary64, binary32 in the mixed path
-  const Rs* den = reinterpret_cast<const Rs*>(a.den);
-  const Rs* dencg_in = reinterpret_cast<const Rs*>(a.dencg_in);
-  const Rs* delj4_in = reinterpret_cast<const Rs*>(a.delj4_in);
-  const Rs* extra = reinterpret_cast<const Rs*>(a.extra);
-  const Rs* extra2 = reinterpret_cast<const Rs*>(a.extra2);
-  Rs* out1 = reinterpret_cast<Rs*>(a.out1);
-  Rs* out2 = reinterpret_cast<Rs*>(a.out2);
+  const Rs* den = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.den, mem));
+  const Rs* dencg_in = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.dencg_in, mem));
+  const Rs* delj4_in = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.delj4_in, mem));
+  const Rs* extra = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.extra, mem));
+  const Rs* extra2 = reinterpret_cast<const Rs*>(on_member<G>(a.mm, a.extra2, mem));
+  Rs* out1 = reinterpret_cast<Rs*>(on_member<G>(a.mm, a.out1, mem));
+  Rs* out2 = reinterpret_cast<Rs*>(on_member<G>(a.mm, a.out2, mem));
   C* smem = smem_as<C>();
-  C* specA = reinterpret_cast<C*>(a.specA);
-  const C* specB = reinterpret_cast<const C*>(a.specB);
+  C* specA = reinterpret_cast<C*>(on_member<G>(a.mm, a.specA, mem));
+  const C* specB = reinterpret_cast<const C*>(on_member<G>(a.mm, a.specB, mem));
   const int n = (N > 0) ? N : a.nx;
   const int nxh = n / 2 + 1;
   const int ls = line_stride(n);
@@ -388,6 +387,9 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a_in
     }
   }
 }
+#else
+;
+#endif
 
 struct YZArgs {
   int nxh, ny, nz;
@@ -405,20 +407,16 @@ struct YZArgs {
   const float* k2f;
   int narr;                  // k_ypass: arrays per member (blockIdx.z = member x narr + array)
   MemberMap mm;              // group members (k_zconv: blockIdx.z is the member)
-  HE_D void remap(int m) {
-    arr[0] = mm(arr[0], m); arr[1] = mm(arr[1], m);
-    io = mm(io, m); out2 = mm(out2, m); fden_out = mm(fden_out, m);
-    k1 = mm(k1, m); k2 = mm(k2, m); k1f = mm(k1f, m); k2f = mm(k2f, m);
-  }
 };
 
-template <int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a_in) {
+template <int N, int TILE, typename Rt, bool G>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
-  const int narr = a_in.narr > 0 ? a_in.narr : (int)gridDim.z;
-  YZArgs a = a_in;
-  a.remap((int)blockIdx.z / narr);
-  const int ai = (int)blockIdx.z % narr;
+  // G: blockIdx.z = member x narr + array; otherwise blockIdx.z is the array
+  const int mem = G ? (int)blockIdx.z / a.narr : 0;
+  const int ai = G ? (int)blockIdx.z % a.narr : (int)blockIdx.z;
   using C = typename Cx<Rt>::T;
   C* smem = smem_as<C>();
   const int n = (N > 0) ? N : a.ny;
@@ -428,7 +426,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a_in)
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int z = blockIdx.y;
-  C* arr = reinterpret_cast<C*>(a.arr[ai]);
+  C* arr = reinterpret_cast<C*>(on_member<G>(a.mm, a.arr[ai], mem));
   C* tw = smem;
   C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
   C* P1 = P0 + TK * ls;
@@ -447,20 +445,28 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a_in)
     if (kx < nxh) arr[base + kx + (long)nxh * j] = R[c * ls + sw<N>(j)];
   }
 }
+#else
+;
+#endif
 
-template <int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a_in) {
+template <int N, int TILE, typename Rt, bool G>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
-  YZArgs a = a_in;
-  a.remap(blockIdx.z);
+  const int mem = G ? (int)blockIdx.z : 0;  // G: blockIdx.z is the group member
   using C = typename Cx<Rt>::T;
   using X = Cx<Rt>;
   constexpr bool F32 = sizeof(Rt) == 4;
   C* smem = smem_as<C>();
-  C* io = reinterpret_cast<C*>(a.io);
-  C* out2 = reinterpret_cast<C*>(a.out2);
-  C* fden_out = reinterpret_cast<C*>(a.fden_out);
-  const bool two = F32 ? a.k2f != nullptr : a.k2 != nullptr;
+  C* io = reinterpret_cast<C*>(on_member<G>(a.mm, a.io, mem));
+  C* out2 = reinterpret_cast<C*>(on_member<G>(a.mm, a.out2, mem));
+  C* fden_out = reinterpret_cast<C*>(on_member<G>(a.mm, a.fden_out, mem));
+  const double* kern1 = on_member<G>(a.mm, a.k1, mem);
+  const double* kern2 = on_member<G>(a.mm, a.k2, mem);
+  const float* kern1f = on_member<G>(a.mm, a.k1f, mem);
+  const float* kern2f = on_member<G>(a.mm, a.k2f, mem);
+  const bool two = F32 ? kern2f != nullptr : kern2 != nullptr;
   const int n = (N > 0) ? N : a.nz;
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
@@ -496,10 +502,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a_in)
     const C f = F[s];
     if (fden_out) fden_out[g] = f;
     if (two) {
-      const Rt w2 = F32 ? Rt(a.k2f[g]) : Rt(a.k2[g]);
+      const Rt w2 = F32 ? Rt(kern2f[g]) : Rt(kern2[g]);
       P2[s] = X::make(f.x * w2, f.y * w2);
     }
-    const Rt w1 = F32 ? Rt(a.k1f[g]) : Rt(a.k1[g]);
+    const Rt w1 = F32 ? Rt(kern1f[g]) : Rt(kern1[g]);
     F[s] = X::make(f.x * w1, f.y * w1);
   }
   __syncthreads();
@@ -519,5 +525,8 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a_in)
     if (kx < nxh) out2[base + kx + plane * j] = R2[c * ls + sw<N>(j)];
   }
 }
+#else
+;
+#endif
 
 }  // namespace he

@@ -208,15 +208,17 @@ template <bool INV> struct RDft<16, INV> : RDftComp<4, 4, INV> {};
 // Threads of a y-pass CTA: TK columns x N2.
 HE_HD constexpr int yreg_threads(int n, int tk) { return tk * (n / split_n1(n)); }
 
-template <int N, int TK, bool INV, typename C>
+template <int N, int TK, bool INV, bool G, typename C>
 HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
   using Rt = decltype(T[0].x);
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   const int tid = threadIdx.x;
   const int nxh = a.nxh;
   const int kx0 = blockIdx.x * TK;
-  const int narr = a.narr > 0 ? a.narr : (int)gridDim.z;
-  C* arr = reinterpret_cast<C*>(a.mm(a.arr[blockIdx.z % narr], (int)blockIdx.z / narr));
+  // G: blockIdx.z = member x narr + array; otherwise blockIdx.z is the array
+  C* arr;
+  if constexpr (G) arr = reinterpret_cast<C*>(a.mm(a.arr[blockIdx.z % a.narr], (int)blockIdx.z / a.narr));
+  else arr = reinterpret_cast<C*>(a.arr[blockIdx.z]);
   const long base = (long)nxh * N * blockIdx.y;
   {
     const int c = tid % TK, am = tid / TK;  // phase A: column c, a = am
@@ -248,15 +250,20 @@ HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
   }
 }
 
-template <int N, int TK, typename Rt = double>
+template <int N, int TK, typename Rt, bool G>
 __global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs a,
-                                                                   const typename Cx<Rt>::T* tw2) {
+                                                                   const typename Cx<Rt>::T* tw2)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
   using C = typename Cx<Rt>::T;
   C* T = smem_as<C>();
-  if (a.inv) ypass_reg_body<N, TK, true>(a, tw2, T);
-  else ypass_reg_body<N, TK, false>(a, tw2, T);
+  if (a.inv) ypass_reg_body<N, TK, true, G>(a, tw2, T);
+  else ypass_reg_body<N, TK, false, G>(a, tw2, T);
 }
+#else
+;
+#endif
 
 // z pass of a convolution with the line transform in registers (N = N1 x N2, TK columns kx):
 //   phase A  (thread c, a):  x[kz = a + N2 m] from HBM, DFT_N1 over m, twiddle W_N^(a k1),
@@ -268,8 +275,8 @@ __global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs 
 //            into out2).
 // The forward spectrum never leaves registers between the two transforms, and a CTA needs one
 // (two for two kernels) N x TK exchange buffer instead of three line buffers.
-template <int N, int TK, typename C>
-HE_D void zconv_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T0, C* T1) {
+template <int N, int TK, bool G, typename C>
+HE_D void zconv_reg_body(const YZArgs& a, int mem, const C* __restrict__ tw2, C* T0, C* T1) {
   using Rt = decltype(T0[0].x);
   using X = Cx<Rt>;
   constexpr bool F32 = sizeof(Rt) == 4;
@@ -279,10 +286,14 @@ HE_D void zconv_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T0, C* T
   const int kx0 = blockIdx.x * TK;
   const long plane = (long)nxh * a.ny;
   const long base = (long)nxh * blockIdx.y;
-  C* io = reinterpret_cast<C*>(a.io);
-  C* out2 = reinterpret_cast<C*>(a.out2);
-  C* fden_out = reinterpret_cast<C*>(a.fden_out);
-  const bool two = F32 ? a.k2f != nullptr : a.k2 != nullptr;
+  C* io = reinterpret_cast<C*>(on_member<G>(a.mm, a.io, mem));
+  C* out2 = reinterpret_cast<C*>(on_member<G>(a.mm, a.out2, mem));
+  C* fden_out = reinterpret_cast<C*>(on_member<G>(a.mm, a.fden_out, mem));
+  const double* kern1 = on_member<G>(a.mm, a.k1, mem);
+  const double* kern2 = on_member<G>(a.mm, a.k2, mem);
+  const float* kern1f = on_member<G>(a.mm, a.k1f, mem);
+  const float* kern2f = on_member<G>(a.mm, a.k2f, mem);
+  const bool two = F32 ? kern2f != nullptr : kern2 != nullptr;
   {
     const int c = tid % TK, am = tid / TK;
     const int kx = kx0 + c;
@@ -313,10 +324,10 @@ HE_D void zconv_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T0, C* T
       const long g = g0 + plane * N1 * k2;
       if (ok && fden_out) fden_out[g] = u[k2];
       if (two) {
-        const Rt w2 = ok ? (F32 ? Rt(a.k2f[g]) : Rt(a.k2[g])) : Rt(0);
+        const Rt w2 = ok ? (F32 ? Rt(kern2f[g]) : Rt(kern2[g])) : Rt(0);
         w[k2] = X::make(u[k2].x * w2, u[k2].y * w2);
       }
-      const Rt w1 = ok ? (F32 ? Rt(a.k1f[g]) : Rt(a.k1[g])) : Rt(0);
+      const Rt w1 = ok ? (F32 ? Rt(kern1f[g]) : Rt(kern1[g])) : Rt(0);
       u[k2] = X::make(u[k2].x * w1, u[k2].y * w1);
     }
     RDft<N2, true>::run(u);
@@ -364,15 +375,18 @@ HE_D void zconv_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T0, C* T
   }
 }
 
-template <int N, int TK, typename Rt = double>
-__global__ void __launch_bounds__(yreg_threads(N, TK)) k_zconv_reg(const YZArgs a_in,
-                                                                   const typename Cx<Rt>::T* tw2) {
+template <int N, int TK, typename Rt, bool G>
+__global__ void __launch_bounds__(yreg_threads(N, TK)) k_zconv_reg(const YZArgs a,
+                                                                   const typename Cx<Rt>::T* tw2)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
-  YZArgs a = a_in;
-  a.remap(blockIdx.z);
   using C = typename Cx<Rt>::T;
   C* T0 = smem_as<C>();
-  zconv_reg_body<N, TK>(a, tw2, T0, T0 + N * TK);
+  zconv_reg_body<N, TK, G>(a, G ? (int)blockIdx.z : 0, tw2, T0, T0 + N * TK);  // G: blockIdx.z is the member
 }
+#else
+;
+#endif
 
 }  // namespace he

@@ -129,7 +129,9 @@ struct XYArgs {
 
 // den plane -> forward x (R2C, two rows per complex line) -> forward y -> spectrum plane.
 template <int N>
-__global__ void __launch_bounds__(kXYThreads) k_xy_r2c(const XYArgs a) {
+__global__ void __launch_bounds__(kXYThreads) k_xy_r2c(const XYArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
   constexpr int NH = N / 2 + 1, P = 2 * NH, NP = N / 2;
   float2* W = smem_as<float2>();  // NP packed lines of pitch P = rows of pitch NH
@@ -169,10 +171,15 @@ __global__ void __launch_bounds__(kXYThreads) k_xy_r2c(const XYArgs a) {
   float2* o = a.specA + z * (long)NH * N;
   for (int e = tid; e < NH * N; e += nthr) o[e] = W[e];
 }
+#else
+;
+#endif
 
 // spectrum plane -> inverse y -> C2R along x (rows 2p, 2p+1 in one line) -> pot4 assembly.
 template <int N>
-__global__ void __launch_bounds__(kXYThreads) k_xy_c2r_pot(const XYArgs a) {
+__global__ void __launch_bounds__(kXYThreads) k_xy_c2r_pot(const XYArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
   constexpr int NH = N / 2 + 1, P = 2 * NH, NP = N / 2;
   float2* W = smem_as<float2>();
@@ -223,13 +230,18 @@ __global__ void __launch_bounds__(kXYThreads) k_xy_c2r_pot(const XYArgs a) {
     a.out1[g] = float(pot);
   }
 }
+#else
+;
+#endif
 
 // spectra A, B -> inverse y -> C2R along x (A + iB per row) -> dencg, delj4; correlation source
 // -> R2C along x (two rows per line) -> forward y -> spectrum plane (into specA).  The x work is
 // done kXYChunk rows at a time in a work area; each chunk's correlation spectrum rows go over the
 // A rows that chunk has consumed.
 template <int N>
-__global__ void __launch_bounds__(kXYThreads) k_xy_c2r2_corr(const XYArgs a) {
+__global__ void __launch_bounds__(kXYThreads) k_xy_c2r2_corr(const XYArgs a)
+#ifdef HE_KERNEL_TU
+{
   pdl_wait_and_trigger();
   constexpr int NH = N / 2 + 1, CH = kXYChunk < N ? kXYChunk : N;
   float2* WA = smem_as<float2>();
@@ -292,6 +304,9 @@ __global__ void __launch_bounds__(kXYThreads) k_xy_c2r2_corr(const XYArgs a) {
   float2* o = a.specA + z * (long)NH * N;
   for (int e = tid; e < NH * N; e += nthr) o[e] = WA[e];
 }
+#else
+;
+#endif
 
 // Dynamic shared memory of the three kernels.
 template <int N>

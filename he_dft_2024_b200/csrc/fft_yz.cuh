@@ -115,16 +115,13 @@ struct YZConvArgs {
   const double2* tw2;      // register-DFT twiddles of the line length
   const float2* tw2f;
   MemberMap mm;            // group members (blockIdx.y is the member)
-  HE_D void remap(int m) {
-    io = mm(io, m); out2 = mm(out2, m); fden_out = mm(fden_out, m);
-    k1 = mm(k1, m); k2 = mm(k2, m); k1f = mm(k1f, m); k2f = mm(k2f, m);
-  }
 };
 
-template <int N, int CS, bool TWO, typename Rt>
-__global__ void __launch_bounds__(kYZThreads, 1) k_yzconv(const YZConvArgs a_in) {
-  YZConvArgs a = a_in;
-  a.remap(blockIdx.y);
+template <int N, int CS, bool TWO, typename Rt, bool G>
+__global__ void __launch_bounds__(kYZThreads, 1) k_yzconv(const YZConvArgs a)
+#ifdef HE_KERNEL_TU
+{
+  const int mem = G ? (int)blockIdx.y : 0;  // G: blockIdx.y is the group member
   using C = typename Cx<Rt>::T;
   using X = Cx<Rt>;
   constexpr bool F32 = sizeof(Rt) == 4;
@@ -143,9 +140,13 @@ __global__ void __launch_bounds__(kYZThreads, 1) k_yzconv(const YZConvArgs a_in)
   if constexpr (F32) tw2 = reinterpret_cast<const C*>(a.tw2f);
   else tw2 = reinterpret_cast<const C*>(a.tw2);
   const int tid = threadIdx.x;
-  C* io = reinterpret_cast<C*>(a.io);
-  C* out2 = reinterpret_cast<C*>(a.out2);
-  C* fden = reinterpret_cast<C*>(a.fden_out);
+  C* io = reinterpret_cast<C*>(on_member<G>(a.mm, a.io, mem));
+  C* out2 = reinterpret_cast<C*>(on_member<G>(a.mm, a.out2, mem));
+  C* fden = reinterpret_cast<C*>(on_member<G>(a.mm, a.fden_out, mem));
+  const double* kern1 = on_member<G>(a.mm, a.k1, mem);
+  const double* kern2 = on_member<G>(a.mm, a.k2, mem);
+  const float* kern1f = on_member<G>(a.mm, a.k1f, mem);
+  const float* kern2f = on_member<G>(a.mm, a.k2f, mem);
   // Every data movement below is a loop of EPT elements per thread whose loads are all issued
   // before the first store (register batches of EB), so a thread has many loads in flight.
   constexpr int EPT = NS * N / kYZThreads;
@@ -223,8 +224,8 @@ __global__ void __launch_bounds__(kYZThreads, 1) k_yzconv(const YZConvArgs a_in)
       for (int j = 0; j < EB; ++j) {
         const int e = tid + kYZThreads * (j0 + j);
         const long g = kx + (long)nxh * (r * NS + e % NS) + plane * (e / NS);
-        if constexpr (F32) w[j] = second ? a.k2f[g] : a.k1f[g];
-        else w[j] = second ? a.k2[g] : a.k1[g];
+        if constexpr (F32) w[j] = second ? kern2f[g] : kern1f[g];
+        else w[j] = second ? kern2[g] : kern1[g];
       }
 #pragma unroll
       for (int j = 0; j < EB; ++j) {
@@ -277,5 +278,8 @@ __global__ void __launch_bounds__(kYZThreads, 1) k_yzconv(const YZConvArgs a_in)
     y_out(out2);
   }
 }
+#else
+;
+#endif
 
 }  // namespace he

@@ -16,16 +16,7 @@
 #include <tuple>
 
 #include "../../include/he_dft.h"
-#include "common.cuh"
-#include "fft.cuh"
-#include "fft_kernels.cuh"
-#include "fft_reg.cuh"
-#include "fft_xy.cuh"
-#include "fft_yz.cuh"
-#include "ops.cuh"
-#include "setup.cuh"
-#include "quantum.cuh"
-#include "alphas.cuh"
+#include "kernels.cuh"
 
 using namespace he;
 
@@ -500,14 +491,19 @@ template <class Op>
 static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::T* f, const Op& op,
                        int slot = -1) {
   constexpr size_t smem = stencil_smem<Op, kTX, kTY>();
-  static int occ = -1;  // resident CTAs per SM of this instantiation
+  static int occ = -1;  // resident CTAs per SM of this instantiation (one context)
   if (occ < 0) {
-    CK(set_smem_attr((const void*)k_stencil<Op, kTX, kTY>, smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<Op, kTX, kTY>, kTX * kTY, smem));
+    CK(set_smem_attr((const void*)k_stencil<Op, kTX, kTY, false>, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<Op, kTX, kTY, false>, kTX * kTY, smem));
   }
   TRY(join_aux(ctx));  // stencils read uimp / write den / reduce through the shared partials
-  if (ctx->nmem > 1 && !HasRemap<Op>::value)
-    return fail(ctx, HE_ERR_STATE, "%s does not run over the members of a group", Op::kname());
+  // a group runs the instantiation that maps the op's pointers to each member's buffers; the z
+  // chunking (and so every reduction's order) stays that of one context
+  void (*k)(const typename Op::T*, StencilGeom, Op, ReduceTail) = k_stencil<Op, kTX, kTY, false>;
+  if (ctx->nmem > 1) {
+    if constexpr (HasRemap<Op>::value) k = k_stencil<Op, kTX, kTY, true>;
+    else return fail(ctx, HE_ERR_STATE, "%s does not run over the members of a group", Op::kname());
+  }
   StencilGeom g = g0;
   g.zc = choose_zc(ctx, occ);
   dim3 grid = stencil_grid(ctx, g), block(kTX, kTY);
@@ -519,9 +515,9 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
   g.nzc = (int)grid.z;  // blockIdx.z = member x nzc + chunk
   g.mm = ctx->mm;
   grid.z *= ctx->nmem;
-  CK(set_smem_attr((const void*)k_stencil<Op, kTX, kTY>, smem));
+  CK(set_smem_attr((const void*)k, smem));
   tname(ctx, Op::kname());
-  k_stencil<Op, kTX, kTY><<<grid, block, smem, ctx->stream>>>(f, g, op, rt);
+  k<<<grid, block, smem, ctx->stream>>>(f, g, op, rt);
   LAUNCHED();
   return HE_OK;
 }
@@ -596,9 +592,10 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
                                  "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4", "fft_x_c2r"};
   if (!ctx->xpipe[MODE] || N == 0) {
     const size_t csmem = fft_smem(ctx->plx, rb, 2, sizeof(typename Cx<Rt>::T));
-    CK(set_smem_attr((const void*)k_xpass_c<MODE, N, TILE, Rt>, csmem));
+    void (*kc)(XArgs) = ctx->nmem > 1 ? k_xpass_c<MODE, N, TILE, Rt, true> : k_xpass_c<MODE, N, TILE, Rt, false>;
+    CK(set_smem_attr((const void*)kc, csmem));
     tname(ctx, names[MODE]);
-    CK(launch_chain(ctx, k_xpass_c<MODE, N, TILE, Rt>, dim3((unsigned)ntiles, ctx->nmem), dim3(nthr), csmem, a));
+    CK(launch_chain(ctx, kc, dim3((unsigned)ntiles, ctx->nmem), dim3(nthr), csmem, a));
     LAUNCHED();
     return HE_OK;
   }
@@ -606,18 +603,20 @@ static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   const size_t smem = xpass_smem<MODE, Rt>(ctx->plx.stw_len, rb, ctx->nx);
   // persistent grid: as many CTAs as fit on the device at once (the smem of the run-time-length
   // kernel depends on the grid, so its occupancy is queried per launch size)
+  // (the tiles of a CTA, and so the grid, are those of one context in a group too)
   static size_t occ_smem = 0;
   static int occ = 0;
   if (occ_smem != smem) {
-    CK(set_smem_attr((const void*)k_xpass<MODE, N, TILE, Rt>, smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xpass<MODE, N, TILE, Rt>, pthr, smem));
+    CK(set_smem_attr((const void*)k_xpass<MODE, N, TILE, Rt, false>, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xpass<MODE, N, TILE, Rt, false>, pthr, smem));
     occ_smem = smem;
   }
   if (occ < 1) return fail(ctx, HE_ERR_STATE, "x pass: %zu bytes of shared memory do not fit an SM", smem);
   const unsigned nb = (unsigned)std::min<long>(ntiles, (long)occ * ctx->num_sms);
-  CK(set_smem_attr((const void*)k_xpass<MODE, N, TILE, Rt>, smem));
+  void (*kp)(XArgs) = ctx->nmem > 1 ? k_xpass<MODE, N, TILE, Rt, true> : k_xpass<MODE, N, TILE, Rt, false>;
+  CK(set_smem_attr((const void*)kp, smem));
   tname(ctx, names[MODE]);
-  CK(launch_chain(ctx, k_xpass<MODE, N, TILE, Rt>, dim3(nb, ctx->nmem), dim3(pthr), smem, a));
+  CK(launch_chain(ctx, kp, dim3(nb, ctx->nmem), dim3(pthr), smem, a));
   LAUNCHED();
   return HE_OK;
 }
@@ -653,11 +652,13 @@ static int ypass_n(he_ctx_t* ctx, const YZArgs& a, int narr) {
     const C* tw2;
     if constexpr (sizeof(Rt) == 4) tw2 = ctx->ply.tw2f;
     else tw2 = ctx->ply.tw2;
-    CK(set_smem_attr((const void*)k_ypass_reg<N, TILE, Rt>, rsmem));
-    CK(launch_chain(ctx, k_ypass_reg<N, TILE, Rt>, grid, dim3(yreg_threads(N, TILE)), rsmem, a, tw2));
+    void (*k)(YZArgs, const C*) = ctx->nmem > 1 ? k_ypass_reg<N, TILE, Rt, true> : k_ypass_reg<N, TILE, Rt, false>;
+    CK(set_smem_attr((const void*)k, rsmem));
+    CK(launch_chain(ctx, k, grid, dim3(yreg_threads(N, TILE)), rsmem, a, tw2));
   } else {
-    CK(set_smem_attr((const void*)k_ypass<N, TILE, Rt>, smem));
-    CK(launch_chain(ctx, k_ypass<N, TILE, Rt>, grid, dim3(nthr), smem, a));
+    void (*k)(YZArgs) = ctx->nmem > 1 ? k_ypass<N, TILE, Rt, true> : k_ypass<N, TILE, Rt, false>;
+    CK(set_smem_attr((const void*)k, smem));
+    CK(launch_chain(ctx, k, grid, dim3(nthr), smem, a));
   }
   LAUNCHED();
   return HE_OK;
@@ -690,15 +691,19 @@ static int ypass(he_ctx_t* ctx, double2* a0, double2* a1, bool inv) {
 template <int N, int TILE, typename Rt>
 static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
   const int tk = (N > 0) ? TILE : ctx->tkx;
-  if constexpr (N > 0 && sizeof(Rt) == 4) {
-    if (ctx->zreg) {  // register line transforms (fft_reg.cuh), binary32 chain
+  if constexpr (N > 0) {
+    if (ctx->zreg) {  // register line transforms (fft_reg.cuh)
       using C = typename Cx<Rt>::T;
-      const size_t rsmem = sizeof(C) * (size_t)N * TILE * (a.k2f ? 2 : 1);
-      CK(set_smem_attr((const void*)k_zconv_reg<N, TILE, Rt>, rsmem));
+      const bool two = (sizeof(Rt) == 4) ? a.k2f != nullptr : a.k2 != nullptr;
+      const size_t rsmem = sizeof(C) * (size_t)N * TILE * (two ? 2 : 1);
+      const C* tw2;
+      if constexpr (sizeof(Rt) == 4) tw2 = ctx->plz.tw2f;
+      else tw2 = ctx->plz.tw2;
+      void (*k)(YZArgs, const C*) = ctx->nmem > 1 ? k_zconv_reg<N, TILE, Rt, true> : k_zconv_reg<N, TILE, Rt, false>;
+      CK(set_smem_attr((const void*)k, rsmem));
       dim3 grid((ctx->nxh + TILE - 1) / TILE, ctx->ny, ctx->nmem);
       tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
-      CK(launch_chain(ctx, k_zconv_reg<N, TILE, Rt>, grid, dim3(yreg_threads(N, TILE)), rsmem, a,
-                      (const C*)ctx->plz.tw2f));
+      CK(launch_chain(ctx, k, grid, dim3(yreg_threads(N, TILE)), rsmem, a, tw2));
       LAUNCHED();
       return HE_OK;
     }
@@ -706,9 +711,10 @@ static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, ctx->nmem);
-  CK(set_smem_attr((const void*)k_zconv<N, TILE, Rt>, smem));
+  void (*k)(YZArgs) = ctx->nmem > 1 ? k_zconv<N, TILE, Rt, true> : k_zconv<N, TILE, Rt, false>;
+  CK(set_smem_attr((const void*)k, smem));
   tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
-  CK(launch_chain(ctx, k_zconv<N, TILE, Rt>, grid, dim3(nthr), smem, a));
+  CK(launch_chain(ctx, k, grid, dim3(nthr), smem, a));
   LAUNCHED();
   return HE_OK;
 }
@@ -755,7 +761,7 @@ static bool yz_fusable(const he_ctx_t* ctx) { return ctx->ny == 64 && ctx->nz ==
 template <int N, int CS, bool TWO, typename Rt>
 static int yzconv_n(he_ctx_t* ctx, const YZConvArgs& a) {
   constexpr size_t smem = yz_smem<N, CS, Rt>();
-  void (*k)(YZConvArgs) = k_yzconv<N, CS, TWO, Rt>;
+  void (*k)(YZConvArgs) = ctx->nmem > 1 ? k_yzconv<N, CS, TWO, Rt, true> : k_yzconv<N, CS, TWO, Rt, false>;
   CK(set_smem_attr((const void*)k, smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(((ctx->nxh + 1) / 2) * CS), ctx->nmem);
@@ -862,6 +868,7 @@ static int xy_pass(he_ctx_t* ctx, int kind, const XYArgs& a) {
 }
 // Dynamics_TDDFT/poten.f90:131-218 with fused plane passes: 5 launches instead of 9.
 static int poten_fused(he_ctx_t* ctx, const double* extra, const double* extra2) {
+  if (ctx->nmem > 1) return fail(ctx, HE_ERR_STATE, "the fused x-y field evaluation runs no groups");
   XYArgs a = xyargs(ctx);
   a.den = (const float*)ctx->den;
   a.specA = (float2*)ctx->wA;
@@ -1500,8 +1507,8 @@ static int autotune_tiles(he_ctx_t* ctx) {
   if (st == HE_OK && yz_fast(ctx->nz)) {
     auto zfn = [](he_ctx_t* c) -> int { return zconv(c, c->wA, c->wcgk, c->wB, c->fvlj4, nullptr); };
     st = pick(&ctx->tile_z, zfn, "z");
-    if (st == HE_OK && ctx->mixed) {
-      // the binary32 chain also has the register variant: keep it if it beats the best so far
+    if (st == HE_OK) {
+      // the register variant against the best shared-memory pass so far
       const int tile0 = ctx->tile_z;
       float t0 = 0.0f;
       st = timed(zfn, &t0);
@@ -1695,9 +1702,10 @@ static int zmix_n(he_ctx_t* ctx, const ZMixArgs& a) {
   const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, ctx->nmem);
-  CK(set_smem_attr((const void*)k_zmix<N, TILE, Rt>, smem));
+  void (*k)(ZMixArgs) = ctx->nmem > 1 ? k_zmix<N, TILE, Rt, true> : k_zmix<N, TILE, Rt, false>;
+  CK(set_smem_attr((const void*)k, smem));
   tname(ctx, a.nout == 0 ? "fft_z_fwd" : a.fwd_in ? "fft_z_mix_fwd" : "fft_z_mix");
-  k_zmix<N, TILE, Rt><<<grid, nthr, smem, ctx->stream>>>(a);
+  k<<<grid, nthr, smem, ctx->stream>>>(a);
   LAUNCHED();
   return HE_OK;
 }
@@ -2815,6 +2823,7 @@ int he_ctx_group(he_ctx_t* const* ctxs, int n) {
         c->cglj_pending != L->cglj_pending)
       return fail(L, HE_ERR_ARG, "member %d differs from the leader (mode, precision, grid or core)", m);
     if (!c->kernels_ok) return fail(L, HE_ERR_STATE, "member %d has no k-space kernels", m);
+    if (c->xyfuse) return fail(L, HE_ERR_STATE, "member %d evaluates its field with the fused x-y passes, which run no groups", m);
     for (int i = 0; i < L->nq; ++i)
       if (c->h2o2mx[i] != L->h2o2mx[i]) return fail(L, HE_ERR_ARG, "member %d's impurity masses differ", m);
     // derden's gradients are allocated on first use; every member holds them before pairing
@@ -3788,7 +3797,6 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile) {
       ctx->tile_y = tile;
       return HE_OK;
     case 2:
-      if (variant && !ctx->mixed) return fail(ctx, HE_ERR_ARG, "the register z pass is built for HE_PREC_MIXED");
       ctx->zreg = variant != 0;
       ctx->tile_z = tile;
       return HE_OK;

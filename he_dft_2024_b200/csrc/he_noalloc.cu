@@ -80,10 +80,10 @@ template <typename T>
 int launch_energy(const StencilGeom& g, dim3 grid, const OpEnergy<T>& op, const T* psi,
                   const ReduceTail& rt, cudaStream_t st, char* err, size_t errlen) {
   constexpr size_t smem = stencil_smem<OpEnergy<T>, 32, 8>();
-  cudaError_t e = cudaFuncSetAttribute(k_stencil<OpEnergy<T>, 32, 8>,
+  cudaError_t e = cudaFuncSetAttribute(k_stencil<OpEnergy<T>, 32, 8, false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
-    k_stencil<OpEnergy<T>, 32, 8><<<grid, dim3(32, 8), smem, st>>>(psi, g, op, rt);
+    k_stencil<OpEnergy<T>, 32, 8, false><<<grid, dim3(32, 8), smem, st>>>(psi, g, op, rt);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {

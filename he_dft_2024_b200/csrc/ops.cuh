@@ -567,12 +567,14 @@ HE_D void imp_force_body(ImpDev* s, const double* sums, double dxyz) {
       for (int c = 0; c < 3; ++c) s->F[k + n * c] = s->F[k + n * c] + (-dv * d[c] / a1);
     }
 }
+#ifndef HE_KERNEL_TU
 static __global__ void k_imp_force(ImpDev* g, const double* sums, double dxyz) {
   __shared__ ImpDev st;
   imp_stage_in(&st, g);
   if (threadIdx.x == 0) imp_force_body(&st, sums, dxyz);
   imp_stage_out(g, &st);
 }
+#endif
 
 // aimp = F / m_imp (DFT4He3d.f90:571-573).
 HE_D void imp_accel_body(ImpDev* s) {
@@ -580,12 +582,14 @@ HE_D void imp_accel_body(ImpDev* s) {
   for (int k = 0; k < n; ++k)
     for (int c = 0; c < 3; ++c) s->aimp[k + n * c] = s->F[k + n * c] / s->m[k];
 }
+#ifndef HE_KERNEL_TU
 static __global__ void k_imp_accel(ImpDev* g) {
   __shared__ ImpDev st;
   imp_stage_in(&st, g);
   if (threadIdx.x == 0) imp_accel_body(&st);
   imp_stage_out(g, &st);
 }
+#endif
 
 // Impurity part of one RK-Gill stage (steprk.f90:92-125).
 HE_D void imp_rk_body(ImpDev* s, int jr, double a, double b, double cc, double dt) {
@@ -620,12 +624,14 @@ HE_D void imp_rk_body(ImpDev* s, int jr, double a, double b, double cc, double d
     for (int i = 0; i < 2; ++i) s->iolda[i] = i + 1;
   }
 }
+#ifndef HE_KERNEL_TU
 static __global__ void k_imp_rk(ImpDev* g, int jr, double a, double b, double cc, double dt) {
   __shared__ ImpDev st;
   imp_stage_in(&st, g);
   if (threadIdx.x == 0) imp_rk_body(&st, jr, a, b, cc, dt);
   imp_stage_out(g, &st);
 }
+#endif
 
 // Impurity predictor + modifier (steppc.f90:80-99).  The velocity prediction is stored in
 // vimpold(:,:,ioldv(3)) and vimp keeps v_n, as in the reference.
@@ -655,12 +661,14 @@ HE_D void imp_predict_body(ImpDev* s, double dt) {
   s->iolda[1] = s->iolda[0];
   s->iolda[0] = t;
 }
+#ifndef HE_KERNEL_TU
 static __global__ void k_imp_predict(ImpDev* g, double dt) {
   __shared__ ImpDev st;
   imp_stage_in(&st, g);
   if (threadIdx.x == 0) imp_predict_body(&st, dt);
   imp_stage_out(g, &st);
 }
+#endif
 
 // Impurity corrector (steppc.f90:149-174).  aimp is the value set by the driver before the step
 // (the forceimp inside steppc refreshes F but not aimp), as in the reference.
@@ -700,12 +708,14 @@ HE_D void imp_correct_body(ImpDev* s, double dt) {
   s->ioldv[1] = s->ioldv[0];
   s->ioldv[0] = t;
 }
+#ifndef HE_KERNEL_TU
 static __global__ void k_imp_correct(ImpDev* g, double dt) {
   __shared__ ImpDev st;
   imp_stage_in(&st, g);
   if (threadIdx.x == 0) imp_correct_body(&st, dt);
   imp_stage_out(g, &st);
 }
+#endif
 
 // ---- statics (real psi) ------------------------------------------------------------------------
 // hpsi = -(d2x+d2y+d2z)*h2o2m4 + pot4*psi; acc = sum psi*hpsi  (steppcr.f90:40-42).

@@ -70,10 +70,8 @@ struct ZMixArgs {
 };
 
 // Rt = float: the mixed path (binary32 spectra, kernels given as their binary32 copies).
-template <int N, int TILE, typename Rt = double>
-__global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a_in) {
-  ZMixArgs a = a_in;
-  a.remap(blockIdx.z);
+template <int N, int TILE, typename Rt>
+HE_D void zmix_body(const ZMixArgs& a) {
   using C = typename Cx<Rt>::T;
   C* smem = smem_as<C>();
   const C* fwd_in = reinterpret_cast<const C*>(a.fwd_in);
@@ -151,7 +149,26 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a_in
   }
 }
 
+// G: blockIdx.z is the group member, and the arguments are copied with their pointers mapped to
+// the member's buffers; otherwise they are read as passed.
+template <int N, int TILE, typename Rt, bool G>
+__global__ void __launch_bounds__(tile_threads(TILE)) k_zmix(const ZMixArgs a)
+#ifdef HE_KERNEL_TU
+{
+  if constexpr (G) {
+    ZMixArgs b = a;
+    b.remap(blockIdx.z);
+    zmix_body<N, TILE, Rt>(b);
+  } else {
+    zmix_body<N, TILE, Rt>(a);
+  }
+}
+#else
+;
+#endif
+
 // ---- pointwise passes (grid-stride, deterministic two-level reductions) -----------------------
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_cnorm2(const double2* __restrict__ f, double* __restrict__ out,
                                                 long N, const MemberMap mm) {
   f = mm(f, blockIdx.y);
@@ -159,7 +176,9 @@ __global__ void __launch_bounds__(256) k_cnorm2(const double2* __restrict__ f, d
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
     out[i] = cnorm2(f[i]);
 }
+#endif
 
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const double* __restrict__ b,
                                              long N, const ReduceTail rt_in, const MemberMap mm) {
   a = mm(a, blockIdx.y);
@@ -171,8 +190,10 @@ __global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a, const
   block_reduce_store<1>(acc, rt.partials + blockIdx.x);
   reduce_tail<1>(rt, gridDim.x);
 }
+#endif
 
 // The mixed path: |psix|^2 of the compensated pair (hi and lo planes), rounded once to binary32.
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_cnorm2_pair(const float2* __restrict__ hi,
                                                      const float2* __restrict__ lo,
                                                      float* __restrict__ out, long N,
@@ -185,8 +206,10 @@ __global__ void __launch_bounds__(256) k_cnorm2_pair(const float2* __restrict__ 
     out[i] = (float)(re * re + im * im);
   }
 }
+#endif
 
 // sum a*b of binary32 fields, summed in binary64 (the mixed path's energy sums).
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_dot_f32(const float* __restrict__ a, const float* __restrict__ b,
                                                  long N, const ReduceTail rt_in, const MemberMap mm) {
   a = mm(a, blockIdx.y);
@@ -198,9 +221,11 @@ __global__ void __launch_bounds__(256) k_dot_f32(const float* __restrict__ a, co
   block_reduce_store<1>(acc, rt.partials + blockIdx.x);
   reduce_tail<1>(rt, gridDim.x);
 }
+#endif
 
 // {sum |f|^2, sum |f|^2 x, sum |f|^2 y, sum |f|^2 z} (DFT4He3d.f90:682-700 of the quantum driver).
 // (C = float2: the hi plane of the mixed path's pair, summed in binary64.)
+#ifndef HE_KERNEL_TU
 template <typename C>
 __global__ void __launch_bounds__(256) k_moments(const C* __restrict__ f, int nx, int ny, long N,
                                                  double x0, double y0, double z0, double hx,
@@ -222,6 +247,7 @@ __global__ void __launch_bounds__(256) k_moments(const C* __restrict__ f, int nx
   block_reduce_store<4>(acc, rt.partials + blockIdx.x * 4);
   reduce_tail<4>(rt, gridDim.x);
 }
+#endif
 
 // ---- FT_V_spline --------------------------------------------------------------------------------
 struct FtvArgs {
@@ -237,6 +263,7 @@ struct FtvArgs {
 // Vpp(p) = [core + sum_j closed-form integral of r sin(qr) p_j(r) over [r_j, r_j+1]] * 4 pi / q,
 // q = 2 pi p (FT_V_spline.f90:151-225); p = 0 takes the moments r^2 p_j(r) (:164-188).  The
 // nodes' sin(q r_j), cos(q r_j) are computed once per node through shared memory.
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_ftv(const FtvArgs A) {
   __shared__ double s_s[257], s_c[257];
   const int tid = threadIdx.x;
@@ -295,6 +322,7 @@ __global__ void __launch_bounds__(256) k_ftv(const FtvArgs A) {
     A.vpp[blockIdx.x] = (Vp + tot[0]) * c1oq * Qpi;
   }
 }
+#endif
 
 struct UimpkArgs {
   const double *P, *a, *b, *c, *d;  // momentum table (np) and its spline
@@ -306,6 +334,7 @@ struct UimpkArgs {
 
 // uimp_k(ix,iy,iz) = FT_V_spline(pmod) (potenimpini.f90:136-144): findi's bisection
 // (mates.f:4-33) for the piece, then its cubic in p.
+#ifndef HE_KERNEL_TU
 __global__ void __launch_bounds__(256) k_uimpk(const UimpkArgs A) {
   const long nk = (long)A.nxh * A.ny * A.nz;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nk; i += (long)gridDim.x * blockDim.x) {
@@ -330,5 +359,6 @@ __global__ void __launch_bounds__(256) k_uimpk(const UimpkArgs A) {
     A.out[i] = A.a[k] + p * (A.b[k] + p * (A.c[k] + p * A.d[k]));
   }
 }
+#endif
 
 }  // namespace he

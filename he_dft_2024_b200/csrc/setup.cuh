@@ -111,6 +111,7 @@ struct KernArgs {
   double* kalfs;
 };
 
+#ifndef HE_KERNEL_TU
 __global__ void k_kernels(const KernArgs a) {
   const long nk = (long)a.nxh * a.ny * a.nz;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nk;
@@ -154,5 +155,6 @@ __global__ void k_kernels(const KernArgs a) {
     }
   }
 }
+#endif
 
 }  // namespace he

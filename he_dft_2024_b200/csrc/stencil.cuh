@@ -97,17 +97,13 @@ HE_D ReduceTail remap(const ReduceTail& r, const MemberMap& mm, int m) {
   return ReduceTail{mm(r.partials, m), mm(r.counter, m), mm(r.out, m)};
 }
 
-// Ops (and other argument structs) of kernels that run over the members of a group carry
-// remap(mm, m), which maps their device pointers to member m's buffers.
+// Stencil ops that run over the members of a group carry remap(mm, m), which maps their device
+// pointers to member m's buffers.
 template <class O, class = void>
 struct HasRemap : std::false_type {};
 template <class O>
 struct HasRemap<O, std::void_t<decltype(std::declval<O&>().remap(std::declval<const MemberMap&>(), 0))>>
     : std::true_type {};
-template <class O>
-HE_D void remap_op(O& o, const MemberMap& mm, int m) {
-  if constexpr (HasRemap<O>::value) o.remap(mm, m);
-}
 
 template <int NV>
 __device__ void reduce_tail(const ReduceTail& rt, long nb) {
@@ -173,19 +169,11 @@ HE_HD constexpr size_t stencil_smem() {
          2 * (size_t)Op::N8 * TX * TY * sizeof(typename RT::R);
 }
 
+// The stencil pass of one member; bz is the CTA's z-chunk within the member's grid of nzc.
 template <class Op, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
-    k_stencil(const typename Op::T* __restrict__ f_in, const StencilGeom g, const Op op_in,
-              const ReduceTail rt_in) {
+HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g, const Op& op,
+                      const ReduceTail& rt, int bz, int nzc) {
   using T = typename Op::T;
-  // member of a group (blockIdx.z = member x nzc + chunk) and its buffers
-  const int nzc = g.nzc > 0 ? g.nzc : (int)gridDim.z;
-  const int mem = (int)blockIdx.z / nzc;
-  const int bz = (int)blockIdx.z - mem * nzc;
-  const T* __restrict__ f = g.mm(f_in, mem);
-  Op op = op_in;
-  remap_op(op, g.mm, mem);
-  const ReduceTail rt = remap(rt_in, g.mm, mem);
   using R = typename RealOf<T>::R;
   using Z = typename RealOf<T>::Z;
   constexpr int NT = TX * TY;
@@ -380,5 +368,29 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
     reduce_tail<NV>(rt, nb);
   }
 }
+
+// G = false: one context, blockIdx.z the z chunk, the arguments used as passed.  G = true: a
+// group, blockIdx.z = member x nzc + chunk; the op (copied), the field and the reduction tail
+// are mapped to the member's buffers.  Separate instantiations, so that a context outside a group
+// runs no mapping code at all.
+template <class Op, int TX, int TY, bool G>
+__global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
+    k_stencil(const typename Op::T* __restrict__ f, const StencilGeom g, const Op op,
+              const ReduceTail rt)
+#ifdef HE_KERNEL_TU
+{
+  if constexpr (G) {
+    const int nzc = g.nzc;
+    const int mem = (int)blockIdx.z / nzc;
+    Op o = op;
+    o.remap(g.mm, mem);
+    stencil_run<Op, TX, TY>(g.mm(f, mem), g, o, remap(rt, g.mm, mem), (int)blockIdx.z - mem * nzc, nzc);
+  } else {
+    stencil_run<Op, TX, TY>(f, g, op, rt, (int)blockIdx.z, (int)gridDim.z);
+  }
+}
+#else
+;
+#endif
 
 }  // namespace he

@@ -311,7 +311,7 @@ int he_tuned_tiles(const he_ctx_t* ctx, int* x, int* y, int* z);
 int he_autotune_report(const he_ctx_t* ctx, char* buf, size_t len);
 /* Overrides the autotuner's choice for one pass family (reproducible runs, tests): pass 0 = x
  * (variant 0 one-shot, 1 persistent pipelined; every mode), 1 = y (variant 1, the register
- * transform), 2 = z (variant 0 shared-memory Stockham, 1 register transform, HE_PREC_MIXED only),
+ * transform), 2 = z (variant 0 shared-memory Stockham, 1 register transform),
  * 3 + m = the x pass of one mode m only (0 R2C of den, 1 R2C of the statics correlation source,
  * 2 C2R of two spectra, 3 the same plus the correlation R2C, 4 C2R + pot4, 5 C2R of one
  * spectrum), 9 = the classical field evaluation with fused x-y plane passes (variant 1) or

@@ -78,3 +78,23 @@ def test_fused_yz_runs_match_oracle(mode):
             assert abs(eg - eo) <= 1e-10 * abs(eo), it
             lo, lg = np.linalg.norm(o.get("den")), np.linalg.norm(ctx.download("den"))
             assert abs(lg - lo) <= 1e-10 * lo, it
+
+
+@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("tile", [8, 16])
+def test_register_z_pass_matches_shared_memory_pass_f64(n, tile):
+    """The binary64 convolution with the z lines transformed in registers (k_zconv_reg) against
+    the shared-memory Stockham z pass (k_zconv), separate y / z passes both times."""
+    w = C.replace(C.tddft_1000(n=n), n_imp=0, m_imp_u=(), rimp0=(), vimp0_aps=(), noise=0.05)
+    den = C.woods_saxon(w)
+    out = {}
+    for zreg in (0, 1):
+        with Context(w) as ctx:
+            if n == 64:
+                ctx.set_fft_variant("yz", 0, 8)
+            ctx.set_fft_variant("z", zreg, tile)
+            ctx.upload("den", den)
+            ctx.poten()
+            out[zreg] = {k: ctx.download(k) for k in FIELDS}
+    for k in FIELDS:
+        assert rel(out[1][k], out[0][k]) < 1e-12, (k, rel(out[1][k], out[0][k]))
