@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kXPipeThreads) k_xpass(const XArgs a)
   const int nxh = n / 2 + 1;
   const int ls = line_stride(n);
   const int RB = (N > 0) ? TILE : a.rb;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = threadIdx.x, nthr = kXPipeThreads;
   const long ntiles = a.rows / RB;
   C* tw = smem;
   C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
@@ -299,7 +299,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
   const int nxh = n / 2 + 1;
   const int ls = line_stride(n);
   const int RB = (N > 0) ? TILE : a.rb;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = threadIdx.x;
+  // compile-time thread count for the compile-time lengths: the element loops below unroll and
+  // issue their global loads together
+  const int nthr = (N > 0) ? tile_threads(TILE) : (int)blockDim.x;
   const long r0 = (long)blockIdx.x * RB;
   C* tw = smem;
   C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
@@ -423,7 +426,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a)
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
   const int nxh = a.nxh;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = threadIdx.x;
+  // compile-time thread count for the compile-time lengths: the element loops below unroll and
+  // issue their global loads together
+  const int nthr = (N > 0) ? tile_threads(TILE) : (int)blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int z = blockIdx.y;
   C* arr = reinterpret_cast<C*>(on_member<G>(a.mm, a.arr[ai], mem));
@@ -471,7 +477,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
   const int nxh = a.nxh;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = threadIdx.x;
+  // compile-time thread count for the compile-time lengths: the element loops below unroll and
+  // issue their global loads together
+  const int nthr = (N > 0) ? tile_threads(TILE) : (int)blockDim.x;
   const int kx0 = blockIdx.x * TK;
   const int ky = blockIdx.y;
   C* tw = smem;
@@ -481,6 +490,22 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
   load_twiddles(tw, a.pl);
   const long plane = (long)nxh * a.ny;
   const long base = (long)nxh * ky;
+  // compile-time lengths: element e = tid + j nthr, j < EPT, and the kernel values of the
+  // multiply are loaded before the forward transform, so their latency hides behind it
+  constexpr int EPT = (N > 0) ? N / 16 : 1;  // TK n / nthr with nthr = 16 TK
+  Rt w1p[EPT], w2p[EPT];
+  if constexpr (N > 0) {
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) {
+      const int e = tid + j * nthr;
+      const int jj = e / TK, c = e - jj * TK;
+      const bool ok = kx0 + c < nxh;
+      const long g = base + (ok ? kx0 + c : 0) + plane * jj;
+      w1p[j] = ok ? (F32 ? Rt(kern1f[g]) : Rt(kern1[g])) : Rt(0);
+      w2p[j] = (ok && two) ? (F32 ? Rt(kern2f[g]) : Rt(kern2[g])) : Rt(0);
+    }
+  }
+#pragma unroll
   for (int e = tid; e < TK * n; e += nthr) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
@@ -489,24 +514,32 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
   __syncthreads();
   C* F = fft_lines<N>(P0, P1, TK, ls, a.pl, tw, false);
   C* O = (F == P0) ? P1 : P0;
-  for (int e = tid; e < TK * n; e += nthr) {
+  auto multiply = [&](int e, Rt w1, Rt w2) {
     const int j = e / TK, c = e - j * TK;
     const int kx = kx0 + c;
     const int s = c * ls + sw<N>(j);
     if (kx >= nxh) {
       F[s] = X::make(0, 0);
       if (two) P2[s] = X::make(0, 0);
-      continue;
+      return;
     }
     const long g = base + kx + plane * j;
     const C f = F[s];
     if (fden_out) fden_out[g] = f;
-    if (two) {
-      const Rt w2 = F32 ? Rt(kern2f[g]) : Rt(kern2[g]);
-      P2[s] = X::make(f.x * w2, f.y * w2);
-    }
-    const Rt w1 = F32 ? Rt(kern1f[g]) : Rt(kern1[g]);
+    if (two) P2[s] = X::make(f.x * w2, f.y * w2);
     F[s] = X::make(f.x * w1, f.y * w1);
+  };
+  if constexpr (N > 0) {
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) multiply(tid + j * nthr, w1p[j], w2p[j]);
+  } else {
+    for (int e = tid; e < TK * n; e += nthr) {
+      const int j = e / TK, c = e - j * TK;
+      const long g = base + min(kx0 + c, nxh - 1) + plane * j;
+      const Rt w1 = F32 ? Rt(kern1f[g]) : Rt(kern1[g]);
+      const Rt w2 = two ? (F32 ? Rt(kern2f[g]) : Rt(kern2[g])) : Rt(0);
+      multiply(e, w1, w2);
+    }
   }
   __syncthreads();
   C* R1 = fft_lines<N>(F, O, TK, ls, a.pl, tw, true);

@@ -16,12 +16,11 @@ struct Timec {
     ay = mm(ay, m);
     az = mm(az, m);
   }
-  HE_D double re(int ix, int iy, int iz) const {
-    double s = 1.0 + ax[ix];
-    s = s + 1.0 + ay[iy];
-    s = s + 1.0 + az[iz];
-    return lambdah * s;
-  }
+  // lambdah * (((1 + ax) + 1 + ay) + 1 + az), summed left to right; the stencil pass evaluates
+  // the x-y part once per column (xy) and adds each plane's az (with_z)
+  HE_D double xy(int ix, int iy) const { return (1.0 + ax[ix]) + 1.0 + ay[iy]; }
+  HE_D double with_z(double sxy, double azv) const { return lambdah * (sxy + 1.0 + azv); }
+  HE_D double re(int ix, int iy, int iz) const { return with_z(xy(ix, iy), az[iz]); }
 };
 
 
@@ -81,9 +80,9 @@ struct OpPredictT {
     remap_all(s8, mm, m); remap_all(s16, mm, m);
     po3 = mm(po3, m); h2 = mm(h2, m); pc = mm(pc, m); den = mm(den, m); tm.remap(mm, m);
   }
-  HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               const double* v8, const double2* v16, int vs, double*) const {
-    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
+  HE_D void at_t(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
+               const double* v8, const double2* v16, int vs, double*, double tr) const {
+    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tr, h2o2m);
     const double2 p3 = v16[0], hh1 = v16[vs], hh2 = v16[2 * vs], pcv = v16[3 * vs];
     const double2 t = make_double2(2.0 * s4.x - hh1.x + 2.0 * hh2.x, 2.0 * s4.y - hh1.y + 2.0 * hh2.y);
     const double2 sto1 = make_double2(p3.x + s43 * t.x, p3.y + s43 * t.y);
@@ -113,9 +112,9 @@ struct OpCorrectT {
     remap_all(s8, mm, m); remap_all(s16, mm, m);
     pc = mm(pc, m); out = mm(out, m); den = mm(den, m); tm.remap(mm, m);
   }
-  HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               const double* v8, const double2* v16, int vs, double* acc) const {
-    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
+  HE_D void at_t(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
+               const double* v8, const double2* v16, int vs, double* acc, double tr) const {
+    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tr, h2o2m);
     const double2 a3 = v16[0], a2 = v16[vs], b1 = v16[2 * vs], b2 = v16[3 * vs], p = v16[4 * vs];
     const double2 inner = make_double2(s4.x + 2.0 * b1.x - b2.x, s4.y + 2.0 * b1.y - b2.y);
     const double2 s5 = make_double2(0.125 * (9.0 * a3.x - a2.x + s3 * inner.x),
@@ -148,9 +147,9 @@ struct OpRKT {
     remap_all(s8, mm, m); remap_all(s16, mm, m);
     q = mm(q, m); out = mm(out, m); hsave = mm(hsave, m); den = mm(den, m); tm.remap(mm, m);
   }
-  HE_D void at(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
-               const double* v8, const double2* v16, int vs, double*) const {
-    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tm.re(ix, iy, iz), h2o2m);
+  HE_D void at_t(int ix, int iy, int iz, long i, double2 dx, double2 dy, double2 dz, double2 c,
+               const double* v8, const double2* v16, int vs, double*, double tr) const {
+    const double2 s4 = hpsi_any<QU>(dx, dy, dz, c, v8, vs, mu, tr, h2o2m);
     const double2 qq = v16[0];
     const double2 s1 = make_double2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
     q[i] = make_double2(qq.x + 3.0 * s1.x - cc * s4.x, qq.y + 3.0 * s1.y - cc * s4.y);
@@ -233,9 +232,9 @@ struct OpRKMT {
     q = mm(q, m); out_hi = mm(out_hi, m); out_lo = mm(out_lo, m); hsave = mm(hsave, m);
     den = mm(den, m); tm.remap(mm, m);
   }
-  HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
-               const float* v8, const float2* v16, int vs, double*) const {
-    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
+  HE_D void at_t(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
+               const float* v8, const float2* v16, int vs, double*, double tr) const {
+    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tr, h2o2m);
     const float2 qq = v16[0];
     const float2 s1 = make_float2(a * (s4.x - b * qq.x), a * (s4.y - b * qq.y));
     q[i] = make_float2(qq.x + 3.0f * s1.x - cc * s4.x, qq.y + 3.0f * s1.y - cc * s4.y);
@@ -268,9 +267,9 @@ struct OpPredictMT {
     po3_hi = mm(po3_hi, m); po3_lo = mm(po3_lo, m); h2 = mm(h2, m); den = mm(den, m);
     tm.remap(mm, m);
   }
-  HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
-               const float* v8, const float2* v16, int vs, double*) const {
-    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
+  HE_D void at_t(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
+               const float* v8, const float2* v16, int vs, double*, double tr) const {
+    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tr, h2o2m);
     const float2 hh1 = v16[2 * vs], hh2 = v16[3 * vs], pcv = v16[4 * vs];
     const float2 t = make_float2(2.0f * s4.x - hh1.x + 2.0f * hh2.x, 2.0f * s4.y - hh1.y + 2.0f * hh2.y);
     const float2 d = make_float2(s43 * t.x - c112 * pcv.x, s43 * t.y - c112 * pcv.y);
@@ -304,9 +303,9 @@ struct OpCorrectMT {
     pc = mm(pc, m); out_hi = mm(out_hi, m); out_lo = mm(out_lo, m); den = mm(den, m);
     tm.remap(mm, m);
   }
-  HE_D void at(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
-               const float* v8, const float2* v16, int vs, double* acc) const {
-    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tm.re(ix, iy, iz), h2o2m);
+  HE_D void at_t(int ix, int iy, int iz, long i, float2 dx, float2 dy, float2 dz, float2 c,
+               const float* v8, const float2* v16, int vs, double* acc, double tr) const {
+    const float2 s4 = hpsi_any_f<QU>(dx, dy, dz, c, v8, vs, mu, (float)tr, h2o2m);
     const HL2 pred = hl2(c, v16[0]);
     const HL2 a3 = hl2(v16[vs], v16[2 * vs]), a2 = hl2(v16[3 * vs], v16[4 * vs]);
     const float2 b1 = v16[5 * vs], b2 = v16[6 * vs], pco = v16[7 * vs];

@@ -80,7 +80,8 @@ HE_D void zmix_body(const ZMixArgs& a) {
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
   const int nxh = a.nxh;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = threadIdx.x;
+  const int nthr = (N > 0) ? tile_threads(TILE) : (int)blockDim.x;  // compile-time when N > 0
   const int kx0 = blockIdx.x * TK;
   const int ky = blockIdx.y;
   C* tw = smem;

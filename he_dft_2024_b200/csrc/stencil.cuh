@@ -100,6 +100,13 @@ HE_D ReduceTail remap(const ReduceTail& r, const MemberMap& mm, int m) {
 // Stencil ops that run over the members of a group carry remap(mm, m), which maps their device
 // pointers to member m's buffers.
 template <class O, class = void>
+struct HasTimec : std::false_type {};
+// Ops whose H psi carries the absorbing factor timec (ops.cuh Timec) take it as at_t(..., tr): the
+// pass evaluates its x-y part once per column and loads each plane's z part one plane ahead.
+template <class O>
+struct HasTimec<O, std::void_t<decltype(std::declval<const O&>().tm.with_z(0.0, 0.0))>>
+    : std::true_type {};
+template <class O, class = void>
 struct HasRemap : std::false_type {};
 template <class O>
 struct HasRemap<O, std::void_t<decltype(std::declval<O&>().remap(std::declval<const MemberMap&>(), 0))>>
@@ -307,6 +314,13 @@ HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g
     }
   };
 
+  // timec of this column: the x-y part, and the z part of the next plane (HasTimec)
+  [[maybe_unused]] double txy = 0.0, azn = 0.0;
+  if constexpr (HasTimec<Op>::value) {
+    if (inside) txy = op.tm.xy(ix, iy);
+    azn = op.tm.az[z0];
+  }
+
   // Prologue: z-queue f(z0-6 .. z0+5), the next column value f(z0+6) and plane z0's stage.
   T q[13];
 #pragma unroll
@@ -323,6 +337,7 @@ HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g
   for (int iz = z0; iz < z1; ++iz) {
     const int b = (iz - z0) & 1;
     T* tb = tiles + b * TILE;
+    [[maybe_unused]] const double azc = azn;
 #pragma unroll
     for (int m = 0; m < 12; ++m) q[m] = q[m + 1];
     q[12] = qn;
@@ -337,6 +352,7 @@ HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g
     if (iz + 1 < z1) {
       issue_plane(b ^ 1, iz + 1);
       qn = column(iz + 7);
+      if constexpr (HasTimec<Op>::value) azn = op.tm.az[iz + 1];
     }
     if (PF > 0) {
       prefetch_ops(iz + 1 + PF);
@@ -357,8 +373,12 @@ HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g
 #pragma unroll
         for (int m = 0; m < 13; ++m) dz = axpy(W[2][m], q[m], dz);
       }
-      op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
-            st16 + b * Op::N16 * NT + tid, NT, acc);
+      if constexpr (HasTimec<Op>::value)
+        op.at_t(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
+                st16 + b * Op::N16 * NT + tid, NT, acc, op.tm.with_z(txy, azc));
+      else
+        op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
+              st16 + b * Op::N16 * NT + tid, NT, acc);
     }
   }
   if constexpr (Op::NV > 0) {
