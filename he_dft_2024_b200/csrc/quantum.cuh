@@ -113,23 +113,33 @@ HE_D void zmix_body(const ZMixArgs& a) {
     }
   }
   if (a.nout == 0) return;
-  for (int e = tid; e < TK * n; e += nthr) {
-    const int j = e / TK, c = e - j * TK;
-    const int kx = kx0 + c;
-    const int s = c * ls + sw<N>(j);
-    const long g = base + kx + plane * j;
-    for (int o = 0; o < a.nout; ++o) {
-      C acc = Cx<Rt>::make(0, 0);
-      if (kx < nxh) {
-        for (int t = 0; t < a.nterm[o]; ++t) {
-          const C* src = reinterpret_cast<const C*>(a.src[o][t]);
-          const C v = src ? src[g] : F[s];
-          const Rt w = reinterpret_cast<const Rt*>(a.ker[o][t])[g];
-          acc.x += v.x * w;
-          acc.y += v.y * w;
-        }
+  // out[o] = sum_t src_t * ker_t, term by term: each term's loads of all the thread's elements
+  // are issued together (the element loop unrolls for the compile-time lengths); the running sum
+  // stays in the thread's own slots of O0 / O1, added in term order as a register sum would be
+  for (int o = 0; o < a.nout; ++o) {
+    C* Oo = (o == 0) ? O0 : O1;
+#pragma unroll
+    for (int e = tid; e < TK * n; e += nthr) {
+      const int j = e / TK, c = e - j * TK;
+      Oo[c * ls + sw<N>(j)] = Cx<Rt>::make(0, 0);
+    }
+    for (int t = 0; t < a.nterm[o]; ++t) {
+      const C* src = reinterpret_cast<const C*>(a.src[o][t]);
+      const Rt* ker = reinterpret_cast<const Rt*>(a.ker[o][t]);
+#pragma unroll
+      for (int e = tid; e < TK * n; e += nthr) {
+        const int j = e / TK, c = e - j * TK;
+        const int kx = kx0 + c;
+        if (kx >= nxh) continue;
+        const int s = c * ls + sw<N>(j);
+        const long g = base + kx + plane * j;
+        const C v = src ? src[g] : F[s];
+        const Rt w = ker[g];
+        C acc = Oo[s];
+        acc.x += v.x * w;
+        acc.y += v.y * w;
+        Oo[s] = acc;
       }
-      (o == 0 ? O0 : O1)[s] = acc;
     }
   }
   __syncthreads();
