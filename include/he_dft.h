@@ -331,7 +331,7 @@ int he_set_fft_variant(he_ctx_t* ctx, int pass, int variant, int tile);
 int he_state_fingerprint(const he_ctx_t* ctx, unsigned long long* out);
 int he_timing_report(he_ctx_t* ctx, he_kernel_time_t* out, int max, int* n);
 
-/* ---- groups: several statics droplets advanced by one launch per kernel ----
+/* ---- groups: several statics droplets or quantum-impurity trajectories, one launch per kernel ----
  * No counterpart in the reference (its drivers run one droplet per process).  he_ctx_group makes
  * ctxs[0] the leader of n contexts created alike (same mode, precision, grid, functional and
  * impurity masses; binary64 statics or quantum-impurity mode, OT or OP core), each set up on its own (uploads, he_set_kernels or
