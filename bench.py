@@ -1080,8 +1080,35 @@ def run_serving(args):
     torch.cuda.set_device(local)
     reqs = S.make_requests(count=args.requests, rate_hz=args.rate, steps=args.req_steps,
                            seed=1234 + rank)
-    srv = S.Server(lambda w: Context(w, precision=args.precision), hbm_budget_gb=args.hbm_gb,
-                   max_active=args.max_active if args.max_active > 0 else None)
+    class DeviceStepTimer:
+        """CUDA events around each trajectory's iteration on its context's own stream."""
+        def __init__(self):
+            self.pairs = []
+
+        def start(self, ctx):
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(ctx.torch_stream)
+            self.pairs.append([e, None])
+
+        def stop(self, ctx):
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(ctx.torch_stream)
+            self.pairs[-1][1] = e
+
+        def intervals(self):
+            out = [a.elapsed_time(b) for a, b in self.pairs]
+            self.pairs = []
+            return out
+
+    def make_context(w):
+        c = Context(w, precision=args.precision)
+        c.torch_stream = torch.cuda.Stream()  # one stream per context, as the library's own
+        c.set_stream(c.torch_stream.cuda_stream)
+        return c
+
+    srv = S.Server(make_context, hbm_budget_gb=args.hbm_gb,
+                   max_active=args.max_active if args.max_active > 0 else None,
+                   step_timer=DeviceStepTimer())
     with ClockSampler(local) as clk:
         rep = srv.run(reqs)
     launches = None
@@ -1096,7 +1123,10 @@ def run_serving(args):
                    "requests": args.requests, "rate_hz": args.rate, "steps_per_request": args.req_steps,
                    "hbm_budget_gb": args.hbm_gb, "max_active": args.max_active,
                    "grids": rep["grids"], "parallelism": f"replicas{ws}"},
-        "latency": {k: rep[k] for k in ("step_ms_p50", "step_ms_p99", "trajectory_s_p50",
+        # step_ms: the tick (every active trajectory advances one step per tick); device_step_ms:
+        # a trajectory's own step on its stream; trajectory_s: arrival to completion
+        "latency": {k: rep[k] for k in ("step_ms_p50", "step_ms_p99", "device_step_ms_p50",
+                                         "device_step_ms_p99", "trajectory_s_p50",
                                          "trajectory_s_p99")},
         "peak_active": rep["peak_active"], "peak_device_gb": rep["peak_device_gb"],
         "wall_s": rep["wall_s"], "gpu_launches": launches, "clocks": clk.summary(),

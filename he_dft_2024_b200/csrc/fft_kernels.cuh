@@ -63,17 +63,19 @@ HE_D double corr_source(double den, double dcg, double cp4, double cpp4) {
   return den * dcg * (cp4 + cpp4 * dcg);
 }
 
-// Hermitian-extended packed value Z[k] = A[k] + i B[k] of two half-spectrum rows.
+// Hermitian-extended packed value Z[k] = A[k] + i B[k] of two half-spectrum rows.  hasb = false:
+// the second row is zero (the last, unpaired row of an odd row count).  Only the real parts of
+// the DC term and, for even n, of the Nyquist term enter a C2R.
 template <typename C>
-HE_D C packed_c2r(const C* ra, const C* rb, int k, int n) {
+HE_D C packed_c2r(const C* ra, const C* rb, int k, int n, bool hasb = true) {
   using X = Cx<decltype(ra[0].x)>;
   const int nh = n / 2;
   if (k <= nh) {
-    C a = ra[k], b = rb[k];
-    if (k == 0 || k == nh) { a.y = 0; b.y = 0; }
+    C a = ra[k], b = hasb ? rb[k] : X::make(0, 0);
+    if (k == 0 || 2 * k == n) { a.y = 0; b.y = 0; }
     return X::make(a.x - b.y, a.y + b.x);
   }
-  C a = ra[n - k], b = rb[n - k];
+  C a = ra[n - k], b = hasb ? rb[n - k] : X::make(0, 0);
   return X::make(a.x + b.y, -a.y + b.x);
 }
 
@@ -304,6 +306,9 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
   // issue their global loads together
   const int nthr = (N > 0) ? tile_threads(TILE) : (int)blockDim.x;
   const long r0 = (long)blockIdx.x * RB;
+  // rows past a.rows (the last tile of an odd row count, run-time lengths only) read as zero and
+  // are not stored
+  const long rows = a.rows;
   C* tw = smem;
   C* P0 = smem + ((a.pl.stw_len + 1) & ~1);
   C* P1 = P0 + RB * ls;
@@ -313,15 +318,19 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
     const long g0 = r0 * n;
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
-      double v = den[g0 + e];
-      if constexpr (MODE == X_R2C_CORR) v = corr_source(v, dencg_in[g0 + e], a.cp4, a.cpp4);
+      double v = 0.0;
+      if (r0 + row < rows) {
+        v = den[g0 + e];
+        if constexpr (MODE == X_R2C_CORR) v = corr_source(v, dencg_in[g0 + e], a.cp4, a.cpp4);
+      }
       reinterpret_cast<Rt*>(&P0[(row >> 1) * ls + sw<N>(x)])[row & 1] = Rt(v);
     }
     __syncthreads();
     C* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, false);
     for (int e = tid; e < RB * nxh; e += nthr) {
       const int row = e / nxh, k = e - row * nxh;
-      specA[(r0 + row) * nxh + k] = split_r2c<N>(R + (row >> 1) * ls, k, n, row & 1);
+      if (r0 + row < rows)
+        specA[(r0 + row) * nxh + k] = split_r2c<N>(R + (row >> 1) * ls, k, n, row & 1);
     }
     return;
   }
@@ -329,9 +338,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
   if constexpr (MODE == X_C2R2 || MODE == X_C2R2_CORR) {
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, k = e - row * n;
-      const C* ra = specA + (r0 + row) * nxh;
-      const C* rbp = specB + (r0 + row) * nxh;
-      P0[row * ls + sw<N>(k)] = packed_c2r(ra, rbp, k, n);
+      const bool in = r0 + row < rows;
+      const C* ra = specA + (in ? r0 + row : 0) * nxh;
+      const C* rbp = specB + (in ? r0 + row : 0) * nxh;
+      P0[row * ls + sw<N>(k)] = in ? packed_c2r(ra, rbp, k, n) : Cx<Rt>::make(0, 0);
     }
     __syncthreads();
     C* R = fft_lines<N>(P0, P1, RB, ls, a.pl, tw, true);
@@ -339,13 +349,16 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
       const long g = (r0 + row) * n + x;
+      const bool in = r0 + row < rows;
       const C z = R[row * ls + sw<N>(x)];
       const double dcg = double(z.x) * a.renor1;
-      out1[g] = Rs(dcg);
-      out2[g] = Rs(double(z.y) * a.renor);
+      if (in) {
+        out1[g] = Rs(dcg);
+        out2[g] = Rs(double(z.y) * a.renor);
+      }
       if constexpr (MODE == X_C2R2_CORR)
         reinterpret_cast<Rt*>(&O[(row >> 1) * ls + sw<N>(x)])[row & 1] =
-            Rt(corr_source(den[g], dcg, a.cp4, a.cpp4));
+            in ? Rt(corr_source(den[g], dcg, a.cp4, a.cpp4)) : Rt(0);
     }
     if constexpr (MODE == X_C2R2) return;
     __syncthreads();
@@ -353,7 +366,8 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
     C* R2 = fft_lines<N>(O, S, RB / 2, ls, a.pl, tw, false);
     for (int e = tid; e < RB * nxh; e += nthr) {
       const int row = e / nxh, k = e - row * nxh;
-      specA[(r0 + row) * nxh + k] = split_r2c<N>(R2 + (row >> 1) * ls, k, n, row & 1);
+      if (r0 + row < rows)
+        specA[(r0 + row) * nxh + k] = split_r2c<N>(R2 + (row >> 1) * ls, k, n, row & 1);
     }
     return;
   }
@@ -362,14 +376,16 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_xpass_c(const XArgs a)
     // rows 2p and 2p+1 share complex line p
     for (int e = tid; e < (RB / 2) * n; e += nthr) {
       const int p = e / n, k = e - p * n;
-      const C* ra = specA + (r0 + 2 * p) * nxh;
-      const C* rbp = specA + (r0 + 2 * p + 1) * nxh;
-      P0[p * ls + sw<N>(k)] = packed_c2r(ra, rbp, k, n);
+      const bool ina = r0 + 2 * p < rows, inb = r0 + 2 * p + 1 < rows;
+      const C* ra = specA + (ina ? r0 + 2 * p : 0) * nxh;
+      const C* rbp = specA + (inb ? r0 + 2 * p + 1 : 0) * nxh;
+      P0[p * ls + sw<N>(k)] = ina ? packed_c2r(ra, rbp, k, n, inb) : Cx<Rt>::make(0, 0);
     }
     __syncthreads();
     C* R = fft_lines<N>(P0, P1, RB / 2, ls, a.pl, tw, true);
     for (int e = tid; e < RB * n; e += nthr) {
       const int row = e / n, x = e - row * n;
+      if (r0 + row >= rows) continue;
       const long g = (r0 + row) * n + x;
       const C z = R[(row >> 1) * ls + sw<N>(x)];
       if constexpr (MODE == X_C2R1) {

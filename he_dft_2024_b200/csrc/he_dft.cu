@@ -586,7 +586,9 @@ static bool yz_fast(int n) {
 template <int MODE, int N, int TILE, typename Rt>
 static int xpass_n(he_ctx_t* ctx, const XArgs& a) {
   const int rb = (N > 0) ? TILE : a.rb;
-  const long ntiles = a.rows / rb;  // rb divides ny*nz (x_fast, he_ctx_create)
+  // compile-time lengths: rb divides ny*nz (x_fast); run-time lengths: the last tile may be
+  // partial (an odd row count), its missing rows read as zero and are not stored
+  const long ntiles = (a.rows + rb - 1) / rb;
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   static const char* names[6] = {"fft_x_r2c_den", "fft_x_r2c_corr", "fft_x_c2r_cg_lj",
                                  "fft_x_c2r_cg_lj_r2c_corr", "fft_x_c2r_pot4", "fft_x_c2r"};
@@ -2483,8 +2485,8 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
     bad(HE_ERR_ARG, "icon must be 13, 8, 18 or 24");
   else if (!tstgrid_ok(grid->nx) || !tstgrid_ok(grid->ny) || !tstgrid_ok(grid->nz))
     bad(HE_ERR_ARG, "grid size is not an admissible tstgrid value");
-  else if (grid->nx % 2 || grid->ny < 2 || (grid->ny * (long)grid->nz) % 2)
-    bad(HE_ERR_ARG, "nx must be even and ny*nz even");
+  else if (grid->ny < 2)
+    bad(HE_ERR_ARG, "ny must be at least 2");
   else if (!factor_ok(grid->nx) || !factor_ok(grid->ny) || !factor_ok(grid->nz))
     bad(HE_ERR_ARG, "grid size must be 2^a 3^b 5^c");
   else if (grid->xmax == 0.0 || grid->ymax == 0.0 || grid->zmax == 0.0)
@@ -2547,7 +2549,9 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
   ctx->tkx = tile_rows(nmax);
   ctx->x_rb = tile_rows(ctx->nx);
-  while (ctx->x_rb > 2 && ((long)ctx->ny * ctx->nz) % ctx->x_rb) ctx->x_rb -= 2;
+  // an even tile that divides the row count, else (odd ny*nz) the default with a partial last tile
+  if (((long)ctx->ny * ctx->nz) % 2 == 0)
+    while (ctx->x_rb > 2 && ((long)ctx->ny * ctx->nz) % ctx->x_rb) ctx->x_rb -= 2;
   ctx->smem_x = fft_smem(ctx->plx, tile_rows(ctx->nx), 2);
   ctx->smem_y = fft_smem(ctx->ply, ctx->tkx, 2);
   ctx->smem_z = fft_smem(ctx->plz, ctx->tkx, 3);

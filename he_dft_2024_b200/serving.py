@@ -4,9 +4,10 @@ The reference runs one trajectory per process (Dynamics_TDDFT/DFT4He3d.f90).  A 
 trajectory requests as they arrive needs, around the same call surface, a scheduler that
 
 * picks each request's grid: the smallest n in GRIDS with n*h/2 >= R + MARGIN for some h in
-  [H_MIN, H_MAX], R = 2.22 N^(1/3) (readen.f90:98); the spacing is then H_MAX for every request,
-  so that all requests on the same n share k-space kernels, weights and absorber tables and a
-  retired trajectory's context can serve the next request on that grid;
+  [H_MIN, H_MAX], R = 2.22 N^(1/3) (readen.f90:98), and then the finest spacing of H_STEPS
+  (0.5, 0.6, 0.7 A) at which that box still holds the droplet; requests on the same (n, h) share
+  k-space kernels, weights and absorber tables, and a retired trajectory's context serves the
+  next request on that grid;
 * admits requests while their device footprint fits an HBM budget (footprints are measured from
   the contexts themselves, he_device_bytes), queueing the rest in arrival order;
 * advances every admitted trajectory by one driver iteration per tick (3 RK-Gill starts, then
@@ -34,17 +35,18 @@ from . import driver as D
 
 GRIDS = (64, 96, 128, 160, 192, 256)
 H_MIN, H_MAX = 0.5, 0.7
+H_STEPS = (0.5, 0.6, 0.7)  # spacings served (requests on one (n, h) share contexts)
 MARGIN = 15.0
 
 
 def grid_for(n4: int):
     """(n, h) for a droplet of n4 atoms: the smallest admissible n whose box at h = H_MAX covers
-    R + MARGIN, and h = H_MAX."""
+    R + MARGIN, then the finest spacing of H_STEPS at which that box still covers it."""
     R = 2.22 * n4 ** (1.0 / 3.0)
     need = R + MARGIN
     for n in GRIDS:
         if n * H_MAX / 2.0 >= need:
-            return n, H_MAX
+            return n, next(h for h in H_STEPS if n * h / 2.0 >= need)
     raise ValueError(f"droplet of {n4} atoms does not fit the largest grid")
 
 
@@ -60,7 +62,8 @@ class Request:
     # filled by the server
     admitted_s: Optional[float] = None
     done_s: Optional[float] = None
-    step_ms: List[float] = field(default_factory=list)
+    step_ms: List[float] = field(default_factory=list)       # tick times (the step as seen)
+    device_step_ms: List[float] = field(default_factory=list)  # this trajectory's own step
     final: Optional[dict] = None
 
     def workload(self) -> C.Workload:
@@ -121,8 +124,11 @@ class Server:
     default; tests pass a fake)."""
 
     def __init__(self, make_context: Callable, hbm_budget_gb=120.0, clock: Callable = None,
-                 sleep: Callable = None, max_active: Optional[int] = None):
+                 sleep: Callable = None, max_active: Optional[int] = None, step_timer=None):
         self.make_context = make_context
+        # optional device timer: start(ctx) / stop(ctx) around each trajectory's iteration,
+        # intervals() (after the tick's synchronisation) each one's device time in that order
+        self.step_timer = step_timer
         self.budget = hbm_budget_gb * 1e9
         # cap on concurrently advancing trajectories: every active trajectory shares each tick,
         # so fewer active ones finish sooner (latency) at about the same aggregate throughput
@@ -201,10 +207,17 @@ class Server:
             ts = clock()
             for a in active:
                 w_dt = a.req.workload().deltat if dt_for is None else dt_for(a.req)
+                if self.step_timer:
+                    self.step_timer.start(a.ctx)
                 D.dynamics_iteration(a.ctx, a.it, w_dt, 1)
+                if self.step_timer:
+                    self.step_timer.stop(a.ctx)
             for a in active:
                 a.ctx.synchronize()
             te = clock()
+            if self.step_timer:
+                for a, ms in zip(active, self.step_timer.intervals()):
+                    a.req.device_step_ms.append(ms)
             self.ticks += 1
             self.peak_active = max(self.peak_active, len(active))
             self.peak_bytes = max(self.peak_bytes, self.in_use + self._pooled_bytes())
@@ -232,6 +245,7 @@ class Server:
 
     def report(self, reqs, wall_s):
         steps = np.concatenate([np.asarray(r.step_ms) for r in reqs]) if reqs else np.zeros(1)
+        dev = np.concatenate([np.asarray(r.device_step_ms) for r in reqs]) if reqs else np.zeros(0)
         lat = np.asarray([r.done_s - r.arrival_s for r in reqs])
         pts = float(sum(r.n ** 3 * r.steps for r in reqs))
         return {
@@ -241,6 +255,8 @@ class Server:
             "grid_pt_steps_per_s": pts / wall_s if wall_s > 0 else None,
             "step_ms_p50": float(np.percentile(steps, 50)),
             "step_ms_p99": float(np.percentile(steps, 99)),
+            "device_step_ms_p50": float(np.percentile(dev, 50)) if dev.size else None,
+            "device_step_ms_p99": float(np.percentile(dev, 99)) if dev.size else None,
             "trajectory_s_p50": float(np.percentile(lat, 50)),
             "trajectory_s_p99": float(np.percentile(lat, 99)),
             "peak_active": self.peak_active,

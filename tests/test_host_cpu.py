@@ -49,11 +49,19 @@ def test_tstgrid_sizes_enforced():
     (dict(core=b"OTC", den0s=0.0), "den0s"),
     (dict(core=b"OTE"), "core4"),
     (dict(mode=7), "mode"),
-    (dict(nx=45), "nx must be even"),
+    (dict(ny=1), "ny must be at least 2"),
 ])
 def test_bad_arguments_rejected(kw, text):
     st, msg = _create(**kw)
     assert st == _lib.HE_ERR_ARG and text in msg
+
+
+@pytest.mark.parametrize("shape", [(45, 32, 32), (27, 27, 27), (75, 45, 25)])
+def test_odd_tstgrid_sizes_pass_validation(shape):
+    # odd nx and odd ny*nz are admissible (tstgrid.f90:9-13); without a GPU the create then fails
+    # at the device, not at the argument checks
+    st, msg = _create(*shape)
+    assert st != _lib.HE_ERR_ARG, msg
 
 
 def test_no_cpu_fallback_without_device():

@@ -14,7 +14,11 @@ def test_grid_choice():
         assert n * h / 2 >= R + S.MARGIN
         smaller = [g for g in S.GRIDS if g < n]
         assert all(g * S.H_MAX / 2 < R + S.MARGIN for g in smaller)
-        assert S.H_MIN <= h <= S.H_MAX
+        assert S.H_MIN <= h <= S.H_MAX and h in S.H_STEPS
+        # the finest served spacing whose box still holds the droplet
+        assert all(n * f / 2 < R + S.MARGIN for f in S.H_STEPS if f < h)
+    # a droplet whose box fits 128^3 at 0.6 A gets 0.6 A there (N = 1000: R + 15 = 37.2 A)
+    assert S.grid_for(1000) == (128, 0.6)
 
 
 def test_request_stream_is_seeded():
@@ -140,3 +144,29 @@ def test_max_active_caps_concurrency():
     srv.run(rs, dt_for=lambda r: 1e-5)
     assert srv.peak_active == 2
     assert all(r.final is not None for r in rs)
+
+
+def test_device_step_timer_gets_one_interval_per_trajectory_and_tick():
+    class Timer:
+        def __init__(self):
+            self.open, self.n = [], 0
+
+        def start(self, ctx):
+            self.open.append(ctx)
+
+        def stop(self, ctx):
+            assert self.open[-1] is ctx
+
+        def intervals(self):
+            out = [1.5] * len(self.open)
+            self.open = []
+            return out
+
+    FakeCtx.made = 0
+    clk = FakeClock()
+    srv = S.Server(FakeCtx, hbm_budget_gb=100, clock=clk, sleep=clk.sleep, step_timer=Timer())
+    rs = reqs(3, steps=5, spacing=0.0)
+    rep = srv.run(rs, dt_for=lambda r: 1e-5)
+    for r in rs:
+        assert r.device_step_ms == [1.5] * 5
+    assert rep["device_step_ms_p50"] == 1.5 and rep["device_step_ms_p99"] == 1.5
