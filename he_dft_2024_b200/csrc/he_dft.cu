@@ -131,6 +131,10 @@ struct he_ctx {
   double *denalf = nullptr, *falfs = nullptr, *intxalf = nullptr, *intyalf = nullptr,
          *intzalf = nullptr, *ualphas = nullptr, *ua_raw = nullptr;
   double *as1 = nullptr, *as2 = nullptr, *as3 = nullptr, *as4 = nullptr, *as5 = nullptr;
+  // mixed path with OTC: the binary64 copy of den the alpha_s term runs on, and the binary32 copy
+  // of ualphas the binary32 pot4 epilogue adds
+  double* den64 = nullptr;
+  float* ualphas_f = nullptr;
   // quantum impurities (HE_MODE_QUANTUM); psixold[i][s-1] is Fortran slot s of impurity i
   int nq = 0;
   double mu4 = 0.0, h2o2mx[kMaxQImp] = {};
@@ -1695,6 +1699,73 @@ static double alfa_energy(const he_ctx_t* ctx) {
   return -ctx->fn.h2o2m4 * 0.5 * ctx->fn.alphas * ctx->hsum[S_ALF] * ctx->dxyz;
 }
 
+__global__ void __launch_bounds__(256) k_to_f32(const double* __restrict__ a, float* __restrict__ b,
+                                                long n, double scale);
+__global__ void __launch_bounds__(256) k_to_f64(const float* __restrict__ a, double* __restrict__ b, long n);
+
+// The binary64 passes inside a mixed-precision context: the pass dispatch reads ctx->mixed, the
+// binary64 kernels are unscaled (cg_scale 1) and the x pass runs one-shot (the pipelined variant's
+// tiles were tuned for the binary32 chain's shared memory).  Restored on scope exit.
+struct Binary64Passes {
+  he_ctx_t* c;
+  bool mixed;
+  double cg_scale;
+  bool xpipe[6];
+  explicit Binary64Passes(he_ctx_t* ctx) : c(ctx), mixed(ctx->mixed), cg_scale(ctx->cg_scale) {
+    for (int m = 0; m < 6; ++m) { xpipe[m] = c->xpipe[m]; c->xpipe[m] = false; }
+    c->mixed = false;
+    c->cg_scale = 1.0;
+  }
+  ~Binary64Passes() {
+    for (int m = 0; m < 6; ++m) c->xpipe[m] = xpipe[m];
+    c->mixed = mixed;
+    c->cg_scale = cg_scale;
+  }
+};
+
+// grad den into dxden, dyden, dzden (binary64 den; derden.f90:26-28)
+static int derden_of(he_ctx_t* ctx, const double* den) {
+  if (!ctx->dxden) {
+    TRY(dalloc_t(ctx, &ctx->dxden, ctx->N));
+    TRY(dalloc_t(ctx, &ctx->dyden, ctx->N));
+    TRY(dalloc_t(ctx, &ctx->dzden, ctx->N));
+  }
+  OpDerden op{};
+  op.gx = ctx->dxden; op.gy = ctx->dyden; op.gz = ctx->dzden;
+  return run_stencil(ctx, ctx->g1, den, op);
+}
+
+// core4 = 'OTC' in the dynamics modes: derden, the alpha_s density and term_alfa
+// (Dynamics_TDDFT/poten.f90:144, :200-210; quantum poten.f90:48, :126-139).  The mixed path runs
+// them in binary64 on a binary64 copy of den (denalf = C2R(R2C(den) kalfs), which equals the
+// reference's C2R(fden kalfs) for the current den) and hands the binary32 epilogue a binary32
+// copy of ualphas.  Returns the ualphas array the pot4 epilogue adds (binary32 or binary64).
+static int otc_terms(he_ctx_t* ctx, const double** ualphas) {
+  if (!ctx->mixed) {
+    TRY(derden_of(ctx, ctx->den));
+    TRY(alfa_density(ctx));
+    TRY(term_alfa(ctx));
+    *ualphas = ctx->ualphas;
+    return HE_OK;
+  }
+  tname(ctx, "alphas_convert");
+  k_to_f64<<<kPwBlocks, 256, 0, ctx->stream>>>((const float*)ctx->den, ctx->den64, ctx->N);
+  LAUNCHED();
+  {
+    Binary64Passes f64(ctx);
+    TRY(derden_of(ctx, ctx->den64));
+    const double* in[1] = {ctx->den64};
+    double* out[1] = {ctx->denalf};
+    TRY(conv_fields(ctx, in, out, 1, ctx->kalfs));
+    TRY(term_alfa(ctx));
+  }
+  tname(ctx, "alphas_convert");
+  k_to_f32<<<kPwBlocks, 256, 0, ctx->stream>>>(ctx->ualphas, ctx->ualphas_f, ctx->N, 1.0);
+  LAUNCHED();
+  *ualphas = reinterpret_cast<const double*>(ctx->ualphas_f);
+  return HE_OK;
+}
+
 // ------------------------------------------------------------------------------------------------
 // quantum impurities (HE_MODE_QUANTUM, Dynamics_quantum_impurities)
 // ------------------------------------------------------------------------------------------------
@@ -1859,12 +1930,9 @@ static int q_poten(he_ctx_t* ctx) {
   a.den = ctx->den;
   a.out1 = ctx->dencg; a.out2 = ctx->delj4;
   TRY(xpass<X_C2R2_CORR>(ctx, a));
-  if (ctx->otc) {  // Dynamics_quantum_impurities/poten.f90:48 (derden), :126-139
-    TRY(he_derden(ctx));
-    TRY(alfa_density(ctx));
-    TRY(term_alfa(ctx));
-  }
-  return correlation_tail(ctx, ctx->potx4, ctx->otc ? ctx->ualphas : nullptr);
+  const double* ua = nullptr;
+  if (ctx->otc) TRY(otc_terms(ctx, &ua));  // Dynamics_quantum_impurities/poten.f90:48, :126-139
+  return correlation_tail(ctx, ctx->potx4, ua);
 }
 
 static int q_field(he_ctx_t* ctx) {
@@ -2417,6 +2485,10 @@ __global__ void __launch_bounds__(256) k_to_f32(const double* __restrict__ a, fl
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     b[i] = (float)(a[i] * scale);
 }
+__global__ void __launch_bounds__(256) k_to_f64(const float* __restrict__ a, double* __restrict__ b, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
 // Refreshes the binary32 kernel copies of the mixed chain after the binary64 kernels changed;
 // wcgk's copy carries the power-of-two scale cg_scale (see he_ctx).
 static int kernels_to_f32(he_ctx_t* ctx) {
@@ -2477,8 +2549,8 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS && mode != HE_MODE_QUANTUM)
     bad(HE_ERR_ARG, "unknown mode");
   else if (precision != HE_PREC_F64 && precision != HE_PREC_MIXED) bad(HE_ERR_ARG, "unknown precision");
-  else if (precision == HE_PREC_MIXED && std::strncmp(fun->core4, "OTC", 3) == 0)
-    bad(HE_ERR_ARG, "HE_PREC_MIXED does not cover core4='OTC'");
+  else if (precision == HE_PREC_MIXED && mode == HE_MODE_STATICS && std::strncmp(fun->core4, "OTC", 3) == 0)
+    bad(HE_ERR_ARG, "HE_PREC_MIXED covers core4='OTC' in the dynamics modes only");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
   else if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18 &&
            grid->icon != 24)
@@ -2592,6 +2664,10 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (mode == HE_MODE_QUANTUM || ctx->otc) {
     TRY(dalloc_t(ctx, &ctx->wC, Nk));
     TRY(dalloc_t(ctx, &ctx->wD, Nk));
+  }
+  if (ctx->otc && ctx->mixed) {
+    TRY(dalloc_t(ctx, &ctx->den64, N));
+    TRY(dalloc_t(ctx, &ctx->ualphas_f, N));
   }
   if (ctx->otc) {
     TRY(dalloc_t(ctx, &ctx->kalfs, Nk));
@@ -3059,12 +3135,9 @@ int he_poten(he_ctx_t* ctx) {
   a.den = ctx->den;
   a.out1 = ctx->dencg; a.out2 = ctx->delj4;
   TRY(xpass<X_C2R2_CORR>(ctx, a));
-  if (ctx->otc) {  // Dynamics_TDDFT/poten.f90:144 (derden), :200-210 (denalf, term_alfa)
-    TRY(he_derden(ctx));
-    TRY(alfa_density(ctx));
-    TRY(term_alfa(ctx));
-  }
-  return correlation_tail(ctx, nullptr, ctx->otc ? ctx->ualphas : nullptr);
+  const double* ua = nullptr;
+  if (ctx->otc) TRY(otc_terms(ctx, &ua));  // Dynamics_TDDFT/poten.f90:144, :200-210
+  return correlation_tail(ctx, nullptr, ua);
 }
 
 
@@ -3395,14 +3468,7 @@ int he_energy(he_ctx_t* ctx, he_energies_t* out) {
 int he_derden(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
   if (ctx->mixed) return fail(ctx, HE_ERR_STATE, "derden is not part of the mixed-precision path");
-  if (!ctx->dxden) {
-    TRY(dalloc_t(ctx, &ctx->dxden, ctx->N));
-    TRY(dalloc_t(ctx, &ctx->dyden, ctx->N));
-    TRY(dalloc_t(ctx, &ctx->dzden, ctx->N));
-  }
-  OpDerden op{};
-  op.gx = ctx->dxden; op.gy = ctx->dyden; op.gz = ctx->dzden;
-  return run_stencil(ctx, ctx->g1, ctx->den, op);
+  return derden_of(ctx, ctx->den);
 }
 
 int he_lstopimp(he_ctx_t* ctx, int* flag) {
