@@ -1766,6 +1766,39 @@ static int otc_terms(he_ctx_t* ctx, const double** ualphas) {
   return HE_OK;
 }
 
+// The statics refresh's part of the alpha_s term (BCN4HeDFT.f90:1142-1148): denalf from the
+// refreshed fden (and, through he_derden, the gradients poten's term_alfa uses); in the mixed
+// path both in binary64 from a binary64 copy of the refreshed den.
+static int statics_alfa_density(he_ctx_t* ctx) {
+  if (!ctx->mixed) return alfa_density(ctx);
+  tname(ctx, "alphas_convert");
+  k_to_f64<<<kPwBlocks, 256, 0, ctx->stream>>>((const float*)ctx->den, ctx->den64, ctx->N);
+  LAUNCHED();
+  Binary64Passes f64(ctx);
+  TRY(derden_of(ctx, ctx->den64));
+  const double* in[1] = {ctx->den64};
+  double* out[1] = {ctx->denalf};
+  return conv_fields(ctx, in, out, 1, ctx->kalfs);
+}
+// The statics poten's term_alfa (He_statics/poten.f90:86-91) on the refresh's denalf and
+// gradients; the mixed path runs it in binary64 and returns ualphas' binary32 copy.
+static int statics_term_alfa(he_ctx_t* ctx, const double** ualphas) {
+  if (!ctx->mixed) {
+    TRY(term_alfa(ctx));
+    *ualphas = ctx->ualphas;
+    return HE_OK;
+  }
+  {
+    Binary64Passes f64(ctx);
+    TRY(term_alfa(ctx));
+  }
+  tname(ctx, "alphas_convert");
+  k_to_f32<<<kPwBlocks, 256, 0, ctx->stream>>>(ctx->ualphas, ctx->ualphas_f, ctx->N, 1.0);
+  LAUNCHED();
+  *ualphas = reinterpret_cast<const double*>(ctx->ualphas_f);
+  return HE_OK;
+}
+
 // ------------------------------------------------------------------------------------------------
 // quantum impurities (HE_MODE_QUANTUM, Dynamics_quantum_impurities)
 // ------------------------------------------------------------------------------------------------
@@ -2549,8 +2582,6 @@ int he_ctx_create(const he_grid_t* grid, const he_functional_t* fun, int mode, i
   if (mode != HE_MODE_DYNAMICS && mode != HE_MODE_STATICS && mode != HE_MODE_QUANTUM)
     bad(HE_ERR_ARG, "unknown mode");
   else if (precision != HE_PREC_F64 && precision != HE_PREC_MIXED) bad(HE_ERR_ARG, "unknown precision");
-  else if (precision == HE_PREC_MIXED && mode == HE_MODE_STATICS && std::strncmp(fun->core4, "OTC", 3) == 0)
-    bad(HE_ERR_ARG, "HE_PREC_MIXED covers core4='OTC' in the dynamics modes only");
   else if (grid->npd != 13) bad(HE_ERR_ARG, "npd must be 13");
   else if (grid->icon != 13 && grid->icon != 8 && grid->icon != 18 &&
            grid->icon != 24)
@@ -3125,8 +3156,9 @@ int he_poten(he_ctx_t* ctx) {
     a.den = ctx->den; a.dencg_in = ctx->dencg;
     a.specA = ctx->wA;
     TRY(xpass<X_R2C_CORR>(ctx, a));
-    if (ctx->otc) TRY(term_alfa(ctx));  // He_statics/poten.f90:86-91 (denalf from the refresh)
-    return correlation_tail(ctx, nullptr, ctx->otc ? ctx->ualphas : nullptr);
+    const double* ua = nullptr;
+    if (ctx->otc) TRY(statics_term_alfa(ctx, &ua));  // He_statics/poten.f90:86-91 (denalf from the refresh)
+    return correlation_tail(ctx, nullptr, ua);
   }
   if (ctx->xyfuse && !ctx->otc) return poten_fused(ctx, nullptr, nullptr);
   TRY(spectrum_cg_lj(ctx));
@@ -3486,14 +3518,15 @@ int he_refresh_density(he_ctx_t* ctx) {
   if (!ctx) return HE_ERR_ARG;
   if (ctx->mode != HE_MODE_STATICS) return fail(ctx, HE_ERR_STATE, "statics routine");
   if (!ctx->kernels_ok) return fail(ctx, HE_ERR_STATE, "k-space kernels not set");
-  // (the gradients feed only the alpha_s term, which the mixed path does not cover)
+  // the gradients feed only the alpha_s term: binary64 ones of a binary64 copy of den in the
+  // mixed path with OTC, none in the mixed path otherwise
   if (!ctx->mixed) TRY(he_derden(ctx));
   TRY(spectrum_cg_lj(ctx));
   XArgs a = xargs(ctx);
   a.specA = ctx->wA; a.specB = ctx->wB;
   a.out1 = ctx->dencg; a.out2 = ctx->delj4;
   TRY(xpass<X_C2R2>(ctx, a));
-  if (ctx->otc) TRY(alfa_density(ctx));  // BCN4HeDFT.f90:1142-1148
+  if (ctx->otc) TRY(statics_alfa_density(ctx));  // BCN4HeDFT.f90:1142-1148
   return HE_OK;
 }
 

@@ -38,9 +38,9 @@ typedef struct he_ctx he_ctx_t;
 /* HE_MODE_QUANTUM: real-time dynamics with quantum impurities (Dynamics_quantum_impurities):
  * complex psi plus impurity wave functions psix_i (he_set_quantum_impurities). */
 enum he_mode { HE_MODE_DYNAMICS = 0, HE_MODE_STATICS = 1, HE_MODE_QUANTUM = 2 };
-/* HE_PREC_F64: binary64 throughout.  HE_PREC_MIXED (every mode with the OT/OP cores, and the
- * dynamics modes with OTC, whose alpha_s term then runs in binary64 on a binary64 copy of den
- * and adds a binary32 copy of ualphas to pot4; in the quantum mode
+/* HE_PREC_F64: binary64 throughout.  HE_PREC_MIXED (every mode and core; with OTC the alpha_s
+ * term runs in binary64 on a binary64 copy of den and adds a binary32 copy of ualphas to pot4;
+ * in the quantum mode
  * psix and psixold are pairs too, upotx / potx4 / denx binary32; in the statics mode the real
  * psi, psiold and pc are pairs, H psi binary32, and the imaginary-time updates and the norm, mu
  * and error sums binary64): the FFT chain

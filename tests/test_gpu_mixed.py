@@ -70,7 +70,7 @@ def test_mixed_rejects_unsupported_modes():
     with Context(w, precision="mixed") as ctx:
         with pytest.raises(HeError):
             ctx.derden()
-    # core4 = 'OTC' is covered in the dynamics modes (test_gpu_mixed_otc.py), not in statics
+    # core4 = 'OTC' is covered (test_gpu_mixed_otc.py)
 
 
 def test_mixed_field_formats_round_trip():

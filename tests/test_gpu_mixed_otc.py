@@ -1,4 +1,4 @@
-"""core4 = 'OTC' in the mixed-precision path (classical and quantum-impurity dynamics): the alpha_s
+"""core4 = 'OTC' in the mixed-precision path (classical and quantum-impurity dynamics, statics): the alpha_s
 term (term_alfa.f90) runs in binary64 on a binary64 copy of the binary32 density, and its field
 enters the binary32 pot4 epilogue.  Compared with the FP64 run of the same state (itself pinned to
 the oracle in test_gpu_alphas.py), at the mixed path's bars: fields to 2e-6 of their max, energy
@@ -66,8 +66,22 @@ def test_mixed_otc_quantum_dynamics_matches_f64():
     assert np.max(np.abs(mx[2] - f64[2])) < 1e-6
 
 
-def test_mixed_otc_statics_is_refused():
+def test_mixed_otc_statics_matches_f64():
+    """4He_500 statics with OTC on 32^3: set-up and 30 imaginary-time iterations, mu and E/N."""
     w = C.replace(C.statics_500(), nx=32, ny=32, nz=32, xmax=11.2, ymax=11.2, zmax=11.2,
                   core="OTC", lsolid=0)
-    with pytest.raises(Exception):
-        Context(w, mode="statics", precision="mixed")
+    den = C.woods_saxon(w)
+    out = {}
+    for prec in ("f64", "mixed"):
+        with Context(w, mode="statics", precision=prec) as ctx:
+            mu = D.statics_setup(ctx, den, w.n4)
+            ua = ctx.download("ualphas")
+            for it in range(1, 31):
+                mu = D.statics_iteration(ctx, it, w.deltat_statics, mu, w.n4)[0]
+            out[prec] = (mu, ctx.energy(), ua)
+    f64, mx = out["f64"], out["mixed"]
+    assert rel(mx[2], f64[2]) < 2e-6
+    assert abs(mx[0] - f64[0]) <= 1e-5 * abs(f64[0])
+    assert abs(mx[1]["etot"] - f64[1]["etot"]) / w.n4 < 1e-5
+    assert mx[1]["ealphas"] != 0.0
+    assert abs(mx[1]["ealphas"] - f64[1]["ealphas"]) <= 1e-5 * abs(f64[1]["ealphas"])
