@@ -471,7 +471,10 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_ypass(const YZArgs a)
 ;
 #endif
 
-template <int N, int TILE, typename Rt, bool G>
+// TWO: the second kernel k2 (out2, and the forward spectrum stored in fden_out) -- a compile-time
+// choice, so that the one-kernel convolution carries neither its registers nor its third line
+// buffer (the host passes two line buffers of shared memory then).
+template <int N, int TILE, typename Rt, bool G, bool TWO>
 __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
 #ifdef HE_KERNEL_TU
 {
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
   const double* kern2 = on_member<G>(a.mm, a.k2, mem);
   const float* kern1f = on_member<G>(a.mm, a.k1f, mem);
   const float* kern2f = on_member<G>(a.mm, a.k2f, mem);
-  const bool two = F32 ? kern2f != nullptr : kern2 != nullptr;
+  constexpr bool two = TWO;
   const int n = (N > 0) ? N : a.nz;
   const int ls = line_stride(n);
   const int TK = (N > 0) ? TILE : a.tkx;
@@ -509,7 +512,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
   // compile-time lengths: element e = tid + j nthr, j < EPT, and the kernel values of the
   // multiply are loaded before the forward transform, so their latency hides behind it
   constexpr int EPT = (N > 0) ? N / 16 : 1;  // TK n / nthr with nthr = 16 TK
-  Rt w1p[EPT], w2p[EPT];
+  Rt w1p[EPT], w2p[TWO ? EPT : 1];
   if constexpr (N > 0) {
 #pragma unroll
     for (int j = 0; j < EPT; ++j) {
@@ -518,7 +521,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
       const bool ok = kx0 + c < nxh;
       const long g = base + (ok ? kx0 + c : 0) + plane * jj;
       w1p[j] = ok ? (F32 ? Rt(kern1f[g]) : Rt(kern1[g])) : Rt(0);
-      w2p[j] = (ok && two) ? (F32 ? Rt(kern2f[g]) : Rt(kern2[g])) : Rt(0);
+      if constexpr (TWO) w2p[j] = ok ? (F32 ? Rt(kern2f[g]) : Rt(kern2[g])) : Rt(0);
     }
   }
 #pragma unroll
@@ -547,7 +550,7 @@ __global__ void __launch_bounds__(tile_threads(TILE)) k_zconv(const YZArgs a)
   };
   if constexpr (N > 0) {
 #pragma unroll
-    for (int j = 0; j < EPT; ++j) multiply(tid + j * nthr, w1p[j], w2p[j]);
+    for (int j = 0; j < EPT; ++j) multiply(tid + j * nthr, w1p[j], TWO ? w2p[TWO ? j : 0] : Rt(0));
   } else {
     for (int e = tid; e < TK * n; e += nthr) {
       const int j = e / TK, c = e - j * TK;

@@ -714,10 +714,13 @@ static int zconv_n(he_ctx_t* ctx, const YZArgs& a) {
       return HE_OK;
     }
   }
-  const size_t smem = fft_smem(ctx->plz, tk, 3, sizeof(typename Cx<Rt>::T));
+  // one-kernel convolutions: two line buffers and no second kernel's registers
+  const bool two = (sizeof(Rt) == 4) ? a.k2f != nullptr : a.k2 != nullptr;
+  const size_t smem = fft_smem(ctx->plz, tk, two ? 3 : 2, sizeof(typename Cx<Rt>::T));
   const int nthr = (N > 0) ? tile_threads(TILE) : 256;
   dim3 grid((ctx->nxh + tk - 1) / tk, ctx->ny, ctx->nmem);
-  void (*k)(YZArgs) = ctx->nmem > 1 ? k_zconv<N, TILE, Rt, true> : k_zconv<N, TILE, Rt, false>;
+  void (*k)(YZArgs) = two ? (ctx->nmem > 1 ? k_zconv<N, TILE, Rt, true, true> : k_zconv<N, TILE, Rt, false, true>)
+                          : (ctx->nmem > 1 ? k_zconv<N, TILE, Rt, true, false> : k_zconv<N, TILE, Rt, false, false>);
   CK(set_smem_attr((const void*)k, smem));
   tname(ctx, a.k2 ? "fft_z_conv2" : "fft_z_conv1");
   CK(launch_chain(ctx, k, grid, dim3(nthr), smem, a));
