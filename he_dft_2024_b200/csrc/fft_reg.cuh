@@ -207,6 +207,11 @@ template <bool INV> struct RDft<16, INV> : RDftComp<4, 4, INV> {};
 
 // Threads of a y-pass CTA: TK columns x N2.
 HE_HD constexpr int yreg_threads(int n, int tk) { return tk * (n / split_n1(n)); }
+// Resident CTAs the y pass asks the compiler for: 24 warps per SM where a line's N1 values fit
+// without spilling (N1 <= 8; 128: 6 CTAs of 128 threads, 85 registers), no minimum otherwise.
+HE_HD constexpr int yreg_min_blocks(int n, int tk) {
+  return split_n1(n) <= 8 ? 768 / yreg_threads(n, tk) : 0;
+}
 
 template <int N, int TK, bool INV, bool G, typename C>
 HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
@@ -251,7 +256,7 @@ HE_D void ypass_reg_body(const YZArgs& a, const C* __restrict__ tw2, C* T) {
 }
 
 template <int N, int TK, typename Rt, bool G>
-__global__ void __launch_bounds__(yreg_threads(N, TK)) k_ypass_reg(const YZArgs a,
+__global__ void __launch_bounds__(yreg_threads(N, TK), yreg_min_blocks(N, TK)) k_ypass_reg(const YZArgs a,
                                                                    const typename Cx<Rt>::T* tw2)
 #ifdef HE_KERNEL_TU
 {
