@@ -1157,12 +1157,12 @@ __global__ void __launch_bounds__(256) k_stat_rk(const StatPW s_in, const Reduce
 
 // psi = |psi| * sqrt(n4/(sum psi^2 dxyz)); den = psi^2.
 __global__ void __launch_bounds__(256) k_stat_normalize(double* psi, double* den, long N,
-                                                        const double* sums, double n4,
+                                                        const double* sums, int slot, double n4,
                                                         double dxyz, const MemberMap mm) {
   psi = mm(psi, blockIdx.y);
   den = mm(den, blockIdx.y);
   sums = mm(sums, blockIdx.y);
-  const double cnorm = sqrt(n4 / (sums[S_STAT_N] * dxyz));
+  const double cnorm = sqrt(n4 / (sums[slot] * dxyz));
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N;
        i += (long)gridDim.x * blockDim.x) {
     const double v = fabs(psi[i]) * cnorm;
@@ -1287,8 +1287,9 @@ __global__ void __launch_bounds__(256) k_stat_rk_m(const StatPWM s, const Reduce
   reduce_tail<1>(rt, gridDim.x);
 }
 __global__ void __launch_bounds__(256) k_stat_normalize_m(float* psi, float* den, long N,
-                                                          const double* sums, double n4, double dxyz) {
-  const double cnorm = sqrt(n4 / (sums[S_STAT_N] * dxyz));
+                                                          const double* sums, int slot, double n4,
+                                                          double dxyz) {
+  const double cnorm = sqrt(n4 / (sums[slot] * dxyz));
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
     const double v = fabs(ld_pair(psi, i, N)) * cnorm;
     st_pair(psi, i, N, v);
@@ -1397,14 +1398,17 @@ static int stat_hpsi(he_ctx_t* ctx, double* out, int slot) {
   return run_stencil_red(ctx, ctx->g2, (const double*)ctx->psi, op, slot);
 }
 
-static int stat_normalize(he_ctx_t* ctx, int n4) {
+// psi *= sqrt(n4 / (sum psi^2 dxyz)), den = psi^2, with the norm sum from `slot`
+static int stat_normalize(he_ctx_t* ctx, int n4, int slot = S_STAT_N) {
   tname(ctx, "statics_normalize");
   if (ctx->mixed)
     k_stat_normalize_m<<<pw_blocks(ctx), 256, 0, ctx->stream>>>((float*)ctx->psi, (float*)ctx->den,
-                                                                ctx->N, ctx->sums, (double)n4, ctx->dxyz);
+                                                                ctx->N, ctx->sums, slot, (double)n4,
+                                                                ctx->dxyz);
   else
     k_stat_normalize<<<pw_grid(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
-                                                            ctx->sums, (double)n4, ctx->dxyz, ctx->mm);
+                                                            ctx->sums, slot, (double)n4, ctx->dxyz,
+                                                            ctx->mm);
   LAUNCHED();
   return HE_OK;
 }
@@ -3680,11 +3684,8 @@ static int steppcr_launch(he_ctx_t* ctx, double deltat, int n4) {
     LAUNCHED();
     std::swap(ctx->psi, ctx->scratch);
   }
-  // k_stat_correct leaves sum psi^2 in S_STAT_PC+1; the normalisation reads S_STAT_N.
-  tname(ctx, "copy_slot");
-  k_copy_slot<<<dim3(1, ctx->nmem), 32, 0, ctx->stream>>>(ctx->sums, S_STAT_N, S_STAT_PC + 1, ctx->mm);
-  LAUNCHED();
-  TRY(stat_normalize(ctx, n4));
+  // k_stat_correct leaves sum psi^2 in S_STAT_PC+1, which the normalisation reads
+  TRY(stat_normalize(ctx, n4, S_STAT_PC + 1));
   const int a = ctx->ioldp[2];
   ctx->ioldp[2] = ctx->ioldp[1];
   ctx->ioldp[1] = ctx->ioldp[0];
