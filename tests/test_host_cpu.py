@@ -21,6 +21,19 @@ def test_library_exports_every_header_symbol():
     assert not missing, missing
 
 
+def test_library_defines_every_kernel_it_launches():
+    # the heavy kernels are compiled in their own translation units from the host objects'
+    # undefined symbols; the linked library must leave none of the package's symbols undefined
+    import shutil
+    import subprocess
+    if not shutil.which("nm"):
+        pytest.skip("nm not available")
+    lib = _lib.load()._name
+    und = subprocess.run(["nm", "-u", "-C", lib], capture_output=True, text=True, check=True).stdout
+    missing = [ln.strip() for ln in und.splitlines() if "he::" in ln]
+    assert not missing, missing[:5]
+
+
 def _create(nx=32, ny=32, nz=32, npd=13, icon=13, core=b"OT ", mode=0, den0s=0.04):
     L = _lib.load()
     g = _lib.HeGrid(nx, ny, nz, 10.0, 10.0, 10.0, npd, icon)
