@@ -1069,6 +1069,10 @@ struct StatPW {
   double* den;
   double a, b, c;
   int jr;
+  // reduction blocks: nlb logical blocks (one partial each, the element split of a grid of nlb
+  // CTAs), lpb of them per CTA; groups give a CTA several so that it carries more work, with the
+  // same partials, hence the same sums, as a context run alone (0: one per CTA, nlb = gridDim.x)
+  int nlb, lpb;
   MemberMap mm;       // group members (blockIdx.y is the member)
   HE_D void remap(int m) {
     sums = mm(sums, m); psi = mm(psi, m); out = mm(out, m); po3 = mm(po3, m); po2 = mm(po2, m);
@@ -1088,9 +1092,11 @@ __global__ void __launch_bounds__(256) k_stat_predict(const StatPW s_in, const R
   const ReduceTail rt = remap(rt_in, s.mm, blockIdx.y);
   const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
   const double hmean = s.sums[S_STAT_H] * s.dxyz / s.n4;
+  const int nlb = s.lpb > 0 ? s.nlb : (int)gridDim.x, lpb = s.lpb > 0 ? s.lpb : 1;
+  for (int j = 0; j < lpb; ++j) {
+  const int lb = blockIdx.x * lpb + j;
   double acc[1] = {0.0};
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < s.N;
-       i += (long)gridDim.x * blockDim.x) {
+  for (long i = lb * (long)blockDim.x + threadIdx.x; i < s.N; i += (long)nlb * blockDim.x) {
     const double ps = s.psi[i], hp = s.hpsi[i];
     const double tc = local_dt(hp, ps, s);
     s.timec[i] = tc;
@@ -1102,8 +1108,10 @@ __global__ void __launch_bounds__(256) k_stat_predict(const StatPW s_in, const R
     s.h2[i] = s4;
     acc[0] += pn * pn;
   }
-  block_reduce_store<1>(acc, rt.partials + blockIdx.x);
-  reduce_tail<1>(rt, gridDim.x);
+  if (j > 0) __syncthreads();  // the block reduction's shared buffer is reused
+  block_reduce_store<1>(acc, rt.partials + lb);
+  }
+  reduce_tail<1>(rt, nlb, gridDim.x);
 }
 
 // steppcr corrector + final value (steppcr.f90:78-90); acc = {sum |pc|, sum psi_new^2}.
@@ -1113,9 +1121,11 @@ __global__ void __launch_bounds__(256) k_stat_correct(const StatPW s_in, const R
   const ReduceTail rt = remap(rt_in, s.mm, blockIdx.y);
   const double c9 = 9.0 / 121.0;
   const double mu = s.sums[S_STAT_MU] * s.dxyz / s.n4;
+  const int nlb = s.lpb > 0 ? s.nlb : (int)gridDim.x, lpb = s.lpb > 0 ? s.lpb : 1;
+  for (int j = 0; j < lpb; ++j) {
+  const int lb = blockIdx.x * lpb + j;
   double acc[2] = {0.0, 0.0};
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < s.N;
-       i += (long)gridDim.x * blockDim.x) {
+  for (long i = lb * (long)blockDim.x + threadIdx.x; i < s.N; i += (long)nlb * blockDim.x) {
     const double ps = s.psi[i];
     const double s4 = -(s.hpsi[i] - mu * ps);
     const double s5 =
@@ -1127,8 +1137,10 @@ __global__ void __launch_bounds__(256) k_stat_correct(const StatPW s_in, const R
     acc[0] += fabs(p);
     acc[1] += o * o;
   }
-  block_reduce_store<2>(acc, rt.partials + 2 * blockIdx.x);
-  reduce_tail<2>(rt, gridDim.x);
+  if (j > 0) __syncthreads();  // the block reduction's shared buffer is reused
+  block_reduce_store<2>(acc, rt.partials + 2 * lb);
+  }
+  reduce_tail<2>(rt, nlb, gridDim.x);
 }
 
 // steprkr stage update (steprkr.f90:160-179); acc = sum psi_new^2.
@@ -1329,6 +1341,10 @@ static int pw_blocks(const he_ctx_t* ctx) {
 }
 // Grid of a pointwise kernel: blockIdx.y is the member of a group.
 static dim3 pw_grid(const he_ctx_t* ctx) { return dim3(pw_blocks(ctx), ctx->nmem); }
+// Logical reduction blocks per CTA of the statics pointwise passes: 4 in a group (so that a CTA
+// carries more than a couple of points per thread), 1 for a context alone.
+static int pw_lpb(const he_ctx_t* ctx) { return (ctx->nmem > 1 && pw_blocks(ctx) % 4 == 0) ? 4 : 1; }
+static dim3 pw_grid_lb(const he_ctx_t* ctx) { return dim3(pw_blocks(ctx) / pw_lpb(ctx), ctx->nmem); }
 
 template <int NI, typename TT>
 static int launch_impfield_t(he_ctx_t* ctx) {
@@ -1406,7 +1422,7 @@ static int stat_normalize(he_ctx_t* ctx, int n4, int slot = S_STAT_N) {
                                                                 ctx->N, ctx->sums, slot, (double)n4,
                                                                 ctx->dxyz);
   else
-    k_stat_normalize<<<pw_grid(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
+    k_stat_normalize<<<pw_grid_lb(ctx), 256, 0, ctx->stream>>>((double*)ctx->psi, ctx->den, ctx->N,
                                                             ctx->sums, slot, (double)n4, ctx->dxyz,
                                                             ctx->mm);
   LAUNCHED();
@@ -3645,7 +3661,9 @@ static int steppcr_launch(he_ctx_t* ctx, double deltat, int n4) {
     s.h2 = (double*)ctx->hpsiold[ctx->ioldh[1] - 1];
     s.pc = (double*)ctx->pc;
     tname(ctx, "statics_predict");
-    k_stat_predict<<<pw_grid(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
+    s.nlb = pw_blocks(ctx);
+    s.lpb = pw_lpb(ctx);
+    k_stat_predict<<<pw_grid_lb(ctx), 256, 0, ctx->stream>>>(s, tail(ctx, S_STAT_N));
     LAUNCHED();
     std::swap(ctx->psi, ctx->psiold[ctx->ioldp[2] - 1]);
     std::swap(ctx->ioldh[0], ctx->ioldh[1]);
@@ -3680,7 +3698,9 @@ static int steppcr_launch(he_ctx_t* ctx, double deltat, int n4) {
     s.out = (double*)ctx->scratch;
     ReduceTail rt = tail(ctx, S_STAT_PC);
     tname(ctx, "statics_correct");
-    k_stat_correct<<<pw_grid(ctx), 256, 0, ctx->stream>>>(s, rt);
+    s.nlb = pw_blocks(ctx);
+    s.lpb = pw_lpb(ctx);
+    k_stat_correct<<<pw_grid_lb(ctx), 256, 0, ctx->stream>>>(s, rt);
     LAUNCHED();
     std::swap(ctx->psi, ctx->scratch);
   }

@@ -113,14 +113,16 @@ struct HasRemap<O, std::void_t<decltype(std::declval<O&>().remap(std::declval<co
     : std::true_type {};
 
 template <int NV>
-__device__ void reduce_tail(const ReduceTail& rt, long nb) {
+// nb partials, written by ncta CTAs (ncta < 0: one partial per CTA); the last CTA to finish sums
+// them in a fixed order that depends on nb and the CTA's thread count only.
+__device__ void reduce_tail(const ReduceTail& rt, long nb, long ncta = -1) {
   __shared__ bool s_last;
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nthr = blockDim.x * blockDim.y * blockDim.z;
   if (tid == 0) {
     __threadfence();
     const unsigned t = atomicAdd(rt.counter, 1u);
-    s_last = (t == (unsigned)(nb - 1));
+    s_last = (t == (unsigned)((ncta < 0 ? nb : ncta) - 1));
   }
   __syncthreads();
   if (!s_last) return;
