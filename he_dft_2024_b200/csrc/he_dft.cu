@@ -1341,9 +1341,9 @@ static int pw_blocks(const he_ctx_t* ctx) {
 }
 // Grid of a pointwise kernel: blockIdx.y is the member of a group.
 static dim3 pw_grid(const he_ctx_t* ctx) { return dim3(pw_blocks(ctx), ctx->nmem); }
-// Logical reduction blocks per CTA of the statics pointwise passes: 4 in a group (so that a CTA
+// Logical reduction blocks per CTA of the statics pointwise passes: 8 in a group (so that a CTA
 // carries more than a couple of points per thread), 1 for a context alone.
-static int pw_lpb(const he_ctx_t* ctx) { return (ctx->nmem > 1 && pw_blocks(ctx) % 4 == 0) ? 4 : 1; }
+static int pw_lpb(const he_ctx_t* ctx) { return (ctx->nmem > 1 && pw_blocks(ctx) % 8 == 0) ? 8 : 1; }
 static dim3 pw_grid_lb(const he_ctx_t* ctx) { return dim3(pw_blocks(ctx) / pw_lpb(ctx), ctx->nmem); }
 
 template <int NI, typename TT>
