@@ -516,9 +516,12 @@ static int run_stencil(he_ctx_t* ctx, const StencilGeom& g0, const typename Op::
     TRY(ensure_partials(ctx, (size_t)grid.x * grid.y * grid.z * Op::NV));
     rt = tail(ctx, slot);
   }
-  g.nzc = (int)grid.z;  // blockIdx.z = member x nzc + chunk
+  g.nzc = (int)grid.z;  // z-chunks per member
   g.mm = ctx->mm;
-  grid.z *= ctx->nmem;
+  // a group's CTAs each stream through lcz consecutive chunks (at least 16 planes), so that the
+  // 12-plane start of a chunk is paid once per CTA; the partials are still one per chunk
+  g.lcz = ctx->nmem > 1 ? std::max(1, std::min(g.nzc, 16 / std::max(1, g.zc))) : 1;
+  grid.z = (unsigned)(((g.nzc + g.lcz - 1) / g.lcz) * ctx->nmem);
   CK(set_smem_attr((const void*)k, smem));
   tname(ctx, Op::kname());
   k<<<grid, block, smem, ctx->stream>>>(f, g, op, rt);

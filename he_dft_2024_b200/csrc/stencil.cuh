@@ -34,6 +34,7 @@ struct StencilGeom {
   int icon;          // 13, 8, 18 or 24
   int axis_on[3];    // 0 when n(axis) < npd
   int nzc;           // z-chunks per member: grid.z = nzc x members (0: grid.z, one member)
+  int lcz;           // groups: consecutive z-chunks one CTA streams through (one partial each)
   MemberMap mm;      // group members' buffers (nmem = 1 outside a group)
   double w[3][13];   // scaled weights per axis
   float wf[3][13];   // the same in binary32 (stencils over binary32 fields)
@@ -178,10 +179,12 @@ HE_HD constexpr size_t stencil_smem() {
          2 * (size_t)Op::N8 * TX * TY * sizeof(typename RT::R);
 }
 
-// The stencil pass of one member; bz is the CTA's z-chunk within the member's grid of nzc.
+// The stencil pass of one member; the CTA streams through z-chunks bz .. bz + nchunk - 1 of the
+// member's nzc, with one reduction partial per chunk (so the sums do not depend on nchunk), and
+// ncta CTAs per member report to the reduction tail (< 0: one per chunk).
 template <class Op, int TX, int TY>
 HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g, const Op& op,
-                      const ReduceTail& rt, int bz, int nzc) {
+                      const ReduceTail& rt, int bz, int nzc, int nchunk = 1, long ncta = -1) {
   using T = typename Op::T;
   using R = typename RealOf<T>::R;
   using Z = typename RealOf<T>::Z;
@@ -199,7 +202,7 @@ HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int ix = x0 + tx, iy = y0 + ty;
   const int z0 = bz * g.zc;
-  const int z1 = min(z0 + g.zc, g.nz);
+  const int z1 = min(z0 + nchunk * g.zc, g.nz);
   const bool inside = (ix < g.nx) && (iy < g.ny);
   const long plane = (long)g.nx * g.ny;
   const long idx0 = (long)min(ix, g.nx - 1) + (long)g.nx * min(iy, g.ny - 1);
@@ -382,12 +385,24 @@ HE_D void stencil_run(const typename Op::T* __restrict__ f, const StencilGeom& g
         op.at(ix, iy, iz, idx0 + plane * iz, dx, dy, dz, q[6], st8 + b * Op::N8 * NT + tid,
               st16 + b * Op::N16 * NT + tid, NT, acc);
     }
+    if constexpr (Op::NV > 0) {
+      // the end of a chunk other than the last: its partial (the next flush is at least one
+      // plane, and so one barrier, later)
+      if (nchunk > 1 && iz + 1 < z1 && (iz + 1 - z0) % g.zc == 0) {
+        const long c = bz + (iz - z0) / g.zc;
+        const long blk = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * c);
+        block_reduce_store<NV>(acc, rt.partials + blk * NV);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+      }
+    }
   }
   if constexpr (Op::NV > 0) {
     const long nb = (long)gridDim.x * gridDim.y * nzc;
-    const long blk = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * bz);
+    const long c = bz + (z1 - 1 - z0) / g.zc;  // the last chunk
+    const long blk = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * c);
     block_reduce_store<NV>(acc, rt.partials + blk * NV);
-    reduce_tail<NV>(rt, nb);
+    reduce_tail<NV>(rt, nb, ncta);
   }
 }
 
@@ -402,11 +417,15 @@ __global__ void __launch_bounds__(TX* TY, stencil_min_blocks<Op>())
 #ifdef HE_KERNEL_TU
 {
   if constexpr (G) {
-    const int nzc = g.nzc;
-    const int mem = (int)blockIdx.z / nzc;
+    // blockIdx.z = member x nphys + p; CTA p streams chunks p lcz .. p lcz + lcz - 1
+    const int nzc = g.nzc, lcz = g.lcz > 0 ? g.lcz : 1;
+    const int nphys = (nzc + lcz - 1) / lcz;
+    const int mem = (int)blockIdx.z / nphys;
+    const int bz = ((int)blockIdx.z - mem * nphys) * lcz;
     Op o = op;
     o.remap(g.mm, mem);
-    stencil_run<Op, TX, TY>(g.mm(f, mem), g, o, remap(rt, g.mm, mem), (int)blockIdx.z - mem * nzc, nzc);
+    stencil_run<Op, TX, TY>(g.mm(f, mem), g, o, remap(rt, g.mm, mem), bz, nzc, min(lcz, nzc - bz),
+                            (long)gridDim.x * gridDim.y * nphys);
   } else {
     stencil_run<Op, TX, TY>(f, g, op, rt, (int)blockIdx.z, (int)gridDim.z);
   }
